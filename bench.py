@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the distance-driven projector path.
+
+Workload (the headline configuration): cone-beam flat detector, volume
+512x512x256 at 0.75 mm (random-ellipsoid phantom, densities in [0, 1]),
+1440 views over 2*pi, detector 1024x256 at 0.8 mm, SOD 595 mm, SDD 1085 mm.
+One step = forward projection A followed by backprojection B of the
+resulting sinogram, FP32, inputs resident in HBM (both larger than L2).
+
+    value = B*C*Nx*Ny*Nz*V / (t_A + t_B) / 1e9      [Gvoxel-views/s]
+
+summed over ranks (one independent reconstruction per GPU, weak scaling).
+The roofline denominator is the measured HBM copy bandwidth; the algorithmic
+bytes of one operator application are V*(Nvox + Nu*Nv)*4 (each view streams
+the volume and its own projection once).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DD fwd+back Gvoxel-views/s (batched/BF16 vs plain FP32 @1e-3 rel); %HBM peak"
+UNIT = "Gvoxel-views/s"
+WL = dict(W=512, H=512, D=256, Nu=1024, Nv=256, V=1440, dx=0.75, du=0.8, sod=595.0, sdd=1085.0)
+WORKLOAD_NAME = "cone-flat 512x512x256 vol, 1440 views, 1024x256 det, fwd A + back B"
+FALLBACK_HBM = 6650.0
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+def nvox(wl=WL):
+    return wl["W"] * wl["H"] * wl["D"]
+
+
+def algo_bytes_op(wl=WL, s=4):
+    return wl["V"] * (nvox(wl) + wl["Nu"] * wl["Nv"]) * s
+
+
+def make_projector():
+    import xrecon_b200 as xr
+    return xr.Projector3d(xr.Volume3d((WL["W"], WL["H"], WL["D"]), WL["dx"]),
+                          xr.ConeBeam3d(xr.Detector3d((WL["Nu"], WL["Nv"]), WL["du"]), WL["sod"], WL["sdd"], "flat"))
+
+
+def angles_np():
+    import numpy as np
+    return (np.arange(WL["V"]) * (2 * np.pi / WL["V"])).astype(np.float32)
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = Path(f"/tmp/xr_bench_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.idx), "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------- CPU reference
+
+_CPU_VOL = None
+
+
+def cpu_volume():
+    """The seeded phantom of rank 0, rasterised with torch on the host."""
+    global _CPU_VOL
+    if _CPU_VOL is None:
+        from xrecon_b200.phantom import ellipsoid_volume_torch, random_ellipsoids3d
+        v = ellipsoid_volume_torch((WL["D"], WL["H"], WL["W"]), random_ellipsoids3d(20, seed=0, density=(0.0, 1.0)),
+                                   "cpu")
+        _CPU_VOL = v.numpy()[None, None]
+    return _CPU_VOL
+
+
+def cpu_reference_sample(nviews: int = 4, vol=None):
+    """The reference's own CPU operators (oracle/_ref, std::thread x
+    hardware_concurrency) on `nviews` views of the workload: A then B."""
+    from oracle import refcpu
+    if not refcpu.available():
+        return None
+    P = make_projector()
+    opts = P.options.numpy()
+    vol = cpu_volume() if vol is None else vol
+    ang = angles_np()[:: WL["V"] // nviews][:nviews].copy()
+    t0 = time.perf_counter()
+    sino = refcpu.dd3d("A", vol, opts, ang)
+    t1 = time.perf_counter()
+    refcpu.dd3d("B", sino, opts, ang)
+    t2 = time.perf_counter()
+    cores = os.cpu_count() or 1
+    value = nvox() * nviews / (t2 - t0) / 1e9
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{nviews} of {WL['V']} views of the workload (A {t1 - t0:.1f}s + B {t2 - t1:.1f}s)",
+            "seconds": t2 - t0}
+
+
+def run_reference_arm(args, rank: int):
+    if rank != 0:
+        return 0
+    nviews = 2
+    samples = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_sample(nviews)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU library oracle/_ref not built"}))
+            return 0
+        if i >= args.warmup:
+            samples.append(r)
+    t = sum(s["seconds"] for s in samples) / len(samples)
+    value = nvox() * nviews / t / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random ellipsoids)",
+        "config": {"workload": WORKLOAD_NAME, "step": f"A+B on {nviews} views (bounded CPU sample)"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": samples[0]["cores"], "kind": "reference",
+                         "sample": samples[0]["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def run_gpu_arm(args, rank: int, world: int, local_rank: int):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from xrecon_b200.phantom import ellipsoid_volume_torch, random_ellipsoids3d
+
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    P = make_projector().to(dev)
+    D, H, W = WL["D"], WL["H"], WL["W"]
+    vol = ellipsoid_volume_torch((D, H, W), random_ellipsoids3d(20, seed=rank, density=(0.0, 1.0)), dev)
+    vol = vol[None, None].contiguous()
+    ang = torch.from_numpy(angles_np()).to(dev)
+
+    def step(x):
+        s = P.projection(x, ang)
+        return P.backprojection(s, ang)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        step(vol)
+    torch.cuda.synchronize()
+
+    # timed region: per-operator CUDA events on the launching stream
+    stream = torch.cuda.current_stream(dev)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        s = P.projection(vol, ang)
+        ev[i][1].record(stream)
+        r = P.backprojection(s, ang)
+        ev[i][2].record(stream)
+        del s, r
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    t_total = e0.elapsed_time(e1) / 1e3
+    t_a = sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps / 1e3
+    t_b = sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps / 1e3
+    t_step = t_total / args.steps
+    if world > 1:
+        t = torch.tensor([t_step], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_step = float(t.item())
+    value = world * nvox() * WL["V"] / t_step / 1e9
+
+    # end-to-end through the public API with host buffers
+    host_vol = vol.cpu().pin_memory()
+    host_out = torch.empty_like(host_vol).pin_memory()
+    dvol = torch.empty_like(vol)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    torch.cuda.synchronize()
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        dvol.copy_(host_vol, non_blocking=True)
+        out = step(dvol)
+        host_out.copy_(out, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = f0.elapsed_time(f1) / 1e3 / e2e_steps
+    if world > 1:
+        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e_value = world * nvox() * WL["V"] / t_e2e / 1e9
+    vol_bytes = vol.numel() * 4
+
+    # BF16-stored form of the same step (volume and sinogram in BF16, FP32
+    # accumulation), reported beside the FP32 number.
+    bf = {}
+    if not args.no_bf16:
+        vol16 = vol.to(torch.bfloat16)
+        for _ in range(1):
+            step(vol16)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nb = max(1, min(args.steps, 3))
+        g0.record(stream)
+        for _ in range(nb):
+            out16 = step(vol16)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        t16 = g0.elapsed_time(g1) / 1e3 / nb
+        ref32 = step(vol)
+        rel = float((out16.float() - ref32).norm() / ref32.norm())
+        bf = {"value": world * nvox() * WL["V"] / t16 / 1e9, "unit": UNIT, "ms_per_step": t16 * 1e3,
+              "rel_l2_vs_fp32": rel}
+        del vol16, out16, ref32
+
+    hbm, src = peaks()
+    dom_t = max(t_a, t_b)
+    dom = "cell_gather3d (projection A)" if t_a >= t_b else "vox_gather3d (backprojection B)"
+    achieved = algo_bytes_op() / dom_t / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        traffic = json.loads(tp.read_text()).get("A" if t_a >= t_b else "B")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random ellipsoids)",
+        "config": {"workload": WORKLOAD_NAME, "volume": [WL["D"], WL["H"], WL["W"]], "views": WL["V"],
+                   "detector": [WL["Nv"], WL["Nu"]], "ms_projection": t_a * 1e3,
+                   "ms_backprojection": t_b * 1e3,
+                   "l2": "inputs larger than L2 (volume 256 MiB, sinogram 1.41 GiB)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": algo_bytes_op()},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": vol_bytes, "d2h_bytes_per_step": vol_bytes},
+        "gpu_launches": 5 * args.steps,
+        "clocks": clk,
+    }
+    if bf:
+        line["bf16"] = bf
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample = cpu_reference_sample(4, vol.cpu().numpy())
+        line["cpu_baseline"] = {k: v for k, v in sample.items() if k != "seconds"} if sample else None
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-bf16", action="store_true", help="skip the BF16-storage measurement")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_gpu_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

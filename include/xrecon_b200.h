@@ -1,0 +1,118 @@
+/*
+ * xrecon_b200.h -- C ABI of the B200 distance-driven (DD) projector library
+ * (libxrecon_b200.so).  Plain pointers, sizes and a CUDA stream; no torch
+ * types.  Every call is asynchronous on `stream`, allocates nothing (the
+ * caller passes a device workspace sized by the matching *_workspace_size
+ * call), never exits the process, and returns an xr_status.
+ *
+ * Reference interface being replaced: the pybind module `xrecon_C` of XRecon
+ * (src/api/torch_binding.cpp:615-638), whose functions all take
+ * (Tensor input, Tensor options float32, Tensor angles float32 [V]) and
+ * return a new tensor.  The geometry structs below carry exactly the fields
+ * the reference unpacks from `options` (torch_binding.cpp:62-124), in the same
+ * packed units (3D flat: raw du and the raw shift in mm, the kernels apply
+ * SOD/SDD; 3D arc: du/SDD in radians; 2D: the "effective" spacing of
+ * xrecon/projector/geometry.py:105-113).
+ */
+#ifndef XRECON_B200_H
+#define XRECON_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    XR_OK = 0,
+    XR_ERR_INVALID_ARGUMENT = 1,  /* bad geometry, shape, op or dtype      */
+    XR_ERR_WORKSPACE = 2,         /* workspace missing or too small         */
+    XR_ERR_CUDA = 3,              /* a CUDA launch or runtime call failed   */
+    XR_ERR_UNSUPPORTED = 4        /* valid request this build does not do  */
+} xr_status;
+
+/* Operators, numbered as the six per-dimension bindings of the reference. */
+typedef enum {
+    XR_PROJECTION = 0,                 /* forward_projection{2,3}d                    */
+    XR_PROJECTION_T = 1,               /* projection_transpose{2,3}d                  */
+    XR_BACKPROJECTION = 2,             /* backward_projection{2,3}d                   */
+    XR_BACKPROJECTION_T = 3,           /* backward_projection_transpose{2,3}d         */
+    XR_WEIGHTED_BACKPROJECTION = 4,    /* weighted_backward_projection{2,3}d          */
+    XR_WEIGHTED_BACKPROJECTION_T = 5   /* weighted_backward_projection_transpose{2,3}d*/
+} xr_op;
+
+/* Scan geometry, values of the reference's scan_id (geometry.py:63-103). */
+typedef enum { XR_PARALLEL = 0, XR_FAN_FLAT = 1, XR_FAN_ARC = 2 } xr_geometry_type;
+
+/* Storage dtype of image / sinogram buffers.  Accumulation is FP32 always. */
+typedef enum { XR_FLOAT32 = 0, XR_BFLOAT16 = 1, XR_FLOAT16 = 2 } xr_dtype;
+
+/* 2D geometry: the 12 packed options of Projector2d (projector.py:106-110),
+ * unpacked as torch_binding.cpp:62-79. */
+typedef struct {
+    int W, H, Nu, type;
+    float dx, dy, du, sod, sdd, shift_x, shift_y, shift_u;
+} xr_geom2d;
+
+/* 3D geometry: the 18 packed options of Projector3d (projector3d.py:98-107),
+ * unpacked as torch_binding.cpp:82-124 (helical fields are not part of this
+ * path). */
+typedef struct {
+    int W, H, D, Nu, Nv, type;
+    float dx, dy, dz, du, dv, sod, sdd;
+    float shift_x, shift_y, shift_z, shift_u, shift_v;
+} xr_geom3d;
+
+/* Device workspace (bytes) that xr_dd2d / xr_dd3d need for these arguments. */
+size_t xr_dd2d_workspace_size(int op, const xr_geom2d* geom, int nbatch, int nview);
+size_t xr_dd3d_workspace_size(int op, const xr_geom3d* geom, int nbatch, int nview);
+
+/*
+ * Apply one 2D DD operator (replaces the six *2d bindings,
+ * torch_binding.cpp:140-351).
+ *   in / out : device buffers; image layout [nbatch, H, W], sinogram layout
+ *              [nbatch, nview, Nu] (nbatch = B*C of the reference).  `out` is
+ *              fully overwritten (no zero-fill needed).
+ *   angles   : device float32 [nview], radians.
+ *   dtype_in / dtype_out : xr_dtype of `in` / `out`.
+ */
+int xr_dd2d(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,
+            const float* angles, int nbatch, int nview, void* workspace, size_t workspace_bytes,
+            void* stream);
+
+/*
+ * Apply one 3D DD operator (replaces forward_projection3d,
+ * projection_transpose3d, backward_projection3d,
+ * weighted_backward_projection3d, backward_projection_transpose3d and
+ * weighted_backward_projection_transpose3d, torch_binding.cpp:407-523).
+ *   image layout [nbatch, D, H, W], sinogram layout [nbatch, nview, Nv, Nu].
+ */
+int xr_dd3d(int op, const xr_geom3d* geom, const void* in, int dtype_in, void* out, int dtype_out,
+            const float* angles, int nbatch, int nview, void* workspace, size_t workspace_bytes,
+            void* stream);
+
+/*
+ * Fused FBP/FDK pre-filter (replaces the `sino * weight` and
+ * conv2d/conv3d(padding Nu-1) steps of filtered_backprojection,
+ * projector.py:200-201 and projector3d.py:189-190):
+ *   out[row, i] = sum_j in[row, j] * pw[row_view, j] * cosw[j] * filt[j - i + Nu - 1]
+ * for every detector row (nrows = nbatch*nview*Nv rows of Nu samples).
+ *   cosw   : device float32 [Nu] cosine weight (may be NULL = ones)
+ *   filt   : device float32 [2*Nu-1] spatial filter
+ *   parker : device float32 [nview, Nu] short-scan weight or NULL
+ *   rows_per_view : Nv (3D) or 1 (2D), to index `parker` by view.
+ */
+int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, int nview, int rows_per_view,
+                  const float* cosw, const float* filt, const float* parker, void* stream);
+
+/* Human-readable message for the last non-OK status returned on this thread. */
+const char* xr_last_error(void);
+
+/* Library version string. */
+const char* xr_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XRECON_B200_H */

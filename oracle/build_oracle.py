@@ -1,0 +1,71 @@
+"""Build recipe for the test oracle (test infrastructure only).
+
+* ``oracle/lib/libxr_oracle.so`` -- the FP64 C restatement ``dd_oracle.c``.
+* ``oracle/_ref/libxrecon_ref_cpu.so`` -- the reference's own CPU operators
+  (XRecon ``src/cpu/{forward2d,backward2d,system_matrix2d,forward3d,
+  backward3d}.cpp``) compiled in place from the reference sources together with
+  ``ref_shim.cpp``.  Built only where the reference tree is present; the
+  resulting .so travels with the repository snapshot (it is git-ignored).
+
+The reference's own build system is not used: its CPU path is five C++ files
+that only need the reference ``include/`` directory and the CUDA headers for
+the ``__host__ __device__`` qualifiers of ``include/types.h``.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_DIR = HERE / "lib"
+REF_DIR = HERE / "_ref"
+ORACLE_SO = LIB_DIR / "libxr_oracle.so"
+REF_SO = REF_DIR / "libxrecon_ref_cpu.so"
+REFERENCE_ROOT = Path(os.environ.get("XRECON_REFERENCE_ROOT", "/root/reference"))
+REF_CPU_SOURCES = ["forward2d.cpp", "backward2d.cpp", "system_matrix2d.cpp",
+                   "forward3d.cpp", "backward3d.cpp"]
+CUDA_INCLUDE = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "include"
+
+
+def _run(cmd: list[str]) -> None:
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"command failed ({proc.returncode}): {' '.join(cmd)}\n{proc.stderr}")
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps if d.exists())
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = HERE / "dd_oracle.c"
+    LIB_DIR.mkdir(exist_ok=True)
+    if force or _stale(ORACLE_SO, [src]):
+        _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-o", str(ORACLE_SO), str(src), "-lm"])
+    return ORACLE_SO
+
+
+def build_ref(force: bool = False) -> Path | None:
+    """Compile the reference CPU operators; returns None when the reference
+    tree is absent (the prebuilt .so, if shipped, is then used as is)."""
+    cpu_dir = REFERENCE_ROOT / "src" / "cpu"
+    if not cpu_dir.is_dir():
+        return REF_SO if REF_SO.exists() else None
+    srcs = [cpu_dir / s for s in REF_CPU_SOURCES] + [HERE / "ref_shim.cpp"]
+    REF_DIR.mkdir(exist_ok=True)
+    if force or _stale(REF_SO, srcs):
+        # -O3 matches the reference's own C++ flags (setup.py:15).
+        _run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread",
+              f"-I{REFERENCE_ROOT / 'include'}", f"-I{CUDA_INCLUDE}",
+              "-o", str(REF_SO)] + [str(s) for s in srcs])
+    return REF_SO
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="--force" in sys.argv))
+    print(build_ref(force="--force" in sys.argv))

@@ -1,0 +1,405 @@
+/*
+ * dd_oracle.c -- FP64 CPU restatement of XRecon's distance-driven (DD)
+ * operators.  TEST INFRASTRUCTURE ONLY: the product never links, loads or
+ * calls this file; tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline use it as the checker.
+ *
+ * What it restates (paths relative to the XRecon project root):
+ *   geometry conventions   include/types.h:35-119, include/xrmath.h:8-226
+ *   2D projection A        src/cpu/system_matrix2d.cpp:96-365
+ *                          (matrix_parallel / matrix_fanflat / matrix_fanarc)
+ *   2D A^T                 src/cpu/forward2d.cpp:80-112 (adjoint of A)
+ *   2D B, Bw               src/cpu/backward2d.cpp:30-250
+ *   2D B^T, Bw^T           src/cpu/backward2d.cpp:258-473
+ *   3D cone A, A^T         src/cpu/forward3d.cpp:299-585
+ *   3D cone B, Bw, B^T     include/cpu3d_common.h:48-202,
+ *                          src/cpu/backward3d.cpp:10-135
+ *   3D parallel            src/cpu/forward3d.cpp:37-181 (B = A^T, B^T = A)
+ *
+ * Formulation.  For every view the reference maps detector-cell boundaries
+ * and voxel boundaries onto one common axis (the x axis when cos^2 > 1/2,
+ * else the y axis) and, in 3D, maps z boundaries onto that axis' plane with
+ * the magnification of the detector column centre (cells) and of the voxel
+ * line centre (voxels).  Every operator is the same overlap kernel
+ *     K[cell, voxel] = |pixel_axis cap column_axis| * |voxel_z cap row_z|
+ * with a diagonal scale on one side:
+ *     A   = S_cell K,        A^T = K^T S_cell,
+ *     B^T = K T_vox,         B   = T_vox K^T       (Bw: T_vox includes w).
+ * The reference evaluates K with sequential merges in float32; this file
+ * evaluates the identical overlaps with a two-pointer merge in double
+ * precision.  The decisions the reference takes in float (which axis, which
+ * detector traversal order) are taken from float sin/cos of the float angle,
+ * as the reference CPU path does (std::sin/std::cos on float).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+enum { GEO_PARALLEL = 0, GEO_FLAT = 1, GEO_ARC = 2 };
+enum { OP_A = 0, OP_AT = 1, OP_B = 2, OP_BT = 3, OP_BW = 4, OP_BWT = 5 };
+
+typedef struct {
+    int use_x;   /* common axis is x (xrmath.h usage: cos^2 > 0.5) */
+    int keep;    /* detector traversed in index order (keep_dim) */
+    double beta, s, c;
+    double sx, sy;        /* source position, xrmath.h:116-123 */
+    double spar, sperp;   /* source coordinate along / across the axis */
+} view_t;
+
+static view_t make_view(float ang, double sod)
+{
+    view_t v;
+    const float cf = cosf(ang);
+    const float sf = sinf(ang);
+    v.use_x = (cf * cf > 0.5f);
+    v.keep = v.use_x ? (cf >= 0.0f) : (sf >= 0.0f);
+    v.beta = (double)ang;
+    v.s = sin(v.beta);
+    v.c = cos(v.beta);
+    v.sx = -v.s * sod;
+    v.sy = v.c * sod;
+    v.spar = v.use_x ? v.sx : v.sy;
+    v.sperp = v.use_x ? v.sy : v.sx;
+    return v;
+}
+
+/* Signed boundary offset of traversal boundary k (k may be fractional for
+ * cell centres): xrmath.h / forward3d.cpp:236-238 use (k - Nu/2) when the
+ * detector is kept in order and (Nu/2 - k) when it is reversed. */
+static double sigma(const view_t* v, double k, int nu)
+{
+    return v->keep ? (k - 0.5 * nu) : (0.5 * nu - k);
+}
+
+/* map2x / map2y of xrmath.h:8-22: intercept of the ray source->point with
+ * the common axis. */
+static double map_point(const view_t* v, double px, double py)
+{
+    if (v->use_x) return (v->sx * py - v->sy * px) / (py - v->sy);
+    return (v->sy * px - v->sx * py) / (px - v->sx);
+}
+
+/* map2x / map2y for a ray leaving the source at angle a (xrmath.h:24-38). */
+static double map_angle(const view_t* v, double a)
+{
+    if (v->use_x) return v->sx + v->sy * tan(a);
+    return v->sy + v->sx / tan(a);
+}
+
+/* Two-pointer merge of the interval sequences [a_i, a_{i+1}] (i < na) and
+ * [b_j, b_{j+1}] (j < nb), both increasing.  Writes the overlapping pairs. */
+static int overlaps(const double* a, int na, const double* b, int nb,
+                    int* ia, int* ib, double* len)
+{
+    int i = 0, j = 0, n = 0;
+    while (i < na && j < nb) {
+        const double lo = a[i] > b[j] ? a[i] : b[j];
+        const double hi = a[i + 1] < b[j + 1] ? a[i + 1] : b[j + 1];
+        if (hi > lo) { ia[n] = i; ib[n] = j; len[n] = hi - lo; ++n; }
+        if (a[i + 1] < b[j + 1]) ++i; else ++j;
+    }
+    return n;
+}
+
+/* ---------------------------------------------------------------- 3D ---- */
+
+typedef struct {
+    int W, H, D, Nu, Nv, type;
+    double dx, dy, dz, shx, shy, shz;
+    double du, dv, shu, shv, sod, sdd;
+} geo3_t;
+
+/* Per view: column boundaries on the axis (Nu+1), column-centre z scale
+ * (Nu), row boundaries before magnification (Nv+1). */
+static void view_columns3d(const geo3_t* g, const view_t* v,
+                           double* D, double* M, double* zd)
+{
+    const double vs = g->sod / g->sdd;
+    for (int k = 0; k <= g->Nu; ++k) {
+        if (g->type == GEO_FLAT) {
+            /* forward3d.cpp:229-243 (virtual detector through isocentre) */
+            const double u = (sigma(v, k, g->Nu) * g->du + g->shu) * vs;
+            D[k] = map_point(v, u * v->c, u * v->s);
+        } else if (g->type == GEO_ARC) {
+            /* forward3d.cpp:271-283 */
+            const double a = sigma(v, k, g->Nu) * g->du + g->shu + v->beta;
+            D[k] = map_angle(v, a);
+        } else {
+            /* forward3d.cpp:53-56 (parallel: u / cos or u / sin) */
+            const double u = sigma(v, k, g->Nu) * g->du + g->shu;
+            D[k] = v->use_x ? u / v->c : u / v->s;
+        }
+    }
+    for (int k = 0; k < g->Nu; ++k) {
+        double cx, cy;
+        if (g->type == GEO_FLAT) {
+            /* forward3d.cpp:258-269 */
+            const double u = (sigma(v, k + 0.5, g->Nu) * g->du + g->shu) * vs;
+            cx = u * v->c; cy = u * v->s;
+        } else if (g->type == GEO_ARC) {
+            /* forward3d.cpp:285-297 */
+            const double a = sigma(v, k + 0.5, g->Nu) * g->du + g->shu + v->beta;
+            cx = sin(a) * g->sdd + v->sx; cy = -cos(a) * g->sdd + v->sy;
+        } else {
+            cx = cy = 0.0;
+        }
+        if (g->type == GEO_PARALLEL) M[k] = 1.0;
+        else M[k] = v->use_x ? v->sy / (v->sy - cy) : v->sx / (v->sx - cx);
+    }
+    /* forward3d.cpp:318-320: flat rows live on the virtual detector. */
+    const double rs = (g->type == GEO_FLAT) ? vs : 1.0;
+    for (int r = 0; r <= g->Nv; ++r) zd[r] = ((r - 0.5 * g->Nv) * g->dv + g->shv) * rs;
+}
+
+/* Axis boundaries of the pixels of one line and the line's z magnification.
+ * Lines are volume rows iy (x axis) or volume columns ix (y axis);
+ * forward3d.cpp:372-384 and :432-444. */
+static int line_pixels3d(const geo3_t* g, const view_t* v, int line,
+                         double* X, double* Mv, double* perp_coord)
+{
+    if (v->use_x) {
+        const double py = (0.5 * g->H - line - 0.5) * g->dy + g->shy;
+        const double x0 = -0.5 * g->W * g->dx + g->shx;
+        for (int i = 0; i <= g->W; ++i) {
+            const double x = x0 + i * g->dx;
+            X[i] = (g->type == GEO_PARALLEL) ? (v->s / v->c) * py + x : map_point(v, x, py);
+        }
+        *Mv = (g->type == GEO_PARALLEL) ? 1.0 : v->sy / (v->sy - py);
+        *perp_coord = py;
+        return g->W;
+    } else {
+        const double px = (line - 0.5 * g->W + 0.5) * g->dx + g->shx;
+        const double y0 = -0.5 * g->H * g->dy + g->shy;
+        for (int i = 0; i <= g->H; ++i) {
+            const double y = y0 + i * g->dy;
+            X[i] = (g->type == GEO_PARALLEL) ? (v->c / v->s) * px + y : map_point(v, px, y);
+        }
+        *Mv = (g->type == GEO_PARALLEL) ? 1.0 : v->sx / (v->sx - px);
+        *perp_coord = px;
+        return g->H;
+    }
+}
+
+/* Voxel centre coordinates (xrmath.h:163-173; image row 0 is the top). */
+static void voxel_xy(const geo3_t* g, int ix, int iy, double* px, double* py)
+{
+    *px = (ix - 0.5 * g->W + 0.5) * g->dx + g->shx;
+    *py = (0.5 * g->H - iy - 0.5) * g->dy + g->shy;
+}
+
+/* FBP voxel weight: cone_voxel_weight_flat / _arc (xrmath.h:215-226). */
+static double fbp_weight(int type, const view_t* v, double sod, double px, double py)
+{
+    if (type == GEO_FLAT) {
+        const double d = (v->sx * px + v->sy * py) / sod;
+        return sod * sod / ((sod - d) * (sod - d));
+    }
+    if (type == GEO_ARC) {
+        const double ex = v->sx - px, ey = v->sy - py;
+        return 1.0 / (ex * ex + ey * ey);
+    }
+    return 1.0;
+}
+
+/* Apply one 3D operator.  Layouts: image [nb][D][H][W], sino [nb][V][Nv][Nu].
+ * `in` is read, `out` is overwritten. */
+int xo_dd3d(int op, const int* ni, const double* fv, const double* fg, int type,
+            const double* in, double* out, const float* ang, int nbatch, int nview)
+{
+    geo3_t g;
+    g.W = ni[0]; g.H = ni[1]; g.D = ni[2]; g.Nu = ni[3]; g.Nv = ni[4]; g.type = type;
+    g.dx = fv[0]; g.dy = fv[1]; g.dz = fv[2]; g.shx = fv[3]; g.shy = fv[4]; g.shz = fv[5];
+    g.du = fg[0]; g.dv = fg[1]; g.shu = fg[2]; g.shv = fg[3]; g.sod = fg[4]; g.sdd = fg[5];
+    if (op < 0 || op > 5) return 1;
+    if (type == GEO_PARALLEL) {
+        /* backward3d.cpp:101-135: parallel B = Bw = A^T and B^T = Bw^T = A. */
+        if (op == OP_B || op == OP_BW) op = OP_AT;
+        else if (op == OP_BT || op == OP_BWT) op = OP_A;
+    }
+    const long long nvox = (long long)g.W * g.H * g.D;
+    const long long ncell = (long long)g.Nu * g.Nv;
+    const int out_is_sino = (op == OP_A || op == OP_BT || op == OP_BWT);
+    memset(out, 0, sizeof(double) * (size_t)nbatch *
+           (size_t)(out_is_sino ? ncell * nview : nvox));
+
+    const int nline_max = g.W > g.H ? g.W : g.H;
+    double* D = malloc(sizeof(double) * (g.Nu + 1));
+    double* M = malloc(sizeof(double) * g.Nu);
+    double* zd = malloc(sizeof(double) * (g.Nv + 1));
+    double* X = malloc(sizeof(double) * (nline_max + 1));
+    double* Zv = malloc(sizeof(double) * (g.D + 1));
+    double* Zc = malloc(sizeof(double) * (g.Nv + 1));
+    const int nxo = nline_max + g.Nu + 2, nzo = g.D + g.Nv + 2;
+    int* xa = malloc(sizeof(int) * nxo); int* xb = malloc(sizeof(int) * nxo);
+    double* xl = malloc(sizeof(double) * nxo);
+    int* za = malloc(sizeof(int) * nzo); int* zb = malloc(sizeof(int) * nzo);
+    double* zl = malloc(sizeof(double) * nzo);
+
+    const double z0 = -0.5 * g.D * g.dz + g.shz;
+    const double cw = (type == GEO_FLAT) ? g.du * g.sod / g.sdd
+                    : (type == GEO_ARC) ? 2.0 * g.sod * tan(0.5 * g.du) : g.du;
+
+    for (int view = 0; view < nview; ++view) {
+        const view_t v = make_view(ang[view], g.sod);
+        view_columns3d(&g, &v, D, M, zd);
+        const double dperp = v.use_x ? g.dy : g.dx;
+        const int nlines = v.use_x ? g.H : g.W;
+        for (int line = 0; line < nlines; ++line) {
+            double Mv, perp;
+            const int npix = line_pixels3d(&g, &v, line, X, &Mv, &perp);
+            for (int i = 0; i <= g.D; ++i) Zv[i] = Mv * (z0 + i * g.dz);
+            const int nx = overlaps(X, npix, D, g.Nu, xa, xb, xl);
+            for (int e = 0; e < nx; ++e) {
+                const int p = xa[e], k = xb[e];
+                const int ix = v.use_x ? p : line;
+                const int iy = v.use_x ? line : g.H - 1 - p;
+                const int col = v.keep ? k : g.Nu - 1 - k;
+                for (int r = 0; r <= g.Nv; ++r) Zc[r] = M[k] * zd[r];
+                const int nz = overlaps(Zv, g.D, Zc, g.Nv, za, zb, zl);
+                /* voxel-side scale: reference voxel_area = |(X1-X0)(z1-z0)|
+                 * (cpu3d_common.h:80) and the FBP weight (:84-85). */
+                double tvox = 0.0;
+                if (op == OP_B || op == OP_BT || op == OP_BW || op == OP_BWT) {
+                    tvox = cw / ((X[p + 1] - X[p]) * Mv * g.dz);
+                    if (op == OP_BW || op == OP_BWT) {
+                        double px, py;
+                        voxel_xy(&g, ix, iy, &px, &py);
+                        tvox *= fbp_weight(type, &v, g.sod, px, py);
+                    }
+                }
+                for (int q = 0; q < nz; ++q) {
+                    const int iz = za[q], r = zb[q];
+                    const double coef = xl[e] * zl[q];
+                    double sa = 1.0;
+                    if (op == OP_A || op == OP_AT) {
+                        if (type == GEO_PARALLEL) {
+                            /* forward3d.cpp:58, :98: xy_scale / dv */
+                            sa = dperp / (g.du * g.dv);
+                        } else {
+                            /* forward3d.cpp:331-343 */
+                            const double dD = D[k + 1] - D[k];
+                            const double dZ = Zc[r + 1] - Zc[r];
+                            const double a = 0.5 * (D[k + 1] + D[k]) - v.spar;
+                            const double b = 0.5 * (Zc[r + 1] + Zc[r]);
+                            const double cosw = fabs(v.sperp) / sqrt(a * a + b * b + v.sperp * v.sperp);
+                            sa = dperp / (dD * dZ * cosw);
+                        }
+                    }
+                    for (int bt = 0; bt < nbatch; ++bt) {
+                        const long long vi = ((long long)(bt * g.D + iz) * g.H + iy) * g.W + ix;
+                        const long long ci = (((long long)bt * nview + view) * g.Nv + r) * g.Nu + col;
+                        switch (op) {
+                        case OP_A:   out[ci] += coef * sa * in[vi]; break;
+                        case OP_AT:  out[vi] += coef * sa * in[ci]; break;
+                        case OP_B:
+                        case OP_BW:  out[vi] += coef * tvox * in[ci]; break;
+                        default:     out[ci] += coef * tvox * in[vi]; break;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    free(D); free(M); free(zd); free(X); free(Zv); free(Zc);
+    free(xa); free(xb); free(xl); free(za); free(zb); free(zl);
+    return 0;
+}
+
+/* ---------------------------------------------------------------- 2D ---- */
+
+/* 2D geometry values are the packed ones of the reference options tensor
+ * (projector.py:97-110): du and shu are already "effective" (flat: scaled to
+ * the isocentre; arc: angular). */
+int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
+            const double* in, double* out, const float* ang, int nbatch, int nview)
+{
+    const int W = ni[0], H = ni[1], Nu = ni[2];
+    const double dx = fv[0], dy = fv[1], shx = fv[2], shy = fv[3];
+    const double du = fg[0], shu = fg[1], sod = fg[2];
+    if (op < 0 || op > 5) return 1;
+    const int out_is_sino = (op == OP_A || op == OP_BT || op == OP_BWT);
+    memset(out, 0, sizeof(double) * (size_t)nbatch *
+           (size_t)(out_is_sino ? (long long)Nu * nview : (long long)W * H));
+    const int nline_max = W > H ? W : H;
+    double* D = malloc(sizeof(double) * (Nu + 1));
+    double* X = malloc(sizeof(double) * (nline_max + 1));
+    const int nxo = nline_max + Nu + 2;
+    int* xa = malloc(sizeof(int) * nxo); int* xb = malloc(sizeof(int) * nxo);
+    double* xl = malloc(sizeof(double) * nxo);
+    /* B column width: backward2d.cpp:87 (flat du), :109 (arc 2 SOD tan(du/2)),
+     * :185 (parallel du / pixel). */
+    const double cw = (type == GEO_ARC) ? 2.0 * sod * tan(0.5 * du) : du;
+
+    for (int view = 0; view < nview; ++view) {
+        const view_t v = make_view(ang[view], sod);
+        for (int k = 0; k <= Nu; ++k) {
+            const double sg = sigma(&v, k, Nu);
+            if (type == GEO_FLAT) {
+                /* system_matrix2d.cpp:185-189 */
+                const double u = sg * du + shu;
+                D[k] = map_point(&v, u * v.c, u * v.s);
+            } else if (type == GEO_ARC) {
+                /* system_matrix2d.cpp:280-283 */
+                D[k] = map_angle(&v, sg * du + shu + v.beta);
+            } else {
+                /* system_matrix2d.cpp:104-107 */
+                const double u = sg * du + shu;
+                D[k] = v.use_x ? u / v.c : u / v.s;
+            }
+        }
+        const double dperp = v.use_x ? dy : dx;
+        const int nlines = v.use_x ? H : W;
+        for (int line = 0; line < nlines; ++line) {
+            int npix;
+            if (v.use_x) {
+                const double py = (0.5 * H - line - 0.5) * dy + shy;
+                const double x0 = -0.5 * W * dx + shx;
+                for (int i = 0; i <= W; ++i)
+                    X[i] = (type == GEO_PARALLEL) ? (v.s / v.c) * py + x0 + i * dx
+                                                   : map_point(&v, x0 + i * dx, py);
+                npix = W;
+            } else {
+                const double px = (line - 0.5 * W + 0.5) * dx + shx;
+                const double y0 = -0.5 * H * dy + shy;
+                for (int i = 0; i <= H; ++i)
+                    X[i] = (type == GEO_PARALLEL) ? (v.c / v.s) * px + y0 + i * dy
+                                                   : map_point(&v, px, y0 + i * dy);
+                npix = H;
+            }
+            const int nx = overlaps(X, npix, D, Nu, xa, xb, xl);
+            for (int e = 0; e < nx; ++e) {
+                const int p = xa[e], k = xb[e];
+                const int ix = v.use_x ? p : line;
+                const int iy = v.use_x ? line : H - 1 - p;
+                const int col = v.keep ? k : Nu - 1 - k;
+                double scale;
+                if (op == OP_A || op == OP_AT) {
+                    if (type == GEO_PARALLEL) {
+                        scale = dperp / du;            /* system_matrix2d.cpp:109 */
+                    } else {
+                        /* system_matrix2d.cpp:213, :251 (cos_weight_x/y) */
+                        const double a = 0.5 * (D[k + 1] + D[k]) - v.spar;
+                        const double cosw = fabs(v.sperp) / sqrt(a * a + v.sperp * v.sperp);
+                        scale = dperp / ((D[k + 1] - D[k]) * cosw);
+                    }
+                } else {
+                    scale = cw / (X[p + 1] - X[p]);
+                    if ((op == OP_BW || op == OP_BWT) && type != GEO_PARALLEL) {
+                        const double px = (ix - 0.5 * W + 0.5) * dx + shx;
+                        const double py = (0.5 * H - iy - 0.5) * dy + shy;
+                        scale *= fbp_weight(type, &v, sod, px, py);
+                    }
+                }
+                const double coef = xl[e] * scale;
+                for (int bt = 0; bt < nbatch; ++bt) {
+                    const long long vi = ((long long)bt * H + iy) * W + ix;
+                    const long long ci = ((long long)bt * nview + view) * Nu + col;
+                    if (op == OP_A || op == OP_BT || op == OP_BWT) out[ci] += coef * in[vi];
+                    else out[vi] += coef * in[ci];
+                }
+            }
+        }
+    }
+    free(D); free(X); free(xa); free(xb); free(xl);
+    return 0;
+}

@@ -1,0 +1,184 @@
+"""FP64 CPU oracle for the distance-driven projector path.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import this module; the product package never
+does.
+
+* :func:`dd2d` / :func:`dd3d` run the C restatement ``dd_oracle.c`` in double
+  precision.  They take the reference's packed ``options`` vector (12 entries
+  in 2D, 18 in 3D) and unpack it exactly as the reference binding does
+  (XRecon ``src/api/torch_binding.cpp:62-124``), so both sides see identical
+  float32 parameter values.
+* :func:`filtered_backprojection2d` / :func:`filtered_backprojection3d`
+  restate the reference's FBP / FDK pipelines (``xrecon/projector/
+  projector.py:176-313`` and ``projector3d.py:165-287``) in numpy float64,
+  with the filter correlation evaluated directly.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from pathlib import Path
+
+import numpy as np
+
+from . import build_oracle
+
+OPS = {"A": 0, "AT": 1, "B": 2, "BT": 3, "BW": 4, "BWT": 5}
+SINO_OUT = {"A", "BT", "BWT"}
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        so = build_oracle.ORACLE_SO
+        if not so.exists():
+            build_oracle.build_oracle()
+        lib = ctypes.CDLL(str(so))
+        for name in ("xo_dd2d", "xo_dd3d"):
+            fn = getattr(lib, name)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int]
+        _lib = lib
+    return _lib
+
+
+def _p(a, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def unpack2d(options):
+    """Same field order as torch_binding.cpp:62-79."""
+    o = np.asarray(options, dtype=np.float32)
+    return dict(W=int(o[0]), H=int(o[1]), Nu=int(o[2]), dx=o[3], dy=o[4], du=o[5],
+                SOD=o[6], SDD=o[7], shx=o[8], shy=o[9], shu=o[10], type=int(o[11]))
+
+
+def unpack3d(options):
+    """Same field order as torch_binding.cpp:82-124 (helical fields ignored)."""
+    o = np.asarray(options, dtype=np.float32)
+    return dict(W=int(o[0]), H=int(o[1]), D=int(o[2]), Nu=int(o[3]), Nv=int(o[4]),
+                dx=o[5], dy=o[6], dz=o[7], du=o[8], dv=o[9], SOD=o[10], SDD=o[11],
+                shx=o[12], shy=o[13], shz=o[14], shu=o[15], shv=o[16], type=int(o[17]))
+
+
+def dd2d(op: str, x, options, angles):
+    """Apply a 2D operator.  x: [B, C, H, W] (image in) or [B, C, V, Nu]
+    (sinogram in); returns float64 ndarray of the output shape."""
+    g = unpack2d(options)
+    ang = np.ascontiguousarray(angles, dtype=np.float32)
+    V = ang.shape[0]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    B, C = x.shape[:2]
+    out_shape = (B, C, V, g["Nu"]) if op in SINO_OUT else (B, C, g["H"], g["W"])
+    out = np.zeros(out_shape, dtype=np.float64)
+    ni = np.array([g["W"], g["H"], g["Nu"]], dtype=np.int32)
+    fv = np.array([g["dx"], g["dy"], g["shx"], g["shy"]], dtype=np.float64)
+    fg = np.array([g["du"], g["shu"], g["SOD"], g["SDD"]], dtype=np.float64)
+    rc = _load().xo_dd2d(OPS[op], _p(ni, ctypes.c_int), _p(fv, ctypes.c_double), _p(fg, ctypes.c_double),
+                         g["type"], _p(x, ctypes.c_double), _p(out, ctypes.c_double),
+                         _p(ang, ctypes.c_float), B * C, V)
+    if rc != 0:
+        raise RuntimeError(f"oracle dd2d failed with status {rc}")
+    return out
+
+
+def dd3d(op: str, x, options, angles):
+    """Apply a 3D operator.  x: [B, C, D, H, W] or [B, C, V, Nv, Nu]."""
+    g = unpack3d(options)
+    ang = np.ascontiguousarray(angles, dtype=np.float32)
+    V = ang.shape[0]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    B, C = x.shape[:2]
+    out_shape = (B, C, V, g["Nv"], g["Nu"]) if op in SINO_OUT else (B, C, g["D"], g["H"], g["W"])
+    out = np.zeros(out_shape, dtype=np.float64)
+    ni = np.array([g["W"], g["H"], g["D"], g["Nu"], g["Nv"]], dtype=np.int32)
+    fv = np.array([g["dx"], g["dy"], g["dz"], g["shx"], g["shy"], g["shz"]], dtype=np.float64)
+    fg = np.array([g["du"], g["dv"], g["shu"], g["shv"], g["SOD"], g["SDD"]], dtype=np.float64)
+    rc = _load().xo_dd3d(OPS[op], _p(ni, ctypes.c_int), _p(fv, ctypes.c_double), _p(fg, ctypes.c_double),
+                         g["type"], _p(x, ctypes.c_double), _p(out, ctypes.c_double),
+                         _p(ang, ctypes.c_float), B * C, V)
+    if rc != 0:
+        raise RuntimeError(f"oracle dd3d failed with status {rc}")
+    return out
+
+
+# ---------------------------------------------------------------- FBP / FDK
+
+def ramp_filter(num_det: int, det_size: float) -> np.ndarray:
+    """Spatial Ram-Lak kernel of length 2*Nu-1 (filters.py:19-32)."""
+    x = np.arange(2 * num_det - 1) - num_det + 1
+    f = np.zeros(2 * num_det - 1, dtype=np.float64)
+    odd = (x % 2) != 0
+    f[odd] = -1.0 / (math.pi ** 2 * det_size ** 2 * (x[odd].astype(np.float64) ** 2 + 1e-12))
+    f[num_det - 1] = 1.0 / (4.0 * det_size ** 2)
+    return f
+
+
+def correlate_rows(sino: np.ndarray, filt: np.ndarray) -> np.ndarray:
+    """out[..., i] = sum_j sino[..., j] * filt[j - i + Nu - 1]: the reference's
+    conv2d/conv3d with padding Nu-1 along u (projector.py:201,
+    projector3d.py:190; torch conv is cross-correlation)."""
+    nu = sino.shape[-1]
+    f = np.asarray(filt, dtype=np.float64).reshape(-1)
+    assert f.shape[0] == 2 * nu - 1
+    # T[j, i] = f[j - i + nu - 1]
+    j = np.arange(nu)[:, None]
+    i = np.arange(nu)[None, :]
+    T = f[j - i + nu - 1]
+    return np.asarray(sino, dtype=np.float64) @ T
+
+
+def mean_angle_step(angles) -> float:
+    """projector.py:303-313."""
+    a = np.asarray(angles, dtype=np.float64)
+    if a.size < 2:
+        return 0.0
+    d = np.diff(a)
+    wrap = np.mod(d + math.pi, 2 * math.pi) - math.pi
+    return float(np.abs(wrap).mean())
+
+
+def cosine_weight(scan: str, nu: int, du_eff: float, shu_eff: float, sod: float) -> np.ndarray:
+    """projector.py:255-277 / projector3d.py:233-246 (3D: in-plane only)."""
+    u = np.arange(-nu / 2 + 0.5, nu / 2, 1.0, dtype=np.float64)
+    s = u * du_eff + shu_eff
+    if scan == "flat":
+        return sod / np.sqrt(s * s + sod * sod)
+    if scan == "arc":
+        return np.cos(s)
+    return np.ones_like(s)
+
+
+def filtered_backprojection2d(sino, options, angles, weight, filt, redundant=True, parker=None):
+    """Restates Projector2d.filtered_backprojection (projector.py:176-206)."""
+    s = np.asarray(sino, dtype=np.float64)
+    if parker is not None:
+        s = s * np.asarray(parker, dtype=np.float64)
+    s = s * np.asarray(weight, dtype=np.float64).reshape(-1)
+    f = correlate_rows(s, filt)
+    recon = dd2d("BW", f, options, angles) * mean_angle_step(angles)
+    return recon / 2 if redundant else recon
+
+
+def filtered_backprojection3d(sino, options, angles, weight, filt, redundant=True, parker=None):
+    """Restates Projector3d.filtered_backprojection (projector3d.py:165-195)."""
+    s = np.asarray(sino, dtype=np.float64)
+    if parker is not None:
+        s = s * np.asarray(parker, dtype=np.float64)
+    s = s * np.asarray(weight, dtype=np.float64).reshape(-1)
+    f = correlate_rows(s, filt)
+    recon = dd3d("BW", f, options, angles) * mean_angle_step(angles)
+    return recon / 2 if redundant else recon
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = np.linalg.norm(b.ravel())
+    return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))

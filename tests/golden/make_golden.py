@@ -1,0 +1,157 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+Run in a container where the XRecon reference tree is importable (default
+/root/reference, override with XRECON_REFERENCE_ROOT):
+
+    python tests/golden/make_golden.py
+
+The reference's own Python package (xrecon/projector/*.py, pure Python) is
+imported from the reference tree with its native module ``xrecon_C`` served
+by the reference's own C++ CPU kernels (src/cpu/*.cpp compiled by
+oracle/build_oracle.py into oracle/_ref/).  So every number stored here comes
+from the reference's code path on CPU:
+
+* dd2d_<geom>.npz / dd3d_<geom>.npz: seeded inputs and the outputs of the six
+  operators (forward_projection, projection_transpose, backward_projection,
+  weighted_backward_projection and the two backprojection transposes);
+* fbp2d_<case>.npz / fdk3d_<case>.npz: Projector.filtered_backprojection
+  results (TF32 is irrelevant: this is the CPU conv path);
+* options.npz: the packed options vectors of Projector2d/3d for the benchmark
+  geometries; filters.npz: the filter tables.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+REF_ROOT = Path(os.environ.get("XRECON_REFERENCE_ROOT", "/root/reference"))
+sys.path.insert(0, str(ROOT))
+
+from oracle import refcpu  # noqa: E402
+
+
+def import_reference():
+    """Import the reference package with xrecon_C served by its CPU kernels."""
+    sys.modules["xrecon_C"] = refcpu.RefXreconC()
+    sys.path.insert(0, str(REF_ROOT))
+    import xrecon.projector.filters as rfilters  # noqa: F401
+    from xrecon.projector.projector import Projector2d
+    from xrecon.projector.projector3d import Projector3d
+    import xrecon.projector.geometry as rgeom
+    return Projector2d, Projector3d, rgeom, rfilters
+
+
+OPS2D = {"A": "projection", "AT": "projection_t", "B": "backprojection", "BW": "backprojection_weighted",
+         "BT": "backprojection_t", "BWT": "backprojection_weighted_t"}
+
+
+def angles_set(V: int, offset: float = 0.1) -> np.ndarray:
+    a = (np.arange(V) * (2 * np.pi / V) + offset).astype(np.float32)
+    special = np.array([0.0, np.pi / 4, np.pi / 2, 3 * np.pi / 4, np.pi, 5 * np.pi / 4], np.float32)
+    return np.concatenate([a, special]).astype(np.float32)
+
+
+def main():
+    P2, P3, G, F = import_reference()
+    rng = np.random.default_rng(20261203)
+
+    # ---------------------------------------------------------------- 2D ops
+    for scan in ("parallel", "flat", "arc"):
+        if scan == "parallel":
+            geo = G.ParallelBeam2d(G.Detector2d(53, 1.7, 0.25))
+        else:
+            geo = G.FanBeam2d(G.Detector2d(53, 1.7, 0.25), 500.0, 1000.0, scan)
+        P = P2(G.Volume2d((37, 29), (1.0, 1.1), (0.3, -0.2)), geo)
+        ang = angles_set(18)
+        img = rng.random((2, 1, 29, 37)).astype(np.float32)
+        sino = rng.random((2, 1, ang.size, 53)).astype(np.float32)
+        at = torch.from_numpy(ang)
+        out = {"options": P.options.numpy(), "angles": ang, "image": img, "sino": sino}
+        for op, meth in OPS2D.items():
+            x = img if op in ("A", "BT", "BWT") else sino
+            out[op] = getattr(P, meth)(torch.from_numpy(x), at).numpy()
+        np.savez_compressed(HERE / f"dd2d_{scan}.npz", **out)
+
+    # ---------------------------------------------------------------- 3D ops
+    for scan in ("parallel", "flat", "arc"):
+        det = G.Detector3d((41, 13), (1.5, 1.3), (0.25, -0.5))
+        geo = G.ParallelBeam3d(det) if scan == "parallel" else G.ConeBeam3d(det, 500.0, 1000.0, scan)
+        P = P3(G.Volume3d((23, 19, 11), (1.0, 1.1, 0.9), (0.2, -0.3, 0.5)), geo)
+        ang = angles_set(10)
+        img = rng.random((1, 1, 11, 19, 23)).astype(np.float32)
+        sino = rng.random((1, 1, ang.size, 13, 41)).astype(np.float32)
+        at = torch.from_numpy(ang)
+        out = {"options": P.options.numpy(), "angles": ang, "image": img, "sino": sino}
+        for op, meth in OPS2D.items():
+            x = img if op in ("A", "BT", "BWT") else sino
+            out[op] = getattr(P, meth)(torch.from_numpy(x), at).numpy()
+        np.savez_compressed(HERE / f"dd3d_{scan}.npz", **out)
+
+    # ------------------------------------------------------------- FBP / FDK
+    from xrecon.utils.phantom import phantom as rphantom  # pure numpy
+    img = torch.from_numpy(rphantom(64, dim=2)).float()[None, None]
+    cases2d = [("flat_ramp", "flat", "ramp", 90, 2 * np.pi, False),
+               ("arc_ramp", "arc", "ramp", 90, 2 * np.pi, False),
+               ("parallel_shepplogan", "parallel", "shepplogan", 60, np.pi, False),
+               ("flat_hann", "flat", "hann", 90, 2 * np.pi, False),
+               ("flat_parker", "flat", "ramp", 80, np.pi + 0.6, True)]
+    for name, scan, filt, V, rng_ang, parker in cases2d:
+        if scan == "parallel":
+            geo = G.ParallelBeam2d(G.Detector2d(96, 1.0))
+        else:
+            geo = G.FanBeam2d(G.Detector2d(96, 2.0), 500.0, 1000.0, scan)
+        P = P2(G.Volume2d(64, 1.0), geo, filter_type=filt)
+        ang = torch.from_numpy((np.arange(V) * (rng_ang / V)).astype(np.float32))
+        sino = P.projection(img, ang)
+        recon = P.filtered_backprojection(sino, ang, parker=parker)
+        np.savez_compressed(HERE / f"fbp2d_{name}.npz", options=P.options.numpy(), angles=ang.numpy(),
+                            sino=sino.numpy(), weight=P.weight.numpy(), filter=P.filter.numpy(),
+                            parker=P.parker_weight(ang).numpy() if parker else np.zeros(0, np.float32),
+                            recon=recon.numpy())
+
+    vol = torch.from_numpy(np.ascontiguousarray(
+        np.transpose(rphantom((32, 32, 8), dim=3), (2, 0, 1)))).float()[None, None]
+    for name, scan in (("flat", "flat"), ("arc", "arc")):
+        geo = G.ConeBeam3d(G.Detector3d((48, 12), (1.5, 1.5)), 500.0, 1000.0, scan)
+        P = P3(G.Volume3d((32, 32, 8), 1.0), geo)
+        ang = torch.from_numpy((np.arange(60) * (2 * np.pi / 60)).astype(np.float32))
+        sino = P.projection(vol, ang)
+        recon = P.filtered_backprojection(sino, ang)
+        np.savez_compressed(HERE / f"fdk3d_{name}.npz", options=P.options.numpy(), angles=ang.numpy(),
+                            sino=sino.numpy(), weight=P.weight.numpy(), filter=P.filter.numpy(),
+                            recon=recon.numpy())
+
+    # ------------------------------------------------- packing + filter tables
+    opts = {}
+    opts["c1_2d_flat"] = P2(G.Volume2d(256, 1.0), G.FanBeam2d(G.Detector2d(256, 2.0), 500., 1000., "flat")).options.numpy()
+    opts["c2_3d_flat"] = P3(G.Volume3d((256, 256, 64), 1.0),
+                            G.ConeBeam3d(G.Detector3d((384, 96), 1.5), 500., 1000., "flat")).options.numpy()
+    opts["c3_3d_arc"] = P3(G.Volume3d((128, 128, 32), 1.0),
+                           G.ConeBeam3d(G.Detector3d((256, 64), 1.5), 500., 1000., "arc")).options.numpy()
+    opts["c4_2d_arc"] = P2(G.Volume2d(384, 512 / 384), G.FanBeam2d(G.Detector2d(500, 1.3, 0.5), 450., 900., "arc")).options.numpy()
+    opts["c5_3d_flat"] = P3(G.Volume3d((512, 512, 256), 0.75),
+                            G.ConeBeam3d(G.Detector3d((1024, 256), 0.8), 595., 1085., "flat")).options.numpy()
+    opts["x_3d_parallel"] = P3(G.Volume3d((40, 30, 20), (1.0, 1.2, 0.8), (0.5, -1, 2)),
+                               G.ParallelBeam3d(G.Detector3d((64, 24), (1.1, 0.9), (0.3, -0.7)))).options.numpy()
+    opts["x_2d_parallel"] = P2(G.Volume2d((40, 30), (1.0, 1.2), (0.5, -1)),
+                               G.ParallelBeam2d(G.Detector2d(64, 1.1, 0.3))).options.numpy()
+    opts["x_3d_arc_shift"] = P3(G.Volume3d((40, 30, 20), (1.0, 1.2, 0.8), (0.5, -1, 2)),
+                                G.ConeBeam3d(G.Detector3d((64, 24), (1.1, 0.9), (0.3, -0.7)), 600., 1100., "arc")).options.numpy()
+    np.savez_compressed(HERE / "options.npz", **opts)
+
+    filt = {}
+    for name in ("ramp", "shepplogan", "cosine", "hamming", "hann"):
+        filt[name] = F.filter_generate(96, 0.75, name, torch.float32).numpy()
+    np.savez_compressed(HERE / "filters.npz", **filt)
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,146 @@
+"""Parity of the CUDA operators (through the C ABI) with the FP64 oracle and
+with the reference's own outputs.
+
+Tolerances (relative L2):
+* against the FP64 oracle: 1e-5 (the north-star bar for FP32);
+* against the reference fixtures: the oracle's own distance from the
+  reference plus 1e-5 (the reference's float32 geometry sits 1e-6..1e-4 away
+  from the exact operator, see test_oracle_pin.py);
+* adjoint pairs <Ax, y> = <x, A^T y>: 1e-5;
+* BF16/FP16 storage with FP32 accumulation: 1e-3 against the oracle applied
+  to the same (rounded) input; outputs stored in BF16 add their own rounding
+  (2^-9 relative RMS), bounded at 3e-3.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden, rel_l2
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+OPS = ("A", "AT", "B", "BT", "BW", "BWT")
+IMG_IN = ("A", "BT", "BWT")
+
+
+def run(dim, op, x, options, angles, dev, dtype=torch.float32, out_dtype=None):
+    from xrecon_b200 import _native
+    from xrecon_b200.backend import HostGeometry
+    g = HostGeometry(dim, np.asarray(options).tolist()).struct
+    xt = torch.as_tensor(np.ascontiguousarray(x)).to(device=dev, dtype=dtype)
+    at = torch.as_tensor(np.asarray(angles, np.float32)).to(dev)
+    y = _native.apply(dim, op, xt, g, at, out_dtype=out_dtype)
+    torch.cuda.synchronize()
+    return y.float().cpu().numpy()
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_ops_match_oracle_and_reference(cuda, dim, scan):
+    g = load_golden(f"dd{dim}d_{scan}")
+    ofn = O.dd2d if dim == 2 else O.dd3d
+    for op in OPS:
+        x = g["image"] if op in IMG_IN else g["sino"]
+        got = run(dim, op, x, g["options"], g["angles"], cuda)
+        exact = ofn(op, x, g["options"], g["angles"])
+        e_oracle = rel_l2(got, exact)
+        assert e_oracle < 1e-5, f"{dim}D {scan} {op}: vs oracle {e_oracle:.2e}"
+        e_ref = rel_l2(got, g[op])
+        bound = rel_l2(exact, g[op]) + 1e-5
+        assert e_ref < bound, f"{dim}D {scan} {op}: vs reference {e_ref:.2e} (bound {bound:.2e})"
+
+
+def _opts3d(W, H, D, Nu, Nv, dx, dy, dz, du, dv, sod, sdd, sh, shu, shv, scan):
+    from xrecon_b200 import geometry as G
+    det = G.Detector3d((Nu, Nv), (du, dv), (shu, shv))
+    geo = G.ParallelBeam3d(det) if scan == "parallel" else G.ConeBeam3d(det, sod, sdd, scan)
+    return np.array(G.pack_options3d(G.Volume3d((W, H, D), (dx, dy, dz), sh), geo), np.float32)
+
+
+def _opts2d(W, H, Nu, dx, dy, du, sod, sdd, sh, shu, scan):
+    from xrecon_b200 import geometry as G
+    det = G.Detector2d(Nu, du, shu)
+    geo = G.ParallelBeam2d(det) if scan == "parallel" else G.FanBeam2d(det, sod, sdd, scan)
+    return np.array(G.pack_options2d(G.Volume2d((W, H), (dx, dy), sh), geo), np.float32)
+
+
+@pytest.mark.parametrize("scan", ["flat", "arc", "parallel"])
+def test_config2_shapes_against_oracle(cuda, scan):
+    """256x256x64 volume, 384x96 detector (config 2 geometry) on a subset of
+    views including the 45-degree axis switches, random (worst-case) data."""
+    opts = _opts3d(256, 256, 64, 384, 96, 1.0, 1.0, 1.0, 1.5, 1.5, 500., 1000., 0.0, 0.0, 0.0, scan)
+    ang = (np.array([3, 90, 180, 270, 500, 719]) * (2 * np.pi / 720)).astype(np.float32)
+    rng = np.random.default_rng(2)
+    img = rng.random((1, 1, 64, 256, 256)).astype(np.float32)
+    sino = rng.random((1, 1, ang.size, 96, 384)).astype(np.float32)
+    for op in ("A", "B", "AT", "BWT"):
+        x = img if op in IMG_IN else sino
+        got = run(3, op, x, opts, ang, cuda)
+        exact = O.dd3d(op, x, opts, ang)
+        assert rel_l2(got, exact) < 1e-5, (scan, op)
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_adjoint_dot_products(cuda, dim, scan):
+    if dim == 3:
+        opts = _opts3d(33, 29, 17, 45, 21, 1.0, 0.9, 1.1, 1.3, 1.2, 400., 800., (0.4, -0.3, 0.2), 0.3, -0.2, scan)
+    else:
+        opts = _opts2d(61, 47, 77, 0.9, 1.1, 1.3, 400., 800., (0.4, -0.3), 0.3, scan)
+    ang = (np.arange(40) * (2 * np.pi / 40) + 0.05).astype(np.float32)
+    rng = np.random.default_rng(3)
+    if dim == 3:
+        x = rng.standard_normal((1, 1, 17, 29, 33)).astype(np.float32)
+        y = rng.standard_normal((1, 1, 40, 21, 45)).astype(np.float32)
+    else:
+        x = rng.standard_normal((1, 1, 47, 61)).astype(np.float32)
+        y = rng.standard_normal((1, 1, 40, 77)).astype(np.float32)
+    for fwd, adj in (("A", "AT"), ("BT", "B"), ("BWT", "BW")):
+        lhs = float(np.sum(run(dim, fwd, x, opts, ang, cuda).astype(np.float64) * y))
+        rhs = float(np.sum(x.astype(np.float64) * run(dim, adj, y, opts, ang, cuda)))
+        assert abs(lhs - rhs) <= 1e-5 * (abs(lhs) + abs(rhs)) / 2, (fwd, adj, lhs, rhs)
+
+
+def test_deterministic_and_batched(cuda):
+    g = load_golden("dd3d_flat")
+    rng = np.random.default_rng(4)
+    img = rng.random((2, 3) + g["image"].shape[2:]).astype(np.float32)
+    sino = rng.random((2, 3) + g["sino"].shape[2:]).astype(np.float32)
+    for op in OPS:
+        x = img if op in IMG_IN else sino
+        a = run(3, op, x, g["options"], g["angles"], cuda)
+        b = run(3, op, x, g["options"], g["angles"], cuda)
+        assert np.array_equal(a, b), f"{op} not bitwise reproducible"
+        one = run(3, op, x[1:2, 2:3], g["options"], g["angles"], cuda)
+        assert np.array_equal(a[1:2, 2:3], one), f"{op}: batch element differs from single call"
+
+
+@pytest.mark.parametrize("dtype", [torch.bfloat16, torch.float16])
+def test_half_storage_forms(cuda, dtype):
+    g = load_golden("dd3d_flat")
+    for op in OPS:
+        x = g["image"] if op in IMG_IN else g["sino"]
+        xq = torch.as_tensor(x).to(dtype).float().numpy()  # what the kernel sees
+        exact = O.dd3d(op, xq, g["options"], g["angles"])
+        got32 = run(3, op, x, g["options"], g["angles"], cuda, dtype=dtype, out_dtype=torch.float32)
+        assert rel_l2(got32, exact) < 1e-5, (dtype, op, "fp32 accumulation")
+        goth = run(3, op, x, g["options"], g["angles"], cuda, dtype=dtype)
+        bound = 3e-3 if dtype == torch.bfloat16 else 1e-3
+        assert rel_l2(goth, exact) < bound, (dtype, op, "half output")
+
+
+def test_edges_odd_shapes_and_empty(cuda):
+    # detector narrower than the volume, strong shifts, Nu not a multiple of 32
+    opts = _opts3d(20, 37, 9, 7, 5, 1.0, 1.0, 1.0, 2.5, 2.5, 300., 700., (3.0, -2.0, 1.5), 1.5, -1.0, "flat")
+    ang = np.array([0.0, 0.3, 1.2, 2.5, 3.9, 5.5], np.float32)
+    rng = np.random.default_rng(5)
+    img = rng.random((1, 1, 9, 37, 20)).astype(np.float32)
+    sino = rng.random((1, 1, 6, 5, 7)).astype(np.float32)
+    for op in OPS:
+        x = img if op in IMG_IN else sino
+        assert rel_l2(run(3, op, x, opts, ang, cuda), O.dd3d(op, x, opts, ang)) < 1e-5, op
+    # zero views: volume outputs are zero, sinogram outputs empty
+    empty = np.zeros(0, np.float32)
+    assert np.all(run(3, "B", np.zeros((1, 1, 0, 5, 7), np.float32), opts, empty, cuda) == 0)
+    assert run(3, "A", img, opts, empty, cuda).shape == (1, 1, 0, 5, 7)

@@ -1,0 +1,133 @@
+"""Host-side logic and the C ABI surface (CPU only, no kernel launches)."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import ROOT, load_golden
+from xrecon_b200 import _native, filters, geometry as G
+from xrecon_b200.projector import Projector2d, Projector3d, mean_angle_step, parker_weights
+
+
+def _ref_geoms():
+    return {
+        "c1_2d_flat": (G.Volume2d(256, 1.0), G.FanBeam2d(G.Detector2d(256, 2.0), 500., 1000., "flat")),
+        "c2_3d_flat": (G.Volume3d((256, 256, 64), 1.0), G.ConeBeam3d(G.Detector3d((384, 96), 1.5), 500., 1000., "flat")),
+        "c3_3d_arc": (G.Volume3d((128, 128, 32), 1.0), G.ConeBeam3d(G.Detector3d((256, 64), 1.5), 500., 1000., "arc")),
+        "c4_2d_arc": (G.Volume2d(384, 512 / 384), G.FanBeam2d(G.Detector2d(500, 1.3, 0.5), 450., 900., "arc")),
+        "c5_3d_flat": (G.Volume3d((512, 512, 256), 0.75),
+                       G.ConeBeam3d(G.Detector3d((1024, 256), 0.8), 595., 1085., "flat")),
+        "x_3d_parallel": (G.Volume3d((40, 30, 20), (1.0, 1.2, 0.8), (0.5, -1, 2)),
+                          G.ParallelBeam3d(G.Detector3d((64, 24), (1.1, 0.9), (0.3, -0.7)))),
+        "x_2d_parallel": (G.Volume2d((40, 30), (1.0, 1.2), (0.5, -1)), G.ParallelBeam2d(G.Detector2d(64, 1.1, 0.3))),
+        "x_3d_arc_shift": (G.Volume3d((40, 30, 20), (1.0, 1.2, 0.8), (0.5, -1, 2)),
+                           G.ConeBeam3d(G.Detector3d((64, 24), (1.1, 0.9), (0.3, -0.7)), 600., 1100., "arc")),
+    }
+
+
+def test_packed_options_equal_reference():
+    ref = load_golden("options")
+    for name, (vol, geo) in _ref_geoms().items():
+        P = (Projector2d if isinstance(vol, G.Volume2d) else Projector3d)(vol, geo)
+        np.testing.assert_array_equal(P.options.numpy(), ref[name], err_msg=name)
+
+
+def test_filter_tables_match_reference():
+    ref = load_golden("filters")
+    for name in ("ramp", "shepplogan", "cosine", "hamming", "hann"):
+        got = filters.filter_generate(96, 0.75, name, torch.float32).numpy()
+        np.testing.assert_allclose(got, ref[name], rtol=2e-6, atol=1e-7 * np.abs(ref[name]).max(), err_msg=name)
+
+
+def test_fbp_host_tables_match_reference():
+    for case in ("flat_ramp", "arc_ramp", "parallel_shepplogan", "flat_hann"):
+        g = load_golden(f"fbp2d_{case}")
+        scan, filt = case.split("_")
+        det = G.Detector2d(96, 2.0 if scan != "parallel" else 1.0)
+        geo = G.ParallelBeam2d(det) if scan == "parallel" else G.FanBeam2d(det, 500.0, 1000.0, scan)
+        P = Projector2d(G.Volume2d(64, 1.0), geo, filter_type=filt)
+        np.testing.assert_array_equal(P.options.numpy(), g["options"])
+        np.testing.assert_allclose(P.weight.numpy(), g["weight"], rtol=1e-6)
+        np.testing.assert_allclose(P.filter.numpy(), g["filter"], rtol=2e-6, atol=1e-7 * np.abs(g["filter"]).max())
+    g = load_golden("fbp2d_flat_parker")
+    P = Projector2d(G.Volume2d(64, 1.0), G.FanBeam2d(G.Detector2d(96, 2.0), 500.0, 1000.0, "flat"))
+    ang = torch.from_numpy(g["angles"])
+    np.testing.assert_allclose(P.parker_weight(ang).numpy(), g["parker"], rtol=1e-6, atol=1e-7)
+
+
+def test_mean_angle_step_wraps():
+    a = torch.tensor([6.0, 6.2, 0.1, 0.3], dtype=torch.float64)
+    step = mean_angle_step(a).item()
+    assert abs(step - np.mean([0.2, 0.1 + 2 * np.pi - 6.2, 0.2])) < 1e-12
+
+
+def test_parker_full_scan_is_ones():
+    ang = torch.linspace(0, 2 * np.pi, 361, dtype=torch.float32)  # closed 2*pi scan
+    w = parker_weights(ang, torch.linspace(-0.2, 0.2, 16), 16)
+    assert torch.all(w == 1)
+    with pytest.raises(ValueError):
+        parker_weights(ang[:100], torch.linspace(-0.2, 0.2, 16), 16)
+
+
+def _header_functions():
+    text = (ROOT / "include" / "xrecon_b200.h").read_text()
+    body = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(xr_[a-z0-9_]+)\s*\(", body)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _native.lib()
+    names = _header_functions()
+    assert "xr_dd3d" in names and "xr_dd2d" in names
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in include/xrecon_b200.h but not exported"
+    assert _native.version().startswith("xrecon_b200")
+
+
+def test_workspace_sizes_and_validation_without_gpu():
+    lib = _native.lib()
+    vals = load_golden("options")["c5_3d_flat"]
+    g = _native.geom3d_from_values(vals)
+    nb_a = lib.xr_dd3d_workspace_size(0, ctypes.byref(g), 1, 1440)
+    nb_at = lib.xr_dd3d_workspace_size(1, ctypes.byref(g), 1, 1440)
+    # forward needs the flipped image copy, cone A^T the scaled sinogram
+    assert nb_a > 512 * 512 * 256 * 4
+    assert nb_at > 1440 * 256 * 1024 * 4
+    bad = _native.geom3d_from_values(vals)
+    bad.dx = -1.0
+    rc = lib.xr_dd3d(0, ctypes.byref(bad), None, 0, None, 0, None, 1, 1, None, 0, None)
+    assert rc == 1
+    assert b"spacings" in lib.xr_last_error()
+    near = _native.geom3d_from_values(vals)
+    near.sod = 100.0  # source inside the image
+    rc = lib.xr_dd3d(0, ctypes.byref(near), ctypes.c_void_p(1), 0, ctypes.c_void_p(1), 0, ctypes.c_void_p(1),
+                     1, 1, None, 0, None)
+    assert rc == 1 and b"iso_source" in lib.xr_last_error()
+    ok = _native.geom3d_from_values(vals)
+    rc = lib.xr_dd3d(0, ctypes.byref(ok), ctypes.c_void_p(256), 0, ctypes.c_void_p(256), 0, ctypes.c_void_p(256),
+                     1, 1, None, 0, None)
+    assert rc == 2 and b"workspace" in lib.xr_last_error()
+    rc = lib.xr_dd3d(9, ctypes.byref(ok), None, 0, None, 0, None, 1, 1, None, 0, None)
+    assert rc == 1
+
+
+def test_cpu_tensors_are_rejected():
+    P = Projector3d(G.Volume3d((8, 8, 4), 1.0), G.ConeBeam3d(G.Detector3d((12, 6), 1.5), 500., 1000., "flat"))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        P.projection(torch.zeros(1, 1, 4, 8, 8), torch.zeros(3))
+
+
+def test_backend_surface_matches_reference_names():
+    from xrecon_b200 import backend
+    names = ["forward_projection2d", "backward_projection2d", "weighted_backward_projection2d",
+             "projection_transpose2d", "backward_projection_transpose2d",
+             "weighted_backward_projection_transpose2d", "back_projection2d", "weighted_back_projection2d",
+             "forward_projection3d", "projection_transpose3d", "backward_projection3d",
+             "weighted_backward_projection3d", "backward_projection_transpose3d",
+             "weighted_backward_projection_transpose3d"]
+    for n in names:
+        assert callable(getattr(backend, n))
+    with pytest.raises(RuntimeError, match="at least 18"):
+        backend._geom(3, torch.zeros(10))

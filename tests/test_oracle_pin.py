@@ -1,0 +1,77 @@
+"""Pin the FP64 oracle against the reference's own outputs (CPU only).
+
+The golden fixtures hold outputs of the reference's CPU path (its Python
+package over its C++ CPU kernels, see tests/golden/make_golden.py).  The
+reference computes its geometry in float32; its distance from the exact
+operator is ~1e-6 (relative L2) for parallel and flat geometries at these
+sizes and up to ~1e-4 for the arc geometry, whose boundary angles
+(k - Nu/2)*du + shift_u + beta are rounded to float32 (a quantum of 4.8e-7 rad
+at |beta| ~ 2 pi, up to 3e-4 of a detector cell).  The tolerances below are
+those measured distances with margin.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_l2
+from oracle import oracle as O
+
+OPS = ("A", "AT", "B", "BT", "BW", "BWT")
+IMG_IN = ("A", "BT", "BWT")
+TOL = {"parallel": 1e-5, "flat": 1e-5, "arc": 3e-4}
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_matches_reference_outputs(dim, scan):
+    g = load_golden(f"dd{dim}d_{scan}")
+    fn = O.dd2d if dim == 2 else O.dd3d
+    for op in OPS:
+        x = g["image"] if op in IMG_IN else g["sino"]
+        got = fn(op, x, g["options"], g["angles"])
+        err = rel_l2(got, g[op])
+        assert err < TOL[scan], f"{dim}D {scan} {op}: rel L2 {err:.3e}"
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_adjoint_pairs(dim, scan):
+    """<Ax, y> = <x, A^T y> and the same for B and Bw, in FP64."""
+    g = load_golden(f"dd{dim}d_{scan}")
+    fn = O.dd2d if dim == 2 else O.dd3d
+    x, y = g["image"].astype(np.float64), g["sino"].astype(np.float64)
+    for fwd, adj in (("A", "AT"), ("BT", "B"), ("BWT", "BW")):
+        lhs = float(np.sum(fn(fwd, x, g["options"], g["angles"]) * y))
+        rhs = float(np.sum(x * fn(adj, y, g["options"], g["angles"])))
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs), (fwd, adj, lhs, rhs)
+
+
+@pytest.mark.parametrize("case", ["flat_ramp", "arc_ramp", "parallel_shepplogan", "flat_hann", "flat_parker"])
+def test_oracle_fbp_matches_reference(case):
+    g = load_golden(f"fbp2d_{case}")
+    redundant = case != "flat_parker"
+    parker = g["parker"].reshape(1, 1, g["angles"].size, -1) if g["parker"].size else None
+    got = O.filtered_backprojection2d(g["sino"], g["options"], g["angles"], g["weight"], g["filter"],
+                                      redundant=redundant, parker=parker)
+    tol = 3e-4 if case.startswith("arc") else 2e-5
+    assert rel_l2(got, g["recon"]) < tol
+
+
+@pytest.mark.parametrize("case", ["flat", "arc"])
+def test_oracle_fdk_matches_reference(case):
+    g = load_golden(f"fdk3d_{case}")
+    got = O.filtered_backprojection3d(g["sino"], g["options"], g["angles"], g["weight"], g["filter"])
+    tol = 3e-4 if case == "arc" else 2e-5
+    assert rel_l2(got, g["recon"]) < tol
+
+
+def test_oracle_reference_library_when_present():
+    """Where oracle/_ref was built, run a fresh seeded case through both."""
+    from oracle import refcpu
+    if not refcpu.available():
+        pytest.skip("reference CPU library not built")
+    g = load_golden("dd3d_flat")
+    rng = np.random.default_rng(7)
+    x = rng.random(g["image"].shape).astype(np.float32)
+    a = O.dd3d("A", x, g["options"], g["angles"])
+    b = refcpu.dd3d("A", x, g["options"], g["angles"])
+    assert rel_l2(b, a) < 1e-5

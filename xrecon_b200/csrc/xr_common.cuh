@@ -1,0 +1,219 @@
+// Shared device-side definitions of the B200 distance-driven projector.
+//
+// Geometry conventions follow the reference (XRecon include/types.h:35-119,
+// include/xrmath.h:8-226): voxel centres at (i - N/2 + 1/2) d + shift with
+// image row 0 at the top (+y), source at (-sin b, cos b) * SOD, detector
+// boundaries mapped onto a common axis (x when cos^2 b > 1/2, else y), z
+// mapped onto the axis plane by the magnification of the detector column
+// centre (cells) and of the voxel line centre (voxels).
+//
+// Every operator of the path is the overlap kernel K[cell, voxel] with a
+// diagonal scale on one side.  The kernels here evaluate K in normalised
+// units: pixel positions along the current image line (one unit = one pixel)
+// and voxel indices along z, in which
+//     K = ovl_pos * ovl_zvox * dpix * dz * Mv(L)^2      (cone)
+//     K = ovl_pos * ovl_zvox * dpix * dz                (3D parallel)
+// where Mv(L) is the magnification of line L onto the axis.  The per-view
+// geometry (boundary positions, column magnifications, cell scales) is set up
+// in FP64 by xr_setup_views3d / xr_setup_views2d; the inner loops run in FP32
+// on small local coordinates.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace xr {
+
+enum GeoType : int { GEO_PARALLEL = 0, GEO_FLAT = 1, GEO_ARC = 2 };
+enum OpKind : int { OP_A = 0, OP_AT = 1, OP_B = 2, OP_BT = 3, OP_BW = 4, OP_BWT = 5 };
+enum DType : int { DT_F32 = 0, DT_BF16 = 1, DT_F16 = 2 };
+
+// Packed geometry; values are the reference's float32 options promoted to
+// double (projector.py:106-110, projector3d.py:98-107).  2D uses Nz = Nv = 1.
+struct Geom {
+    int W, H, D, Nu, Nv, type;
+    double dx, dy, dz, shx, shy, shz;
+    double du, dv, shu, shv, sod, sdd;
+};
+
+// Per-view header (FP64 geometry, decisions taken like the reference CPU path).
+struct ViewHdr {
+    int use_x;      // common axis is x
+    int keep;       // detector traversed in index order
+    int nlines;     // H (use_x: lines are rows iy) or W (lines are columns ix)
+    int npix;       // W or H: pixels along a line
+    double beta, s, c;
+    double sx, sy;          // source
+    double spar, sperp;     // source coordinate along / across the axis
+    double perpA, perpB;    // perpendicular coordinate of line L = perpA + perpB * L
+    double q0, q1;          // 1 / Mv(L) = q0 + q1 * L   (1 for parallel)
+    double dpix;            // pixel size along the line (dx or dy)
+};
+
+// Per-view tables, structure of arrays, view-major.
+//   pos_k(L) = bA[k] + bB[k] * L : position of detector boundary k (traversal
+//              order) on line L in pixel units, k = 0..Nu
+//   colQ[k]  = M_k / dz (3D) ; colE, colF, colM: cell scale of A,
+//              s_A(k, r) = colE[k] * sqrt(colF[k] + (colM[k] * zc_r)^2)
+struct ViewTables {
+    ViewHdr* hdr;
+    double* bA;
+    double* bB;
+    double* colQ;
+    float* colE;
+    float* colF;
+    float* colM;
+};
+
+// ---------------------------------------------------------------- dtype io
+
+template <typename T> __device__ __forceinline__ float ld(const T* p);
+template <> __device__ __forceinline__ float ld<float>(const float* p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(__ldg(p));
+}
+template <> __device__ __forceinline__ float ld<__half>(const __half* p) { return __half2float(__ldg(p)); }
+
+template <typename T> __device__ __forceinline__ void st(T* p, float v);
+template <> __device__ __forceinline__ void st<float>(float* p, float v) { *p = v; }
+template <> __device__ __forceinline__ void st<__nv_bfloat16>(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+template <> __device__ __forceinline__ void st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
+
+// ---------------------------------------------------------------- geometry
+
+// Axis decision and traversal order exactly as the reference CPU path takes
+// them: float sin/cos of the float angle, cos^2 > 0.5 in float
+// (src/cpu/forward3d.cpp:308-310, include/cpu3d_common.h:64-87).
+__device__ __forceinline__ void view_decisions(float ang, int& use_x, int& keep) {
+    const double a = (double)ang;
+    const float cf = __double2float_rn(cos(a));
+    const float sf = __double2float_rn(sin(a));
+    use_x = __fmul_rn(cf, cf) > 0.5f;
+    keep = use_x ? (cf >= 0.0f) : (sf >= 0.0f);
+}
+
+__device__ __forceinline__ double sigma(int keep, double k, int nu) {
+    return keep ? (k - 0.5 * nu) : (0.5 * nu - k);
+}
+
+// Intercept of the ray source -> point with the common axis (xrmath.h:8-22).
+__device__ __forceinline__ double map_point(const ViewHdr& h, double px, double py) {
+    if (h.use_x) return (h.sx * py - h.sy * px) / (py - h.sy);
+    return (h.sy * px - h.sx * py) / (px - h.sx);
+}
+
+// Same for a ray leaving the source at angle a (xrmath.h:24-38).
+__device__ __forceinline__ double map_angle(const ViewHdr& h, double a) {
+    if (h.use_x) return h.sx + h.sy * tan(a);
+    return h.sy + h.sx / tan(a);
+}
+
+// Axis coordinate of detector boundary k (traversal order).
+//   flat: forward3d.cpp:229-243 (3D scales u by SOD/SDD; 2D du is already
+//         the isocentre spacing, projector.py:97) ; arc: forward3d.cpp:271-283 ;
+//   parallel: forward3d.cpp:53-56.
+__device__ __forceinline__ double boundary_axis(const Geom& g, const ViewHdr& h, double k, double uscale) {
+    const double sg = sigma(h.keep, k, g.Nu);
+    if (g.type == GEO_FLAT) {
+        const double u = (sg * g.du + g.shu) * uscale;
+        return map_point(h, u * h.c, u * h.s);
+    }
+    if (g.type == GEO_ARC) return map_angle(h, sg * g.du + g.shu + h.beta);
+    const double u = sg * g.du + g.shu;
+    return h.use_x ? u / h.c : u / h.s;
+}
+
+// Line-position coefficients of the ray through axis point D:
+// pos(L) = A + B * L in pixel units along line L.
+__device__ __forceinline__ void boundary_line_coeffs(const Geom& g, const ViewHdr& h, double D,
+                                                     double& A, double& B) {
+    if (h.use_x) {
+        const double pyA = (0.5 * g.H - 0.5) * g.dy + g.shy, pyB = -g.dy;
+        const double x0 = -0.5 * g.W * g.dx + g.shx;
+        if (g.type == GEO_PARALLEL) {
+            const double t = h.s / h.c;
+            A = (D - t * pyA - x0) / g.dx;
+            B = -t * pyB / g.dx;
+        } else {
+            const double e = D - h.sx;
+            A = (h.sx + e * (1.0 - pyA / h.sy) - x0) / g.dx;
+            B = -e * pyB / (h.sy * g.dx);
+        }
+    } else {
+        const double pxA = (0.5 - 0.5 * g.W) * g.dx + g.shx, pxB = g.dx;
+        const double y0 = -0.5 * g.H * g.dy + g.shy;
+        if (g.type == GEO_PARALLEL) {
+            const double t = h.c / h.s;
+            A = (D - t * pxA - y0) / g.dy;
+            B = -t * pxB / g.dy;
+        } else {
+            const double e = D - h.sy;
+            A = (h.sy + e * (1.0 - pxA / h.sx) - y0) / g.dy;
+            B = -e * pxB / (h.sx * g.dy);
+        }
+    }
+}
+
+// Fractional traversal index of the detector position hit by the ray
+// source -> world point (x, y).  FP32 guess only; callers verify against the
+// FP64 boundary tables.
+__device__ __forceinline__ float col_guess(const Geom& g, const ViewHdr& h, float x, float y, float uscale) {
+    const float s = (float)h.s, c = (float)h.c;
+    float sg;
+    if (g.type == GEO_FLAT) {
+        const float R = (float)g.sod;
+        const float u = R * (x * c + y * s) / (R + x * s - y * c);   // virtual detector coordinate
+        sg = (u / uscale - (float)g.shu) / (float)g.du;
+    } else if (g.type == GEO_ARC) {
+        const float ac = (float)(h.beta + g.shu);
+        const float dcx = sinf(ac), dcy = -cosf(ac);
+        const float ex = x - (float)h.sx, ey = y - (float)h.sy;
+        const float gam = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey);
+        sg = gam / (float)g.du;
+    } else {
+        const float u = x * c + y * s;
+        sg = (u - (float)g.shu) / (float)g.du;
+    }
+    return h.keep ? sg + 0.5f * g.Nu : 0.5f * g.Nu - sg;
+}
+
+// World coordinates of pixel boundary `p` (pixel units) on line L.
+__device__ __forceinline__ void line_point(const Geom& g, const ViewHdr& h, int L, float p,
+                                           float& x, float& y) {
+    if (h.use_x) {
+        y = (float)((0.5 * g.H - L - 0.5) * g.dy + g.shy);
+        x = (float)(-0.5 * g.W * g.dx + g.shx) + p * (float)g.dx;
+    } else {
+        x = (float)((L - 0.5 * g.W + 0.5) * g.dx + g.shx);
+        y = (float)(-0.5 * g.H * g.dy + g.shy) + p * (float)g.dy;
+    }
+}
+
+// FBP voxel weight: cone_voxel_weight_flat / _arc (xrmath.h:215-226,
+// backward2d.cpp:93 / :161).
+__device__ __forceinline__ float fbp_weight(const Geom& g, const ViewHdr& h, float px, float py) {
+    if (g.type == GEO_FLAT) {
+        const float R = (float)g.sod;
+        const float d = ((float)h.sx * px + (float)h.sy * py) / R;
+        const float den = R - d;
+        return R * R / (den * den);
+    }
+    if (g.type == GEO_ARC) {
+        const float ex = (float)h.sx - px, ey = (float)h.sy - py;
+        return 1.0f / (ex * ex + ey * ey);
+    }
+    return 1.0f;
+}
+
+// Voxel-centre world coordinates of pixel index p (pixel units, integer) on line L.
+__device__ __forceinline__ void pixel_center(const Geom& g, const ViewHdr& h, int L, int p,
+                                             float& px, float& py) {
+    int ix, iy;
+    if (h.use_x) { ix = p; iy = L; } else { ix = L; iy = g.H - 1 - p; }
+    px = (float)((ix - 0.5 * g.W + 0.5) * g.dx + g.shx);
+    py = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);
+}
+
+}  // namespace xr

@@ -1,0 +1,522 @@
+// Kernels of the B200 distance-driven projector.
+//
+// Two gather shapes cover all six operators of each geometry (so no kernel
+// needs atomics):
+//   cell gather (detector-cell owned):  A, B^T, Bw^T
+//       y[cell] = S_cell * sum_vox K[cell, vox] * T_vox * x[vox]
+//   voxel gather (voxel owned):         A^T, B, Bw
+//       x[vox]  = sum_views T_vox * sum_cells K[cell, vox] * S_cell * y[cell]
+// with S_cell = s_A (A, A^T) or 1, and T_vox = column width (B family), times
+// the FBP voxel weight for Bw.
+//
+// Reference kernels these replace (XRecon src/kernels): forward3d_flat.cu:7-246
+// and forward3d_arc.cu:7-243 (A), backward3d_flat.cu:7-128 and
+// backward3d_arc.cu:7-128 (B/Bw), forward3d_flat.cu:249-486 and
+// forward3d_arc.cu:246-480 (A^T), backward3d_flat.cu:131-377 and
+// backward3d_arc.cu:131-249 (B^T/Bw^T), forward3d_parallel.cu:33-219 (3D
+// parallel), forward2d.cu / forward2d_t.cu / backward2d.cu / backward2d_t.cu
+// (2D).
+#pragma once
+
+#include "xr_common.cuh"
+
+namespace xr {
+
+constexpr int MAXB = 4;  // pixels per column handled per merge pass
+
+// Sum over the pixel band of one column: sum_i w[i] * vol[j, L, pc + i].
+template <typename TI>
+__device__ __forceinline__ float band_value(const TI* __restrict__ base, int j, size_t plane, int D,
+                                            const float (&w)[MAXB], int np) {
+    if ((unsigned)j >= (unsigned)D) return 0.0f;
+    const TI* p = base + (size_t)j * plane;
+    float s = w[0] * ld(p);
+#pragma unroll
+    for (int i = 1; i < MAXB; ++i)
+        if (i < np) s = fmaf(w[i], ld(p + i), s);
+    return s;
+}
+
+template <typename TI>
+__device__ __forceinline__ float row_value(const TI* __restrict__ colbase, int m, int Nv, int Nu) {
+    if ((unsigned)m >= (unsigned)Nv) return 0.0f;
+    return ld(colbase + (size_t)m * Nu);
+}
+
+// ------------------------------------------------------------------ setup
+
+// One thread per (view, boundary k in 0..Nu).  FP64 throughout.
+__global__ void setup_views_kernel(const Geom g, const int dim3d, const float* __restrict__ ang,
+                                   const int nview, const ViewTables vt) {
+    const int v = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nview || k > g.Nu) return;
+    ViewHdr h;
+    const float a = ang[v];
+    view_decisions(a, h.use_x, h.keep);
+    h.beta = (double)a;
+    h.s = sin(h.beta);
+    h.c = cos(h.beta);
+    h.sx = -h.s * g.sod;
+    h.sy = h.c * g.sod;
+    h.spar = h.use_x ? h.sx : h.sy;
+    h.sperp = h.use_x ? h.sy : h.sx;
+    h.nlines = h.use_x ? g.H : g.W;
+    h.npix = h.use_x ? g.W : g.H;
+    if (h.use_x) { h.perpA = (0.5 * g.H - 0.5) * g.dy + g.shy; h.perpB = -g.dy; }
+    else         { h.perpA = (0.5 - 0.5 * g.W) * g.dx + g.shx; h.perpB = g.dx; }
+    if (g.type == GEO_PARALLEL) { h.q0 = 1.0; h.q1 = 0.0; }
+    else { h.q0 = 1.0 - h.perpA / h.sperp; h.q1 = -h.perpB / h.sperp; }
+    h.dpix = h.use_x ? g.dx : g.dy;
+    if (k == 0) vt.hdr[v] = h;
+
+    const double uscale = (dim3d && g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
+    const double Dk = boundary_axis(g, h, (double)k, uscale);
+    double A, B;
+    boundary_line_coeffs(g, h, Dk, A, B);
+    const size_t ob = (size_t)v * (g.Nu + 1) + k;
+    vt.bA[ob] = A;
+    vt.bB[ob] = B;
+    if (k >= g.Nu) return;
+
+    const size_t oc = (size_t)v * g.Nu + k;
+    const double Dk1 = boundary_axis(g, h, (double)k + 1.0, uscale);
+    const double dperp = h.use_x ? g.dy : g.dx;
+    if (g.type == GEO_PARALLEL) {
+        // forward3d.cpp:58,98 (xy_scale / dv) and system_matrix2d.cpp:109.
+        vt.colQ[oc] = 1.0 / g.dz;
+        vt.colE[oc] = (float)(dim3d ? dperp / (g.du * g.dv) : dperp / g.du);
+        vt.colF[oc] = 1.0f;
+        vt.colM[oc] = 0.0f;
+        return;
+    }
+    // Column centre and its z magnification: forward3d.cpp:258-297.
+    const double sgc = sigma(h.keep, (double)k + 0.5, g.Nu);
+    double cx, cy;
+    if (g.type == GEO_FLAT) {
+        const double u = (sgc * g.du + g.shu) * uscale;
+        cx = u * h.c;
+        cy = u * h.s;
+    } else {
+        const double ac = sgc * g.du + g.shu + h.beta;
+        cx = sin(ac) * g.sdd + h.sx;
+        cy = -cos(ac) * g.sdd + h.sy;
+    }
+    const double M = h.use_x ? h.sy / (h.sy - cy) : h.sx / (h.sx - cx);
+    vt.colQ[oc] = M / g.dz;
+    const double aa = 0.5 * (Dk + Dk1) - h.spar;
+    const double F = aa * aa + h.sperp * h.sperp;
+    if (dim3d) {
+        // s_A = dperp / (area * triangle_cosine): forward3d.cpp:331-343.
+        const double rs = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
+        vt.colE[oc] = (float)(dperp / (fabs(h.sperp) * (Dk1 - Dk) * M * g.dv * rs));
+        vt.colF[oc] = (float)F;
+        vt.colM[oc] = (float)M;
+    } else {
+        // 2D: dperp / ((D1 - D0) * cos_weight), system_matrix2d.cpp:213,251.
+        vt.colE[oc] = (float)(dperp * sqrt(F) / (fabs(h.sperp) * (Dk1 - Dk)));
+        vt.colF[oc] = 1.0f;
+        vt.colM[oc] = 0.0f;
+    }
+}
+
+// Image plane transpose with the y flip: out[b][x][H-1-y] = in[b][y][x], so
+// that lines of the y-axis views (image columns) are contiguous in the
+// pixel coordinate p = H-1-iy.
+template <typename T>
+__global__ void transpose_flip_kernel(const T* __restrict__ in, T* __restrict__ out, int H, int W) {
+    __shared__ T tile[32][33];
+    const size_t plane = (size_t)H * W;
+    const T* src = in + (size_t)blockIdx.z * plane;
+    T* dst = out + (size_t)blockIdx.z * plane;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+        const int y = y0 + dy, x = x0 + threadIdx.x;
+        if (y < H && x < W) tile[dy][threadIdx.x] = src[(size_t)y * W + x];
+    }
+    __syncthreads();
+    for (int dx = threadIdx.y; dx < 32; dx += blockDim.y) {
+        const int x = x0 + dx, y = y0 + threadIdx.x;
+        if (y < H && x < W) dst[(size_t)x * H + (H - 1 - y)] = tile[threadIdx.x][dx];
+    }
+}
+
+// ------------------------------------------------------------- 3D kernels
+
+// Cell gather: lane = detector column (traversal order), warp = run of R
+// detector rows.  Each thread sweeps the image lines; per line it forms the
+// pixel band of its column (FP64 boundaries, FP32 weights) and merges the
+// z voxels of the band against its R rows in local coordinates.
+template <typename TI, typename TO, int R, int MODE>
+__global__ void __launch_bounds__(256)
+cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ vol_rows,
+                     const TI* __restrict__ vol_cols, TO* __restrict__ sino, const int nview,
+                     const int view0, const double z0dz, const double zd0, const double dvv,
+                     const float cw) {
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int r0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
+    const int vb = blockIdx.z + view0;
+    const int v = vb % nview, b = vb / nview;
+    const int Nu = g.Nu;
+    if (k >= Nu || r0 >= g.Nv) return;
+    const ViewHdr h = vt.hdr[v];
+    const size_t ob = (size_t)v * (Nu + 1) + k;
+    const double bA0 = vt.bA[ob], bB0 = vt.bB[ob], bA1 = vt.bA[ob + 1], bB1 = vt.bB[ob + 1];
+    const double Qk = vt.colQ[(size_t)v * Nu + k];
+    const int nlines = h.nlines, npix = h.npix;
+    const size_t plane = (size_t)nlines * npix;
+    const TI* __restrict__ vol = (h.use_x ? vol_rows : vol_cols) + (size_t)b * g.D * plane;
+    const double zr0 = zd0 + r0 * dvv;
+
+    float acc[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = 0.0f;
+
+    for (int L = 0; L < nlines; ++L) {
+        const double pk = fma(bB0, (double)L, bA0);
+        const double pk1 = fma(bB1, (double)L, bA1);
+        const int pa = max((int)floor(pk), 0);
+        const int pb = min((int)ceil(pk1) - 1, npix - 1);
+        if (pa > pb) continue;
+        const double q = fma(h.q1, (double)L, h.q0);
+        const double gq = Qk * q;
+        const double t0 = fma(gq, zr0, -z0dz);
+        const double bt = gq * dvv;
+        if (!(bt > 0.0 && bt < 1.0e6)) continue;
+        if (t0 + R * bt <= 0.0 || t0 >= (double)g.D) continue;
+        const double jf = floor(t0);
+        const int j0 = (int)jf;
+        const float f = (float)(t0 - jf);
+        const float bf = (float)bt;
+        const float lf = (MODE == OP_A) ? (float)(h.dpix * g.dz / (q * q)) : cw;
+        for (int pc = pa; pc <= pb; pc += MAXB) {
+            const int np = min(MAXB, pb - pc + 1);
+            float w[MAXB];
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                float wi = 0.0f;
+                if (i < np) {
+                    const double pp = (double)(pc + i);
+                    wi = (float)(fmin(pp + 1.0, pk1) - fmax(pp, pk)) * lf;
+                    if (MODE == OP_BWT) {
+                        float px, py;
+                        pixel_center(g, h, L, pc + i, px, py);
+                        wi *= fbp_weight(g, h, px, py);
+                    }
+                }
+                w[i] = wi;
+            }
+            const TI* __restrict__ base = vol + (size_t)L * npix + pc;
+            int m = 0;
+            float pos = f;
+            if (j0 < 0) { m = -j0; pos = (float)m; }
+            float jn = (float)(m + 1);
+            float vj = band_value(base, j0 + m, plane, g.D, w, np);
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const float top = fmaf(bf, (float)(i + 1), f);
+                float a = 0.0f;
+                while (jn < top) {
+                    a = fmaf(jn - pos, vj, a);
+                    pos = jn;
+                    ++m;
+                    jn += 1.0f;
+                    vj = band_value(base, j0 + m, plane, g.D, w, np);
+                }
+                if (top > pos) { a = fmaf(top - pos, vj, a); pos = top; }
+                acc[i] += a;
+            }
+        }
+    }
+
+    const int col = h.keep ? k : Nu - 1 - k;
+    TO* out = sino + (((size_t)b * nview + v) * g.Nv) * Nu + col;
+    float E = 1.0f, F = 0.0f, M = 0.0f;
+    if (MODE == OP_A) {
+        const size_t oc = (size_t)v * Nu + k;
+        E = vt.colE[oc]; F = vt.colF[oc]; M = vt.colM[oc];
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int r = r0 + i;
+        if (r < g.Nv) {
+            float s = acc[i];
+            if (MODE == OP_A) {
+                const float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+                s *= E * sqrtf(F + zc * zc);
+            }
+            st(out + (size_t)r * Nu, s);
+        }
+    }
+}
+
+// A^T cell scale applied to the sinogram once (cone geometries).
+template <typename TI>
+__global__ void prescale_at3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ in,
+                                     float* __restrict__ out, const int nview, const size_t total,
+                                     const double zd0, const double dvv) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int c = (int)(idx % g.Nu);
+    const int r = (int)((idx / g.Nu) % g.Nv);
+    const int v = (int)((idx / ((size_t)g.Nu * g.Nv)) % nview);
+    const int keep = vt.hdr[v].keep;
+    const int k = keep ? c : g.Nu - 1 - c;
+    const size_t oc = (size_t)v * g.Nu + k;
+    const float zc = (float)(zd0 + (r + 0.5) * dvv) * vt.colM[oc];
+    out[idx] = ld(in + idx) * vt.colE[oc] * sqrtf(vt.colF[oc] + zc * zc);
+}
+
+// Voxel gather: lane = image column ix (32 consecutive), warp = run of R
+// voxels along z.  Each thread sweeps all views; per view it finds the
+// detector columns overlapping its pixel (FP32 guess, FP64 boundaries) and
+// merges its R voxels against the rows of each column.
+template <typename TI, typename TO, int R, int MODE>
+__global__ void __launch_bounds__(128)
+vox_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ sino, TO* __restrict__ vol,
+                    const int nview, const int nzg, const double z0dz, const double zd0, const double dvv,
+                    const float cw, const float uscale, const float atconst, const float oscale) {
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y;
+    const int zg = blockIdx.z % nzg, b = blockIdx.z / nzg;
+    const int j0 = (zg * blockDim.y + threadIdx.y) * R;
+    if (ix >= g.W || j0 >= g.D) return;
+    const int Nu = g.Nu, Nv = g.Nv;
+    float acc[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = 0.0f;
+    const TI* __restrict__ sinob = sino + (size_t)b * nview * Nv * Nu;
+
+    for (int v = 0; v < nview; ++v) {
+        const ViewHdr h = vt.hdr[v];
+        int L, p;
+        if (h.use_x) { L = iy; p = ix; } else { L = ix; p = g.H - 1 - iy; }
+        const double q = fma(h.q1, (double)L, h.q0);
+        float lf;
+        if (MODE == OP_AT) {
+            lf = (g.type == GEO_PARALLEL) ? atconst : (float)(h.dpix * g.dz / (q * q));
+        } else {
+            lf = cw;
+            if (MODE == OP_BW) {
+                float px, py;
+                pixel_center(g, h, L, p, px, py);
+                lf *= fbp_weight(g, h, px, py);
+            }
+        }
+        lf *= oscale;
+        float xa, ya, xb, yb;
+        line_point(g, h, L, (float)p, xa, ya);
+        line_point(g, h, L, (float)(p + 1), xb, yb);
+        float kf0 = col_guess(g, h, xa, ya, uscale), kf1 = col_guess(g, h, xb, yb, uscale);
+        const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const int ka = max(0, (int)floorf(lo) - 1);
+        const int kb = min(Nu - 1, (int)floorf(hi) + 1);
+        if (ka > kb) continue;
+        const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
+        const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
+        const double* __restrict__ Q = vt.colQ + (size_t)v * Nu;
+        const TI* __restrict__ sv = sinob + (size_t)v * Nv * Nu;
+        double pk = fma(bB[ka], (double)L, bA[ka]);
+        for (int k = ka; k <= kb; ++k) {
+            const double pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
+            const double wd = fmin((double)p + 1.0, pk1) - fmax((double)p, pk);
+            pk = pk1;
+            if (!(wd > 0.0)) continue;
+            const double gq = Q[k] * q;
+            const double T0 = fma(gq, zd0, -z0dz);
+            const double bt = gq * dvv;
+            if (!(bt > 0.0 && bt < 1.0e6)) continue;
+            if (T0 >= (double)(j0 + R) || T0 + Nv * bt <= (double)j0) continue;
+            int rs = (int)floorf((float)((double)j0 - T0) / (float)bt);
+            double trs = fma((double)rs, bt, T0);
+            if (trs > (double)j0) { --rs; trs -= bt; }
+            else if (trs + bt <= (double)j0) { ++rs; trs += bt; }
+            const int col = h.keep ? k : Nu - 1 - k;
+            const TI* __restrict__ sc = sv + col;
+            const float wk = (float)wd * lf;
+            const float bf = (float)bt;
+            int m = rs;
+            float pos = 0.0f;
+            float rn = (float)(trs - (double)j0) + bf;
+            float y = row_value(sc, m, Nv, Nu);
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const float top = (float)(i + 1);
+                float a = 0.0f;
+                while (rn < top) {
+                    a = fmaf(rn - pos, y, a);
+                    pos = rn;
+                    ++m;
+                    rn += bf;
+                    y = row_value(sc, m, Nv, Nu);
+                }
+                a = fmaf(top - pos, y, a);
+                pos = top;
+                acc[i] = fmaf(wk, a, acc[i]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int j = j0 + i;
+        if (j < g.D) st(vol + (((size_t)b * g.D + j) * g.H + iy) * g.W + ix, acc[i]);
+    }
+}
+
+// ------------------------------------------------------------- 2D kernels
+
+// Cell gather, 2D: one thread per (view, column).
+template <typename TI, typename TO, int MODE>
+__global__ void __launch_bounds__(128)
+cell_gather2d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ img_rows,
+                     const TI* __restrict__ img_cols, TO* __restrict__ sino, const int nview,
+                     const float cw) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y, b = blockIdx.z;
+    const int Nu = g.Nu;
+    if (k >= Nu) return;
+    const ViewHdr h = vt.hdr[v];
+    const size_t ob = (size_t)v * (Nu + 1) + k;
+    const double bA0 = vt.bA[ob], bB0 = vt.bB[ob], bA1 = vt.bA[ob + 1], bB1 = vt.bB[ob + 1];
+    const int nlines = h.nlines, npix = h.npix;
+    const TI* __restrict__ img = (h.use_x ? img_rows : img_cols) + (size_t)b * nlines * npix;
+    float acc = 0.0f;
+    for (int L = 0; L < nlines; ++L) {
+        const double pk = fma(bB0, (double)L, bA0);
+        const double pk1 = fma(bB1, (double)L, bA1);
+        const int pa = max((int)floor(pk), 0);
+        const int pb = min((int)ceil(pk1) - 1, npix - 1);
+        if (pa > pb) continue;
+        float lf;
+        if (MODE == OP_A) lf = (float)(h.dpix / fma(h.q1, (double)L, h.q0));
+        else lf = cw;
+        const TI* __restrict__ line = img + (size_t)L * npix;
+        for (int pp = pa; pp <= pb; ++pp) {
+            float w = (float)(fmin((double)pp + 1.0, pk1) - fmax((double)pp, pk)) * lf;
+            if (MODE == OP_BWT) {
+                float px, py;
+                pixel_center(g, h, L, pp, px, py);
+                w *= fbp_weight(g, h, px, py);
+            }
+            acc = fmaf(w, ld(line + pp), acc);
+        }
+    }
+    if (MODE == OP_A) acc *= vt.colE[(size_t)v * Nu + k];
+    const int col = h.keep ? k : Nu - 1 - k;
+    st(sino + ((size_t)b * nview + v) * Nu + col, acc);
+}
+
+// Voxel gather, 2D: one thread per pixel, sweeping the views.
+template <typename TI, typename TO, int MODE>
+__global__ void __launch_bounds__(256)
+vox_gather2d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ sino, TO* __restrict__ img,
+                    const int nview, const float cw, const float oscale) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int b = blockIdx.z;
+    if (ix >= g.W || iy >= g.H) return;
+    const int Nu = g.Nu;
+    const TI* __restrict__ sinob = sino + (size_t)b * nview * Nu;
+    float acc = 0.0f;
+    for (int v = 0; v < nview; ++v) {
+        const ViewHdr h = vt.hdr[v];
+        int L, p;
+        if (h.use_x) { L = iy; p = ix; } else { L = ix; p = g.H - 1 - iy; }
+        float lf;
+        if (MODE == OP_AT) {
+            lf = (float)(h.dpix / fma(h.q1, (double)L, h.q0));
+        } else {
+            lf = cw;
+            if (MODE == OP_BW) {
+                float px, py;
+                pixel_center(g, h, L, p, px, py);
+                lf *= fbp_weight(g, h, px, py);
+            }
+        }
+        float xa, ya, xb, yb;
+        line_point(g, h, L, (float)p, xa, ya);
+        line_point(g, h, L, (float)(p + 1), xb, yb);
+        const float kf0 = col_guess(g, h, xa, ya, 1.0f), kf1 = col_guess(g, h, xb, yb, 1.0f);
+        const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const int ka = max(0, (int)floorf(lo) - 1);
+        const int kb = min(Nu - 1, (int)floorf(hi) + 1);
+        if (ka > kb) continue;
+        const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
+        const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
+        const TI* __restrict__ sv = sinob + (size_t)v * Nu;
+        double pk = fma(bB[ka], (double)L, bA[ka]);
+        for (int k = ka; k <= kb; ++k) {
+            const double pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
+            const double wd = fmin((double)p + 1.0, pk1) - fmax((double)p, pk);
+            pk = pk1;
+            if (!(wd > 0.0)) continue;
+            float w = (float)wd * lf;
+            if (MODE == OP_AT) w *= vt.colE[(size_t)v * Nu + k];
+            const int col = h.keep ? k : Nu - 1 - k;
+            acc = fmaf(w, ld(sv + col), acc);
+        }
+    }
+    st(img + ((size_t)b * g.H + iy) * g.W + ix, acc * oscale);
+}
+
+// -------------------------------------------------------------- FBP filter
+
+// out[row, i] = sum_j x[row, j] * filt[j - i + Nu - 1], x = in * cosw * parker.
+// One CTA per detector row at a time; each thread produces OUTS consecutive
+// outputs with the filter window kept in registers.
+template <typename TI, int OUTS>
+__global__ void __launch_bounds__(256)
+fbp_filter_kernel(const TI* __restrict__ in, float* __restrict__ out, const int nrows, const int Nu,
+                  const int nview, const int rows_per_view, const float* __restrict__ cosw,
+                  const float* __restrict__ filt, const float* __restrict__ parker) {
+    extern __shared__ float smem[];
+    float* f = smem;              // 2*Nu - 1 (+ OUTS padding)
+    float* x = smem + 2 * Nu + OUTS;  // Nu (+ OUTS padding)
+    const int nf = 2 * Nu - 1;
+    for (int i = threadIdx.x; i < nf + OUTS + 1; i += blockDim.x) f[i] = (i < nf) ? filt[i] : 0.0f;
+    for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+        const int view = (row / rows_per_view) % nview;
+        const TI* src = in + (size_t)row * Nu;
+        __syncthreads();
+        for (int j = threadIdx.x; j < Nu + OUTS; j += blockDim.x) {
+            float val = 0.0f;
+            if (j < Nu) {
+                val = ld(src + j);
+                if (cosw) val *= cosw[j];
+                if (parker) val *= parker[(size_t)view * Nu + j];
+            }
+            x[j] = val;
+        }
+        __syncthreads();
+        for (int i0 = threadIdx.x * OUTS; i0 < Nu; i0 += blockDim.x * OUTS) {
+            // out[i0 + t] = sum_j x[j] * f[j + Nu - 1 - i0 - t]
+            float acc[OUTS];
+            float win[OUTS];
+#pragma unroll
+            for (int t = 0; t < OUTS; ++t) acc[t] = 0.0f;
+            // window for j = 0: win[t] = f[Nu - 1 - i0 - t] (index may be < 0 -> treat as 0)
+#pragma unroll
+            for (int t = 0; t < OUTS; ++t) {
+                const int fi = Nu - 1 - i0 - t;
+                win[t] = (fi >= 0) ? f[fi] : 0.0f;
+            }
+            for (int j = 0; j < Nu; ++j) {
+                const float xj = x[j];
+#pragma unroll
+                for (int t = 0; t < OUTS; ++t) acc[t] = fmaf(xj, win[t], acc[t]);
+                // shift: next j uses f[j + 1 + Nu - 1 - i0 - t] = old win[t - 1]
+#pragma unroll
+                for (int t = OUTS - 1; t > 0; --t) win[t] = win[t - 1];
+                const int fi = j + Nu - i0;  // = (j + 1) + Nu - 1 - i0 - 0
+                win[0] = (fi < nf) ? f[fi] : 0.0f;
+            }
+#pragma unroll
+            for (int t = 0; t < OUTS; ++t)
+                if (i0 + t < Nu) out[(size_t)row * Nu + i0 + t] = acc[t];
+        }
+    }
+}
+
+}  // namespace xr

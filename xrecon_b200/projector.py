@@ -1,0 +1,444 @@
+"""``Projector2d`` / ``Projector3d``: drop-in replacements of XRecon's
+projector modules (xrecon/projector/projector.py:21-316 and
+xrecon/projector/projector3d.py:29-287) running on the B200 kernels.
+
+Same constructor arguments, buffers (``options``, ``weight``, ``filter``,
+registered non-persistent unless ``trainable``), method names, shapes,
+assertions and FBP/FDK semantics.  ``filtered_backprojection`` runs the fused
+cosine-weight x Parker x filter kernel followed by the weighted backprojection
+when no gradient is needed; when the sinogram, ``weight`` or ``filter``
+require gradients it runs differentiable torch ops for the weighting and
+filtering (FP32, TF32 disabled) followed by the weighted-backprojection
+autograd Function.
+"""
+from __future__ import annotations
+
+import math
+from typing import List, Optional, Tuple, Union
+
+import torch
+import torch.nn as nn
+from torch import Tensor
+
+from . import _native
+from .backend import HostGeometry
+from .filters import filter_generate
+from .functions import (
+    BackProjection2d, BackProjection3d, BackProjectionTranspose2d, BackProjectionTranspose3d,
+    Projection2d, Projection3d, ProjectionTranspose2d, ProjectionTranspose3d,
+    WeightedBackProjection2d, WeightedBackProjection3d, WeightedBackProjectionTranspose2d,
+    WeightedBackProjectionTranspose3d,
+)
+from .geometry import (
+    ConeBeam3d, FanBeam2d, ParallelBeam2d, ParallelBeam3d, Volume2d, Volume3d, make_geometry2d,
+    make_geometry3d, pack_options2d, pack_options3d,
+)
+
+_SCAN_ALIASES = {"para": "parallel", "parallel": "parallel", "flat": "flat", "arc": "arc"}
+
+
+def mean_angle_step(angles: Tensor) -> Tensor:
+    """Mean wrapped angular step |((d + pi) mod 2pi) - pi| (projector.py:303-313)."""
+    if angles.numel() < 2:
+        return angles.new_tensor(0.0)
+    d = torch.diff(angles)
+    return ((d + math.pi) % (2 * math.pi) - math.pi).abs().mean()
+
+
+def parker_weights(angles: Tensor, gamma: Tensor, num_det: int) -> Tensor:
+    """Short-scan weights (projector.py:208-246): sin^2 ramps of width
+    2*(overscan - gamma) at the start and end of the scan, where
+    overscan = max((range - pi)/2, gamma_max); ones for full scans."""
+    V = angles.numel()
+    ones = torch.ones((V, num_det), device=angles.device, dtype=angles.dtype)
+    if V < 2:
+        return ones
+    beta = angles - angles[0]
+    scan_range = beta[-1].abs()
+    gamma_max = gamma.abs().max()
+    if scan_range >= (2 * math.pi - 1e-4):
+        return ones
+    if scan_range < math.pi + 2.0 * gamma_max - mean_angle_step(angles):
+        raise ValueError("Parker weighting requires a short-scan range of at least "
+                         f"pi + 2 * gamma_max, got {scan_range.item():.6f} rad")
+    overscan = torch.clamp((scan_range - math.pi) / 2.0, min=gamma_max)
+    eps = torch.finfo(angles.dtype).eps
+    left = 2.0 * (overscan - gamma)
+    right = scan_range - 2.0 * (overscan + gamma)
+    b = beta[:, None]
+    w_left = torch.sin(0.5 * math.pi * b / torch.clamp(left, min=eps)[None, :]).pow(2)
+    w_right = torch.sin(0.5 * math.pi * (scan_range - b) / torch.clamp(scan_range - right, min=eps)[None, :]).pow(2)
+    w = torch.where(b < left[None, :], w_left, ones)
+    w = torch.where(b > right[None, :], w_right, w)
+    return w.clamp_(0.0, 1.0)
+
+
+class _ProjectorBase(nn.Module):
+    _dim = 0
+
+    def _host(self) -> HostGeometry:
+        return self._host_geom
+
+    @staticmethod
+    def _prepare_angles(angles: Tensor, ref: Tensor) -> Tensor:
+        return angles.to(device=ref.device, dtype=torch.float32 if ref.dtype in (torch.bfloat16, torch.float16)
+                         else ref.dtype).contiguous()
+
+    @staticmethod
+    def _mean_angle_step(angles: Tensor) -> Tensor:
+        return mean_angle_step(angles)
+
+    def _fbp(self, sino: Tensor, angles: Tensor, filter, filter_type, redundant, parker: bool,
+             rows_per_view: int) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        if filter is not None:
+            filt = filter
+        elif filter_type is None or filter_type.lower() == self.filter_type:
+            filt = self.filter
+        else:
+            filt = self._filter_generate(filter_type.lower(), dtype=torch.float32).to(sino.device)
+        pw = None
+        if parker:
+            pw = self.parker_weight(angles)
+            if redundant is None:
+                redundant = False
+        elif redundant is None:
+            redundant = True
+        scale = self._mean_angle_step(angles.to(torch.float32))
+        if redundant:
+            scale = scale / 2
+        Nu = self._num_u()
+        wt = self.weight
+        needs_grad = torch.is_grad_enabled() and (
+            sino.requires_grad or (isinstance(filt, Tensor) and filt.requires_grad) or wt.requires_grad)
+        if needs_grad:
+            s = sino.to(torch.float32)
+            if pw is not None:
+                s = s * pw.to(device=s.device, dtype=s.dtype)
+            s = s * wt.to(device=s.device, dtype=s.dtype)
+            f = filt.to(device=s.device, dtype=s.dtype)
+            with torch.backends.cudnn.flags(enabled=True, allow_tf32=False):
+                if self._dim == 2:
+                    filtered = nn.functional.conv2d(s, f.reshape(1, 1, 1, -1), padding=(0, Nu - 1))
+                else:
+                    filtered = nn.functional.conv3d(s, f.reshape(1, 1, 1, 1, -1), padding=(0, 0, Nu - 1))
+            recon = self.backprojection_weighted(filtered.contiguous(), angles)
+            return recon * scale.to(device=recon.device, dtype=recon.dtype)
+        with torch.no_grad():
+            s = sino if sino.is_contiguous() else sino.contiguous()
+            filtered = _native.fbp_filter(
+                s, nview=angles.numel(), rows_per_view=rows_per_view,
+                cosw=wt.detach().reshape(-1), filt=filt.detach().reshape(-1),
+                parker=None if pw is None else pw.detach().reshape(angles.numel(), Nu))
+            recon = self.backprojection_weighted(filtered, angles)
+            if sino.dtype != torch.float32:
+                recon = recon.to(sino.dtype)
+            return recon * scale.to(device=recon.device, dtype=recon.dtype)
+
+
+class Projector2d(_ProjectorBase):
+    """Distance-driven 2D CT projector (parallel / fan-flat / fan-arc).
+
+    Shapes: image [B, C, H, W], angles [V], sino [B, C, V, Nu].
+    """
+    _dim = 2
+
+    def __init__(self, image_size: Union[int, Tuple[int, int], List[int], Volume2d],
+                 num_det=None, pix_size=None, det_size: Optional[float] = None,
+                 iso_source: float = 0.0, source_detector: float = 0.0, pixshift=0.0,
+                 binshift: float = 0.0, scan_type: str = "flat", filter_type: str = "ramp",
+                 trainable: bool = False, dtype=None) -> None:
+        super().__init__()
+        if isinstance(image_size, Volume2d):
+            volume = image_size
+            if isinstance(num_det, (FanBeam2d, ParallelBeam2d)) and pix_size is None:
+                pix_size = num_det
+            if not isinstance(pix_size, (FanBeam2d, ParallelBeam2d)):
+                raise TypeError("When image_size is Volume2d, pix_size should be a 2D geometry object")
+            geometry = pix_size
+        else:
+            if num_det is None or pix_size is None or det_size is None:
+                raise TypeError("num_det, pix_size and det_size are required with the legacy constructor")
+            volume = Volume2d(image_size, pix_size, pixshift)
+            geometry = make_geometry2d(scan_type, num_det, det_size, iso_source, source_detector, binshift)
+        scan = geometry.scan_type.lower().strip()
+        scan = _SCAN_ALIASES.get(scan, scan)
+        if scan not in ("parallel", "flat", "arc"):
+            raise ValueError(f"Unsupported scan_type: {scan}")
+        W, H = volume.size
+        sx, sy = volume.spacing
+        shx, shy = volume.shift
+        self.image_size = (W, H)
+        self.pix_size = (sx, sy)
+        self.volume = volume
+        self.geometry = geometry
+        self.num_det = geometry.detector.count
+        self.scan_type = scan
+        self.filter_type = filter_type.lower().strip()
+        self.iso_source = float(geometry.iso_source)
+        self.source_detector = float(geometry.source_detector)
+        self._default_dtype = dtype or torch.float32
+        self.det_size = geometry.effective_det_spacing
+        self.binshift = geometry.effective_det_shift
+        self.pixshift = (shx * sx, shy * sy)
+        packed = pack_options2d(volume, geometry)
+        self._host_geom = HostGeometry(2, packed)
+        self.register_buffer("options", torch.tensor(packed, dtype=self._default_dtype), persistent=False)
+        w = self._make_cosine_weight(dtype=self._default_dtype)
+        if trainable:
+            self.weight = nn.Parameter(w.clone())
+        else:
+            self.register_buffer("weight", w, persistent=False)
+        f = self._filter_generate(filter_type=self.filter_type, dtype=self._default_dtype)
+        if trainable:
+            self.filter = nn.Parameter(f.clone())
+        else:
+            self.register_buffer("filter", f, persistent=False)
+
+    def _num_u(self) -> int:
+        return self.num_det
+
+    def forward(self, image: Tensor, angles: Tensor) -> Tensor:
+        return self.projection(image, angles)
+
+    def projection(self, image: Tensor, angles: Tensor) -> Tensor:
+        _, _, h, w = image.shape
+        assert (w, h) == self.image_size, f"Expected input image size {self.image_size[::-1]}, but got {(h, w)}"
+        return Projection2d.apply(image, self._host(), self._prepare_angles(angles, image))
+
+    def backprojection(self, sino: Tensor, angles: Tensor) -> Tensor:
+        _, _, h, w = sino.shape
+        v, = angles.shape
+        assert (h, w) == (v, self.num_det), f"Expected input sino size {(v, self.num_det)}, but got {(h, w)}"
+        return BackProjection2d.apply(sino, self._host(), self._prepare_angles(angles, sino))
+
+    def backprojection_weighted(self, sino: Tensor, angles: Tensor) -> Tensor:
+        _, _, h, w = sino.shape
+        v, = angles.shape
+        assert (h, w) == (v, self.num_det), f"Expected input sino size {(v, self.num_det)}, but got {(h, w)}"
+        return WeightedBackProjection2d.apply(sino, self._host(), self._prepare_angles(angles, sino))
+
+    def projection_t(self, sino: Tensor, angles: Tensor) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        return ProjectionTranspose2d.apply(sino, self._host(), self._prepare_angles(angles, sino))
+
+    def backprojection_t(self, image: Tensor, angles: Tensor) -> Tensor:
+        _, _, h, w = image.shape
+        assert (w, h) == self.image_size, f"Expected input image size {self.image_size[::-1]}, but got {(h, w)}"
+        return BackProjectionTranspose2d.apply(image, self._host(), self._prepare_angles(angles, image))
+
+    def backprojection_weighted_t(self, image: Tensor, angles: Tensor) -> Tensor:
+        _, _, h, w = image.shape
+        assert (w, h) == self.image_size, f"Expected input image size {self.image_size[::-1]}, but got {(h, w)}"
+        return WeightedBackProjectionTranspose2d.apply(image, self._host(), self._prepare_angles(angles, image))
+
+    projection_transpose = projection_t
+    backprojection_transpose = backprojection_t
+    weighted_backprojection_transpose = backprojection_weighted_t
+
+    def system_matrix(self, angles: Tensor) -> Tensor:
+        raise NotImplementedError("the sparse system-matrix export is not part of this library")
+
+    get_sys_matrix = system_matrix
+
+    def filtered_backprojection(self, sino: Tensor, angles: Tensor, filter: Optional[Tensor] = None,
+                                filter_type: Optional[str] = None, redundant: Optional[bool] = None,
+                                parker: bool = False) -> Tensor:
+        return self._fbp(sino, angles, filter, filter_type, redundant, parker, rows_per_view=1)
+
+    def apply_parker_weight(self, sino: Tensor, angles: Tensor) -> Tensor:
+        return sino * self.parker_weight(angles).to(device=sino.device, dtype=sino.dtype)
+
+    def parker_weight(self, angles: Tensor) -> Tensor:
+        if self.scan_type not in ("flat", "arc") or angles.numel() < 2:
+            return torch.ones((1, 1, angles.numel(), self.num_det), device=angles.device, dtype=angles.dtype)
+        gamma = self._fan_angles(device=angles.device, dtype=angles.dtype)
+        return parker_weights(angles, gamma, self.num_det).view(1, 1, angles.numel(), self.num_det)
+
+    def _filter_generate(self, filter_type: str, dtype=None) -> Tensor:
+        return filter_generate(self.num_det, self.det_size, filter_type, dtype)[None, None, None, :]
+
+    def _make_cosine_weight(self, dtype=None) -> Tensor:
+        dtype = dtype or torch.float32
+        u = torch.arange(-self.num_det / 2 + 0.5, self.num_det / 2, 1.0, dtype=dtype)
+        s = u * self.det_size + self.binshift
+        if self.scan_type == "flat":
+            w = self.iso_source / torch.sqrt(s * s + self.iso_source * self.iso_source)
+        elif self.scan_type == "arc":
+            w = torch.cos(s)
+        else:
+            w = torch.ones_like(s)
+        return w.view(1, 1, 1, self.num_det)
+
+    def _fan_angles(self, device=None, dtype=None) -> Tensor:
+        dtype = dtype or torch.float32
+        u = torch.arange(-self.num_det / 2 + 0.5, self.num_det / 2, 1.0, device=device, dtype=dtype)
+        s = u * self.det_size + self.binshift
+        if self.scan_type == "arc":
+            return s
+        if self.scan_type == "flat":
+            return torch.atan2(s, torch.as_tensor(self.iso_source, device=device, dtype=dtype))
+        return torch.zeros_like(s)
+
+    def _check_sino_angles(self, sino: Tensor, angles: Tensor) -> None:
+        if sino.ndim != 4:
+            raise ValueError(f"Expected sino shape [B, C, V, Nu], got {tuple(sino.shape)}")
+        if angles.ndim != 1:
+            raise ValueError(f"Expected angles shape [V], got {tuple(angles.shape)}")
+        if sino.shape[2] != angles.numel() or sino.shape[3] != self.num_det:
+            raise ValueError(f"Expected sino shape [B, C, {angles.numel()}, {self.num_det}], got {tuple(sino.shape)}")
+
+
+class Projector3d(_ProjectorBase):
+    """Distance-driven 3D projector (parallel / cone-flat / cone-arc).
+
+    Shapes: image [B, C, D, H, W], angles [V], sino [B, C, V, Nv, Nu].
+    """
+    _dim = 3
+
+    def __init__(self, image_size, num_det=None, pix_size=None, det_size=None, iso_source: float = 0.0,
+                 source_detector: float = 0.0, pixshift=0.0, binshift=0.0, scan_type: str = "flat",
+                 filter_type: str = "ramp", trainable: bool = False, dtype=None) -> None:
+        super().__init__()
+        if isinstance(image_size, Volume3d):
+            volume = image_size
+            if isinstance(num_det, (ConeBeam3d, ParallelBeam3d)) and pix_size is None:
+                pix_size = num_det
+            if not isinstance(pix_size, (ConeBeam3d, ParallelBeam3d)):
+                raise TypeError("When image_size is Volume3d, pix_size should be a Geometry3d object")
+            geometry = pix_size
+        else:
+            if num_det is None or pix_size is None or det_size is None:
+                raise TypeError("num_det, pix_size and det_size are required with the legacy constructor")
+            volume = Volume3d(image_size, pix_size, pixshift)
+            geometry = make_geometry3d(scan_type, num_det, det_size, iso_source, source_detector, binshift)
+        scan = geometry.scan_type.lower().strip()
+        if scan not in ("parallel", "flat", "arc"):
+            raise ValueError(f"Unsupported 3D scan_type: {scan}")
+        W, H, D = volume.size
+        dx, dy, dz = volume.spacing
+        shx, shy, shz = volume.shift
+        self.volume = volume
+        self.geometry = geometry
+        self.image_size = (W, H, D)
+        self.pix_size = (dx, dy, dz)
+        self.num_det = tuple(geometry.detector.count)
+        self.det_size = tuple(geometry.effective_det_spacing)
+        self.binshift = tuple(geometry.effective_det_shift)
+        self.pixshift = (shx * dx, shy * dy, shz * dz)
+        self.scan_type = scan
+        self.filter_type = filter_type.lower().strip()
+        self.iso_source = float(getattr(geometry, "iso_source", 0.0))
+        self.source_detector = float(getattr(geometry, "source_detector", 0.0))
+        self._default_dtype = dtype or torch.float32
+        packed = pack_options3d(volume, geometry)
+        self._host_geom = HostGeometry(3, packed)
+        self.register_buffer("options", torch.tensor(packed, dtype=self._default_dtype), persistent=False)
+        w = self._make_cosine_weight(dtype=self._default_dtype)
+        if trainable:
+            self.weight = nn.Parameter(w.clone())
+        else:
+            self.register_buffer("weight", w, persistent=False)
+        f = self._filter_generate(filter_type=self.filter_type, dtype=self._default_dtype)
+        if trainable:
+            self.filter = nn.Parameter(f.clone())
+        else:
+            self.register_buffer("filter", f, persistent=False)
+
+    def _num_u(self) -> int:
+        return self.num_det[0]
+
+    def forward(self, image: Tensor, angles: Tensor) -> Tensor:
+        return self.projection(image, angles)
+
+    def projection(self, image: Tensor, angles: Tensor) -> Tensor:
+        self._check_image(image)
+        return Projection3d.apply(image, self._host(), self._prepare_angles(angles, image))
+
+    def projection_t(self, sino: Tensor, angles: Tensor) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        return ProjectionTranspose3d.apply(sino, self._host(), self._prepare_angles(angles, sino))
+
+    def backprojection(self, sino: Tensor, angles: Tensor) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        return BackProjection3d.apply(sino, self._host(), self._prepare_angles(angles, sino))
+
+    def backprojection_weighted(self, sino: Tensor, angles: Tensor) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        return WeightedBackProjection3d.apply(sino, self._host(), self._prepare_angles(angles, sino))
+
+    def backprojection_t(self, image: Tensor, angles: Tensor) -> Tensor:
+        self._check_image(image)
+        return BackProjectionTranspose3d.apply(image, self._host(), self._prepare_angles(angles, image))
+
+    def backprojection_weighted_t(self, image: Tensor, angles: Tensor) -> Tensor:
+        self._check_image(image)
+        return WeightedBackProjectionTranspose3d.apply(image, self._host(), self._prepare_angles(angles, image))
+
+    def system_matrix(self, angles: Tensor) -> Tensor:
+        raise NotImplementedError("the sparse system-matrix export is not part of this library")
+
+    get_sys_matrix = system_matrix
+    projection_transpose = projection_t
+    backprojection_transpose = backprojection_t
+    weighted_backprojection_transpose = backprojection_weighted_t
+
+    def filtered_backprojection(self, sino: Tensor, angles: Tensor, filter: Optional[Tensor] = None,
+                                filter_type: Optional[str] = None, redundant: Optional[bool] = None,
+                                parker: bool = False) -> Tensor:
+        """FDK: in-plane cosine weight (projector3d.py:233-246, no v term),
+        u-filter, weighted backprojection, x mean angle step (/2 when
+        redundant)."""
+        return self._fbp(sino, angles, filter, filter_type, redundant, parker, rows_per_view=self.num_det[1])
+
+    def parker_weight(self, angles: Tensor) -> Tensor:
+        Nu = self.num_det[0]
+        if angles.numel() < 2 or self.scan_type == "parallel":
+            return torch.ones((1, 1, angles.numel(), 1, Nu), device=angles.device, dtype=angles.dtype)
+        gamma = self._fan_angles(device=angles.device, dtype=angles.dtype)
+        return parker_weights(angles, gamma, Nu).view(1, 1, angles.numel(), 1, Nu)
+
+    def _filter_generate(self, filter_type: str, dtype=None) -> Tensor:
+        return filter_generate(self.num_det[0], self.det_size[0], filter_type, dtype)[None, None, None, None, :]
+
+    def _make_cosine_weight(self, dtype=None) -> Tensor:
+        dtype = dtype or torch.float32
+        Nu, du, shu = self.num_det[0], self.det_size[0], self.binshift[0]
+        u = torch.arange(-Nu / 2 + 0.5, Nu / 2, 1.0, dtype=dtype)
+        s = u * du + shu
+        if self.scan_type == "parallel":
+            return torch.ones((1, 1, 1, 1, Nu), dtype=dtype)
+        if self.scan_type == "flat":
+            w = self.iso_source / torch.sqrt(s * s + self.iso_source * self.iso_source)
+        else:
+            w = torch.cos(s)
+        return w.view(1, 1, 1, 1, Nu)
+
+    def _fan_angles(self, device=None, dtype=None) -> Tensor:
+        dtype = dtype or torch.float32
+        Nu, du, shu = self.num_det[0], self.det_size[0], self.binshift[0]
+        u = torch.arange(-Nu / 2 + 0.5, Nu / 2, 1.0, device=device, dtype=dtype)
+        s = u * du + shu
+        if self.scan_type in ("parallel", "arc"):
+            return s
+        return torch.atan2(s, torch.as_tensor(self.iso_source, device=device, dtype=dtype))
+
+    def _check_image(self, image: Tensor) -> None:
+        if image.ndim != 5:
+            raise ValueError(f"Expected image shape [B, C, D, H, W], got {tuple(image.shape)}")
+        W, H, D = self.image_size
+        if tuple(image.shape[2:]) != (D, H, W):
+            raise ValueError(f"Expected image shape [B, C, {D}, {H}, {W}], got {tuple(image.shape)}")
+
+    def _check_sino_angles(self, sino: Tensor, angles: Tensor) -> None:
+        if sino.ndim != 5:
+            raise ValueError(f"Expected sino shape [B, C, V, Nv, Nu], got {tuple(sino.shape)}")
+        if angles.ndim != 1:
+            raise ValueError(f"Expected angles shape [V], got {tuple(angles.shape)}")
+        Nu, Nv = self.num_det
+        if sino.shape[2] != angles.numel() or sino.shape[3] != Nv or sino.shape[4] != Nu:
+            raise ValueError(f"Expected sino shape [B, C, {angles.numel()}, {Nv}, {Nu}], got {tuple(sino.shape)}")
+
+
+projector2d = Projector2d
+projector3d = Projector3d
