@@ -105,6 +105,21 @@ int xr_dd3d(int op, const xr_geom3d* geom, const void* in, int dtype_in, void* o
 int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, int nview, int rows_per_view,
                   const float* cosw, const float* filt, const float* parker, void* stream);
 
+/*
+ * Read (and optionally clear) the device-wide error word of the current
+ * device: 0 when no kernel has reported a problem.  Bit 0 = a bounded wait
+ * for a TMA transfer gave up.  Synchronous (reads device memory).
+ */
+int xr_device_error(unsigned int* code, int clear);
+
+/* Staging plan of the 3D projection kernel for this geometry: whether the
+ * TMA line windows are used and their box size (pixels x z voxels). */
+int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, int* rows_per_thread);
+
+/* Testing aid: nonzero routes every operator through the plain (non-TMA)
+ * kernels, so both paths can be compared. */
+int xr_set_plain_kernels(int on);
+
 /* Human-readable message for the last non-OK status returned on this thread. */
 const char* xr_last_error(void);
 

@@ -33,3 +33,18 @@ def cuda():
     from xrecon_b200 import _native
     _native.lib()  # fail loudly if the extension is missing
     return torch.device("cuda:0")
+
+
+@pytest.fixture(autouse=True)
+def _device_error_word(request):
+    """After every GPU test: no kernel may have reported a bounded-wait
+    timeout through the device error word."""
+    yield
+    if request.node.get_closest_marker("gpu") is None:
+        return
+    import torch
+    if not torch.cuda.is_available():
+        return
+    from xrecon_b200 import _native
+    torch.cuda.synchronize()
+    assert _native.device_error(clear=True) == 0, "a kernel reported a device error"

@@ -61,6 +61,12 @@ def lib():
     L.xr_fbp_filter.restype = c_int
     L.xr_fbp_filter.argtypes = [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int,
                                 c_void_p, c_void_p, c_void_p, c_void_p]
+    L.xr_device_error.restype = c_int
+    L.xr_device_error.argtypes = [ctypes.POINTER(ctypes.c_uint), c_int]
+    L.xr_cell_plan.restype = c_int
+    L.xr_cell_plan.argtypes = [ctypes.POINTER(Geom3d)] + [ctypes.POINTER(c_int)] * 4
+    L.xr_set_plain_kernels.restype = c_int
+    L.xr_set_plain_kernels.argtypes = [c_int]
     L.xr_last_error.restype = ctypes.c_char_p
     L.xr_version.restype = ctypes.c_char_p
     _lib = L
@@ -196,6 +202,30 @@ def fbp_filter(sino: torch.Tensor, nview: int, rows_per_view: int, cosw: torch.T
     if rc != 0:
         _raise(rc, "xr_fbp_filter")
     return out
+
+
+def device_error(clear: bool = True) -> int:
+    """Device-wide error word (0 = no kernel reported a problem)."""
+    code = ctypes.c_uint(0)
+    rc = lib().xr_device_error(ctypes.byref(code), int(clear))
+    if rc != 0:
+        _raise(rc, "xr_device_error")
+    return int(code.value)
+
+
+def cell_plan(geom: Geom3d) -> dict:
+    """Staging plan of the 3D projection kernel (TMA box size) for a geometry."""
+    vals = [c_int(0) for _ in range(4)]
+    rc = lib().xr_cell_plan(ctypes.byref(geom), *[ctypes.byref(v) for v in vals])
+    if rc != 0:
+        _raise(rc, "xr_cell_plan")
+    return dict(ok=bool(vals[0].value), box_pixels=vals[1].value, box_z=vals[2].value,
+                rows_per_thread=vals[3].value)
+
+
+def set_plain_kernels(on: bool) -> None:
+    """Route operators through the plain (non-TMA) kernels (testing aid)."""
+    lib().xr_set_plain_kernels(int(bool(on)))
 
 
 def version() -> str:

@@ -6,13 +6,25 @@
 #include <cstdio>
 #include <string>
 
-#include "xr_kernels.cuh"
+#include <cudaTypedefs.h>
+
+#include <cstring>
+#include <type_traits>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "xr_cell_tma.cuh"
 #include "../../include/xrecon_b200.h"
+
 
 namespace xr {
 namespace {
 
 thread_local std::string g_last_error;
+
+// Test hook: route every operator through the plain (non-TMA) kernels.
+bool g_force_plain = false;
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -65,6 +77,16 @@ int validate(const Geom& g, int dim3d, int op, int nbatch, int nview) {
         if (g.type == GEO_ARC && !(g.du * g.Nu < 3.0))
             return fail(XR_ERR_INVALID_ARGUMENT, "arc detector fan (Nu*du = %g rad) must be below pi", g.du * g.Nu);
     }
+    if (dim3d) {
+        // detector row height over voxel height on the common axis; the
+        // kernels' merge loops assume it is a sane O(1) ratio.
+        const double rs = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
+        const double ratio = g.dv * rs / g.dz;
+        if (!(ratio > 1e-3 && ratio < 1e3))
+            return fail(XR_ERR_INVALID_ARGUMENT, "detector row / voxel height ratio %g outside [1e-3, 1e3]", ratio);
+        if ((long long)g.D * nbatch > 65535)
+            return fail(XR_ERR_UNSUPPORTED, "depth x batch (%lld) above 65535", (long long)g.D * nbatch);
+    }
     if (nbatch < 1) return fail(XR_ERR_INVALID_ARGUMENT, "batch (B*C) must be >= 1");
     if (nview < 0) return fail(XR_ERR_INVALID_ARGUMENT, "number of views must be >= 0");
     (void)dim3d;
@@ -88,8 +110,121 @@ Geom geom_from(const xr_geom2d* p) {
 }
 
 struct Layout {
-    size_t hdr, bA, bB, colQ, colE, colF, colM, volT, sinoS, total;
+    size_t hdr, bA, bB, colQ, colE, colF, colM, volT, volR, sinoS, total;
 };
+
+// ------------------------------------------------------ TMA staging plans
+
+struct CellPlan {
+    bool ok;
+    int BP, BZ, R;
+};
+
+constexpr int CELL_NW = 8;
+
+int cell_rows_per_thread(const Geom& g) { return g.Nv >= 128 ? 16 : 8; }
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Sizes the line window of the TMA cell gather for this geometry by
+// evaluating the kernel's own window function over the CTAs of views sampled
+// densely in angle (the window depends on the angle only through smooth
+// functions; the 45-degree axis switches are sampled on both sides).  Cached
+// per geometry.
+CellPlan plan_cell(const Geom& g) {
+    static std::mutex mu;
+    static std::map<std::string, CellPlan> cache;
+    const std::string key(reinterpret_cast<const char*>(&g), sizeof(Geom));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    CellPlan p{false, 0, 0, cell_rows_per_thread(g)};
+    const int RG = CELL_NW * p.R;
+    const double uscale = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
+    const double rs = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
+    const double zd0 = (-0.5 * g.Nv * g.dv + g.shv) * rs, dvv = g.dv * rs;
+    const double z0dz = (-0.5 * g.D * g.dz + g.shz) / g.dz;
+    std::vector<double> A(g.Nu + 1), B(g.Nu + 1), Q(g.Nu);
+    std::vector<double> angles;
+    const int NS = 256;
+    for (int i = 0; i < NS; ++i) angles.push_back(2.0 * M_PI * i / NS + 0.37 / NS);
+    for (int i = 0; i < 8; ++i) {
+        angles.push_back(M_PI / 4 * i + 1e-5);
+        angles.push_back(M_PI / 4 * i - 1e-5);
+    }
+    int maxspan = 0;
+    double maxnz = 0.0;
+    for (double ang : angles) {
+        ViewHdr h;
+        make_view_hdr(g, (float)ang, h);
+        for (int k = 0; k <= g.Nu; ++k) {
+            const double D = boundary_axis(g, h, (double)k, uscale);
+            boundary_line_coeffs(g, h, D, A[k], B[k]);
+        }
+        for (int k = 0; k < g.Nu; ++k) Q[k] = column_mag(g, h, k, uscale) / g.dz;
+        for (int k0 = 0; k0 < g.Nu; k0 += 32) {
+            const int kend = std::min(k0 + 32, g.Nu);
+            CellCtaGeo c;
+            c.bAk0 = A[k0]; c.bBk0 = B[k0]; c.bAke = A[kend]; c.bBke = B[kend];
+            c.Qmin = 1e300; c.Qmax = -1e300;
+            for (int k = k0; k < kend; ++k) { c.Qmin = std::min(c.Qmin, Q[k]); c.Qmax = std::max(c.Qmax, Q[k]); }
+            for (int rg0 = 0; rg0 < g.Nv; rg0 += RG) {
+                c.zlo = zd0 + rg0 * dvv;
+                c.zhi = zd0 + (rg0 + RG) * dvv;
+                for (int L : {0, h.nlines - 1}) {
+                    const CellWindow w = cell_window(c, h, L, z0dz, h.npix, g.D, 1 << 30, 1 << 30);
+                    if (w.empty) continue;
+                    const double ph = std::fma(c.bBke, (double)L, c.bAke);
+                    const int phi = std::min((int)std::ceil(ph) - 1, h.npix - 1);
+                    maxspan = std::max(maxspan, phi - w.p0 + 1);
+                    maxnz = std::max(maxnz, (double)(w.zlast - w.z0 + 1));
+                }
+            }
+        }
+    }
+    p.BP = round_up(std::max(maxspan, 8), 8);
+    p.BZ = (int)maxnz;
+    p.ok = p.BP <= 256 && p.BZ <= 256 && p.BZ >= 1 && (size_t)2 * p.BP * p.BZ * 4 <= 200 * 1024;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = p;
+    return p;
+}
+
+using EncodeTiledFn = PFN_cuTensorMapEncodeTiled_v12000;
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    });
+    return fn;
+}
+
+// 4D map over [nbatch][D][nlines][pitch] (pitch >= npix) with box (BP, 1, BZ, 1).
+bool encode_line_map(CUtensorMap* m, int dt, const void* base, int npix, int nlines, int D, int nbatch, int pitch,
+                     int BP, int BZ) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const size_t es = dt == DT_F32 ? 4 : 2;
+    const CUtensorMapDataType t = dt == DT_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                : dt == DT_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    cuuint64_t dims[4] = {(cuuint64_t)npix, (cuuint64_t)nlines, (cuuint64_t)D, (cuuint64_t)nbatch};
+    cuuint64_t strides[3] = {(cuuint64_t)pitch * es, (cuuint64_t)pitch * nlines * es,
+                             (cuuint64_t)pitch * nlines * D * es};
+    cuuint32_t box[4] = {(cuuint32_t)BP, 1u, (cuuint32_t)BZ, 1u};
+    cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+    const CUresult r = fn(m, t, 4, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 
 // Image-input ops of the cell gather need the flipped transpose of the image
 // (lines of y-axis views); cone A^T needs an FP32 pre-scaled sinogram.
@@ -110,8 +245,16 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
         else if (op == OP_BT || op == OP_BWT) eff = OP_A;
     }
     l.volT = o;
-    if (eff == OP_A || eff == OP_BT || eff == OP_BWT)
-        o = align256(o + (size_t)nbatch * g.D * g.H * g.W * dtype_size(dtype_in));
+    l.volR = o;
+    if (eff == OP_A || eff == OP_BT || eff == OP_BWT) {
+        // flipped transpose with a 16-byte-multiple pitch, plus (when the
+        // input rows are not) a padded copy of the input rows
+        const size_t es = dtype_size(dtype_in);
+        o = align256(o + (size_t)nbatch * g.D * g.W * round_up(g.H, 8) * es);
+        l.volR = o;
+        if (dim3d && ((size_t)g.W * es) % 16 != 0)
+            o = align256(o + (size_t)nbatch * g.D * g.H * round_up(g.W, 8) * es);
+    }
     l.sinoS = o;
     if (dim3d && eff == OP_AT && g.type != GEO_PARALLEL)
         o = align256(o + (size_t)nbatch * V * g.Nv * g.Nu * sizeof(float));
@@ -149,9 +292,92 @@ float column_width(const Geom& g, int dim3d) {
     return (float)g.du;
 }
 
+GeomF make_geomf(const Geom& g, int dim3d) {
+    GeomF f;
+    f.x0 = (float)(-0.5 * g.W * g.dx + g.shx);
+    f.y0 = (float)(-0.5 * g.H * g.dy + g.shy);
+    f.xc0 = (float)((0.5 - 0.5 * g.W) * g.dx + g.shx);
+    f.yc0 = (float)((0.5 * g.H - 0.5) * g.dy + g.shy);
+    f.dx = (float)g.dx;
+    f.dy = (float)g.dy;
+    f.sod = (float)g.sod;
+    f.uscale = (dim3d && g.type == GEO_FLAT) ? (float)(g.sod / g.sdd) : 1.0f;
+    f.shu = (float)g.shu;
+    f.du = (float)g.du;
+    f.H = g.H;
+    f.Nu = g.Nu;
+    f.type = g.type;
+    return f;
+}
+
 constexpr int CELL_R = 8;
 constexpr int VOX_R = 16;
 constexpr int VOX_NW = 4;
+
+template <typename T> constexpr int dtype_code();
+template <> constexpr int dtype_code<float>() { return DT_F32; }
+template <> constexpr int dtype_code<__nv_bfloat16>() { return DT_BF16; }
+template <> constexpr int dtype_code<__half>() { return DT_F16; }
+
+template <typename TI, typename TO, int R, int MODE>
+int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr, const CUtensorMap& mc,
+                         const TI* rows, const TI* cols, int pitch_r, int pitch_c, TO* out, int nbatch, int nview,
+                         const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
+    auto kern = cell_tma3d_kernel<TI, TO, R, 2, MODE>;
+    const size_t smem = 2 * (((size_t)p.BP * p.BZ * sizeof(TI) + 127) / 128 * 128) + 16;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
+    const int RG = CELL_NW * R;
+    const int total = nview * nbatch;
+    for (int z0 = 0; z0 < total; z0 += 65535) {
+        const int nz = std::min(65535, total - z0);
+        dim3 grid((g.Nu + 31) / 32, (g.Nv + RG - 1) / RG, nz);
+        kern<<<grid, dim3(32, CELL_NW), smem, st>>>(g, vt, mr, mc, rows, cols, pitch_r, pitch_c, out, nview, z0, z0dz,
+                                                    zd0, dvv, cw, p.BP, p.BZ);
+        if (int rc = check_cuda("cell_tma3d")) return rc;
+    }
+    return XR_OK;
+}
+
+// Cell gather with TMA line windows; returns -1 when this configuration is
+// not covered (the caller then uses the plain kernel).
+template <typename TI, typename TO>
+int run_cell_tma(int eff, const Geom& g, const TI* in, TO* out, int nbatch, int nview, char* ws, const Layout& l,
+                 const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
+    if (!std::is_same<TO, TI>::value && !std::is_same<TO, float>::value) return -1;
+    if (reinterpret_cast<uintptr_t>(in) % 16 != 0) return -1;
+    const CellPlan p = plan_cell(g);
+    if (!p.ok || !encode_fn()) return -1;
+    const size_t es = sizeof(TI);
+    const int Hp = round_up(g.H, 8);
+    TI* cols = reinterpret_cast<TI*>(ws + l.volT);
+    dim3 tg((g.W + 31) / 32, (g.H + 31) / 32, g.D * nbatch);
+    transpose_flip_kernel<TI><<<tg, dim3(32, 8), 0, st>>>(in, cols, g.H, g.W, Hp);
+    if (int rc = check_cuda("transpose")) return rc;
+    const TI* rows = in;
+    int Wp = g.W;
+    if (((size_t)g.W * es) % 16 != 0) {
+        Wp = round_up(g.W, 8);
+        TI* vr = reinterpret_cast<TI*>(ws + l.volR);
+        const size_t nrows = (size_t)nbatch * g.D * g.H;
+        const size_t n = nrows * g.W;
+        pad_rows_kernel<TI><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, vr, g.W, Wp, nrows);
+        if (int rc = check_cuda("pad_rows")) return rc;
+        rows = vr;
+    }
+    CUtensorMap mr, mc;
+    if (!encode_line_map(&mr, dtype_code<TI>(), rows, g.W, g.H, g.D, nbatch, Wp, p.BP, p.BZ) ||
+        !encode_line_map(&mc, dtype_code<TI>(), cols, g.H, g.W, g.D, nbatch, Hp, p.BP, p.BZ))
+        return -1;
+    if (p.R == 16) {
+        if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 16, OP_A>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+        if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 16, OP_BT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+        return launch_cell_tma_mode<TI, TO, 16, OP_BWT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+    }
+    if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 8, OP_A>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+    if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 8, OP_BT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+    return launch_cell_tma_mode<TI, TO, 8, OP_BWT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+}
 
 template <typename TI, typename TO>
 int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nbatch, int nview,
@@ -179,9 +405,13 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
         else if (op == OP_BT || op == OP_BWT) eff = OP_A;
     }
     if (eff == OP_A || eff == OP_BT || eff == OP_BWT) {
+        if (!g_force_plain) {
+            const int rc = run_cell_tma(eff, g, in, out, nbatch, nview, ws, l, vt, st, z0dz, zd0, dvv, cw);
+            if (rc >= 0) return rc;
+        }
         TI* volT = reinterpret_cast<TI*>(ws + l.volT);
         dim3 tg((g.W + 31) / 32, (g.H + 31) / 32, g.D * nbatch);
-        transpose_flip_kernel<TI><<<tg, dim3(32, 8), 0, st>>>(in, volT, g.H, g.W);
+        transpose_flip_kernel<TI><<<tg, dim3(32, 8), 0, st>>>(in, volT, g.H, g.W, g.H);
         if (int rc = check_cuda("transpose")) return rc;
         const int nwarp = std::min(8, (g.Nv + CELL_R - 1) / CELL_R);
         const int rows_per_cta = nwarp * CELL_R;
@@ -206,7 +436,7 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
     if (g.H > 65535) return fail(XR_ERR_UNSUPPORTED, "image height above 65535");
     dim3 grid((g.W + 31) / 32, g.H, nzg * nbatch);
     dim3 block(32, VOX_NW);
-    const float uscale = (g.type == GEO_FLAT) ? (float)(g.sod / g.sdd) : 1.0f;
+    const GeomF gf = make_geomf(g, 1);
     const float atconst = (float)(g.dx * g.dy * g.dz / (g.du * g.dv));
     if (eff == OP_AT) {
         if (g.type != GEO_PARALLEL) {
@@ -215,17 +445,17 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
             prescale_at3d_kernel<TI><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(g, vt, in, sinoS, nview, total, zd0, dvv);
             if (int rc = check_cuda("prescale_at3d")) return rc;
             vox_gather3d_kernel<float, TO, VOX_R, OP_AT><<<grid, block, 0, st>>>(
-                g, vt, sinoS, out, nview, nzg, z0dz, zd0, dvv, cw, uscale, atconst, oscale);
+                g, gf, vt, sinoS, out, nview, nzg, z0dz, zd0, dvv, cw, atconst, oscale);
         } else {
             vox_gather3d_kernel<TI, TO, VOX_R, OP_AT><<<grid, block, 0, st>>>(
-                g, vt, in, out, nview, nzg, z0dz, zd0, dvv, cw, uscale, atconst, oscale);
+                g, gf, vt, in, out, nview, nzg, z0dz, zd0, dvv, cw, atconst, oscale);
         }
     } else if (eff == OP_B) {
         vox_gather3d_kernel<TI, TO, VOX_R, OP_B><<<grid, block, 0, st>>>(
-            g, vt, in, out, nview, nzg, z0dz, zd0, dvv, cw, uscale, atconst, oscale);
+            g, gf, vt, in, out, nview, nzg, z0dz, zd0, dvv, cw, atconst, oscale);
     } else {
         vox_gather3d_kernel<TI, TO, VOX_R, OP_BW><<<grid, block, 0, st>>>(
-            g, vt, in, out, nview, nzg, z0dz, zd0, dvv, cw, uscale, atconst, oscale);
+            g, gf, vt, in, out, nview, nzg, z0dz, zd0, dvv, cw, atconst, oscale);
     }
     return check_cuda("vox_gather3d");
 }
@@ -251,7 +481,7 @@ int run2d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
     if (op == OP_A || op == OP_BT || op == OP_BWT) {
         TI* imgT = reinterpret_cast<TI*>(ws + l.volT);
         dim3 tg((g.W + 31) / 32, (g.H + 31) / 32, nbatch);
-        transpose_flip_kernel<TI><<<tg, dim3(32, 8), 0, st>>>(in, imgT, g.H, g.W);
+        transpose_flip_kernel<TI><<<tg, dim3(32, 8), 0, st>>>(in, imgT, g.H, g.W, g.H);
         if (int rc = check_cuda("transpose")) return rc;
         dim3 grid((g.Nu + 127) / 128, nview, nbatch);
         if (op == OP_A)
@@ -296,7 +526,10 @@ int apply(int dim3d, int op, const Geom& g, const void* in, int dti, void* out, 
           int nbatch, int nview, void* workspace, size_t ws_bytes, void* stream, float oscale) {
     if (int rc = validate(g, dim3d, op, nbatch, nview)) return rc;
     if (!dtype_ok(dti) || !dtype_ok(dto)) return fail(XR_ERR_INVALID_ARGUMENT, "unsupported dtype (%d, %d)", dti, dto);
-    if (!in || !out) return fail(XR_ERR_INVALID_ARGUMENT, "null input or output pointer");
+    // With zero views the sinogram side is empty and may be a null pointer.
+    const bool sino_in = (op == OP_AT || op == OP_B || op == OP_BW);
+    if ((!in && !(sino_in && nview == 0)) || (!out && !(!sino_in && nview == 0)))
+        return fail(XR_ERR_INVALID_ARGUMENT, "null input or output pointer");
     if (nview > 0 && !ang) return fail(XR_ERR_INVALID_ARGUMENT, "null angles pointer");
     const Layout l = layout(dim3d, op, g, nbatch, nview, dti);
     if (!workspace || ws_bytes < l.total)
@@ -372,6 +605,36 @@ int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, i
 }
 
 const char* xr_last_error(void) { return xr::g_last_error.c_str(); }
+
+int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, int* rows_per_thread) {
+    if (!geom || !ok || !box_pixels || !box_z || !rows_per_thread)
+        return xr::fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
+    const xr::Geom g = xr::geom_from(geom);
+    if (int rc = xr::validate(g, 1, 0, 1, 1)) return rc;
+    const xr::CellPlan p = xr::plan_cell(g);
+    *ok = p.ok;
+    *box_pixels = p.BP;
+    *box_z = p.BZ;
+    *rows_per_thread = p.R;
+    return XR_OK;
+}
+
+int xr_set_plain_kernels(int on) {
+    xr::g_force_plain = (on != 0);
+    return XR_OK;
+}
+
+int xr_device_error(unsigned int* code, int clear) {
+    if (!code) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
+    if (cudaMemcpyFromSymbol(code, xr::g_device_error, sizeof(unsigned int)) != cudaSuccess)
+        return xr::fail(XR_ERR_CUDA, "reading the device error word failed");
+    if (clear) {
+        const unsigned int zero = 0;
+        if (cudaMemcpyToSymbol(xr::g_device_error, &zero, sizeof(unsigned int)) != cudaSuccess)
+            return xr::fail(XR_ERR_CUDA, "clearing the device error word failed");
+    }
+    return XR_OK;
+}
 
 const char* xr_version(void) { return "xrecon_b200 0.1.0 (sm_100a)"; }
 

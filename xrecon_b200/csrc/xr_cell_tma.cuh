@@ -1,0 +1,298 @@
+// Cell gather (A, B^T, Bw^T) with TMA-staged line windows.
+//
+// CTA = (view, 32 consecutive detector columns in traversal order, a group of
+// NW*R detector rows).  Lane = column, warp = run of R rows.  The CTA sweeps
+// the image lines; for every line the voxels its rays can touch form a window
+// [p0, p0+BP) x [z0, z0+BZ) of (pixel along the line) x (z) that a single
+// thread loads with one tiled TMA box (double buffered, one line ahead of
+// the consumers; out-of-volume coordinates arrive as zeros).  Each thread then
+// merges the z voxels of its column's pixel band against its R rows from
+// shared memory, without bounds checks.  A line whose window does not fit the
+// box (only for geometries far from the planned ones) falls back to global
+// loads for that line.
+//
+// The window is a uniform function of the line index, evaluated identically
+// by the producer thread (for line L+2) and by every consumer (for line L):
+//   pixels: floor(pos_k0(L)) rounded down to a multiple of 8 (the TMA
+//           alignment of the innermost coordinate) .. ceil(pos_kend(L)) - 1,
+//   z:      floor(min t) .. floor(max t) over the CTA's columns and rows,
+//           t = Q_k q(L) zd_r - z0/dz, extremes at Qmin/Qmax and the group's
+//           first/last row boundary.
+#pragma once
+
+#include "xr_kernels.cuh"
+#include "xr_tma.cuh"
+
+namespace xr {
+
+template <typename TI>
+__device__ __forceinline__ float lds(const TI* p);
+template <> __device__ __forceinline__ float lds<float>(const float* p) { return *p; }
+template <> __device__ __forceinline__ float lds<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+template <> __device__ __forceinline__ float lds<__half>(const __half* p) { return __half2float(*p); }
+
+template <typename TI, int NB>
+__device__ __forceinline__ float band_smem(const TI* p, const float (&w)[NB], int np) {
+    float s = w[0] * lds(p);
+#pragma unroll
+    for (int i = 1; i < NB; ++i)
+        if (i < np) s = fmaf(w[i], lds(p + i), s);
+    return s;
+}
+
+struct CellWindow {
+    int p0, z0, zlast, empty, ok;
+};
+
+struct CellCtaGeo {
+    double bAk0, bBk0, bAke, bBke;  // first / last boundary of the CTA's columns
+    double Qmin, Qmax;              // extremes of Q_k over the CTA's columns
+    double zlo, zhi;                // unmagnified z of the row group's first / last boundary
+};
+
+// Window of line L, clamped to the image: pixels [0, npix), z [-1, D] (the
+// rows -1 and D arrive as zeros from the TMA out-of-bounds fill and bound the
+// voxel walks).  One voxel of margin on each side of the z range absorbs
+// rounding between the window bound and each thread's own t values.
+__host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const ViewHdr& h, int L, double z0dz,
+                                                  int npix, int D, int BP, int BZ) {
+    CellWindow w;
+    w.ok = 1;
+    w.empty = 0;
+    const double pl = fma(c.bBk0, (double)L, c.bAk0);
+    const double ph = fma(c.bBke, (double)L, c.bAke);
+    const double q = fma(h.q1, (double)L, h.q0);
+    const double g0 = c.Qmin * q, g1 = c.Qmax * q;
+    const double a0 = g0 * c.zlo, a1 = g1 * c.zlo, b0 = g0 * c.zhi, b1 = g1 * c.zhi;
+    const double tl = fmin(fmin(a0, a1), fmin(b0, b1)) - z0dz;
+    const double th = fmax(fmax(a0, a1), fmax(b0, b1)) - z0dz;
+    if (!(pl > -1.0e8 && ph < 1.0e8 && tl > -1.0e8 && th < 1.0e8)) {
+        w.p0 = w.z0 = w.zlast = 0;
+        w.ok = 0;
+        return w;
+    }
+    const int plo = max((int)floor(pl), 0);
+    const int phi = min((int)ceil(ph) - 1, npix - 1);
+    w.p0 = plo & ~7;
+    w.z0 = max((int)floor(tl) - 1, -1);
+    w.zlast = min((int)floor(th) + 1, D);
+    w.empty = (plo > phi) || (w.z0 > w.zlast);
+    w.ok = !w.empty && (phi - w.p0 < BP) && (w.zlast - w.z0 + 1 <= BZ);
+    return w;
+}
+
+template <typename TI, typename TO, int R, int NB, int MODE>
+__global__ void __launch_bounds__(256, 2)
+cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUtensorMap map_rows,
+                  const __grid_constant__ CUtensorMap map_cols, const TI* __restrict__ fb_rows,
+                  const TI* __restrict__ fb_cols, const int pitch_rows, const int pitch_cols,
+                  TO* __restrict__ sino, const int nview, const int view0, const double z0dz, const double zd0,
+                  const double dvv, const float cw, const int BP, const int BZ) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // each stage starts on a 128-byte boundary (TMA destination alignment)
+    const int stage_elems = (int)(((size_t)BP * BZ * sizeof(TI) + 127) / 128 * 128 / sizeof(TI));
+    TI* stage = reinterpret_cast<TI*>(smem_raw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)2 * stage_elems * sizeof(TI));
+
+    const int lane = threadIdx.x, tid = threadIdx.y * 32 + threadIdx.x;
+    const int Nu = g.Nu;
+    const int k0 = blockIdx.x * 32;
+    const int k = k0 + lane;
+    const int kc = min(k, Nu - 1);
+    const int rows_per_cta = blockDim.y * R;
+    const int rg0 = blockIdx.y * rows_per_cta;
+    const int r0 = rg0 + threadIdx.y * R;
+    const int vb = blockIdx.z + view0;
+    const int v = vb % nview, b = vb / nview;
+    const bool active = (k < Nu) && (r0 < g.Nv);
+
+    const ViewHdr h = vt.hdr[v];
+    const int use_x = h.use_x, nlines = h.nlines, npix = h.npix;
+    const size_t ob = (size_t)v * (Nu + 1);
+    const double bA0 = vt.bA[ob + kc], bB0 = vt.bB[ob + kc];
+    const double bA1 = vt.bA[ob + kc + 1], bB1 = vt.bB[ob + kc + 1];
+    const double Qk = vt.colQ[(size_t)v * Nu + kc];
+
+    CellCtaGeo cg;
+    {
+        const int kend = min(k0 + 32, Nu);
+        cg.bAk0 = vt.bA[ob + k0];
+        cg.bBk0 = vt.bB[ob + k0];
+        cg.bAke = vt.bA[ob + kend];
+        cg.bBke = vt.bB[ob + kend];
+        double qmn = Qk, qmx = Qk;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            qmn = fmin(qmn, __shfl_xor_sync(0xffffffffu, qmn, o));
+            qmx = fmax(qmx, __shfl_xor_sync(0xffffffffu, qmx, o));
+        }
+        cg.Qmin = qmn;
+        cg.Qmax = qmx;
+        cg.zlo = zd0 + rg0 * dvv;
+        cg.zhi = zd0 + (rg0 + rows_per_cta) * dvv;
+    }
+    const CUtensorMap* map = use_x ? &map_rows : &map_cols;
+    const TI* __restrict__ fb = use_x ? fb_rows : fb_cols;
+    const int pitch = use_x ? pitch_rows : pitch_cols;
+    const size_t fb_plane = (size_t)nlines * pitch;
+    const TI* __restrict__ fbb = fb + (size_t)b * g.D * fb_plane;
+    const unsigned box_bytes = (unsigned)((size_t)BP * BZ * sizeof(TI));
+
+    auto issue = [&](int L, int s) {
+        const CellWindow w = cell_window(cg, h, L, z0dz, npix, g.D, BP, BZ);
+        if (w.ok) {
+            mbar_arrive_expect_tx(&bar[s], box_bytes);
+            tma_load_4d(stage + (size_t)s * stage_elems, map, w.p0, L, w.z0, b, &bar[s]);
+        } else {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar[s])) : "memory");
+        }
+    };
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        issue(0, 0);
+        if (nlines > 1) issue(1, 1);
+    }
+
+    float acc[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = 0.0f;
+    const double zr0 = zd0 + r0 * dvv;
+    const float dpdz = (float)(h.dpix * g.dz);
+
+    for (int L = 0; L < nlines; ++L) {
+        const int s = L & 1;
+        const unsigned parity = (unsigned)((L >> 1) & 1);
+        const CellWindow win = cell_window(cg, h, L, z0dz, npix, g.D, BP, BZ);
+        mbar_wait_bounded(&bar[s], parity);
+        if (active) {
+            const double pk = fma(bB0, (double)L, bA0);
+            const double pk1 = fma(bB1, (double)L, bA1);
+            const int pa = max((int)floor(pk), 0);
+            const int pb = min((int)ceil(pk1) - 1, npix - 1);
+            const double q = fma(h.q1, (double)L, h.q0);
+            const double gq = Qk * q;
+            const double t0 = fma(gq, zr0, -z0dz);
+            const double bt = gq * dvv;
+            const bool live = !win.empty && (pa <= pb) && (bt > 1.0e-4 && bt < 1.0e4) &&
+                              !(t0 + R * bt <= 0.0 || t0 >= (double)g.D);
+            if (live) {
+                const double jf = floor(t0);
+                const int j0 = (int)jf;
+                const float f = (float)(t0 - jf);
+                const float bf = (float)bt;
+                float lf = cw;
+                if (MODE == OP_A) {
+                    const float qf = (float)q;
+                    lf = dpdz / (qf * qf);
+                }
+                const float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
+                for (int pc = pa; pc <= pb; pc += NB) {
+                    const int np = min(NB, pb - pc + 1);
+                    const float off = (float)(pc - pa);
+                    float w[NB];
+#pragma unroll
+                    for (int i = 0; i < NB; ++i) {
+                        float wi = 0.0f;
+                        if (i < np) {
+                            wi = (fminf(off + (float)(i + 1), u1) - fmaxf(off + (float)i, u0)) * lf;
+                            if (MODE == OP_BWT) {
+                                float px, py;
+                                pixel_center(g, h, L, pc + i, px, py);
+                                wi *= fbp_weight(g, h, px, py);
+                            }
+                        }
+                        w[i] = wi;
+                    }
+                    float pos = f, jn = 1.0f, vj;
+                    if (win.ok) {
+                        // Staged voxels win.z0 .. win.zlast; below the window a
+                        // single virtual zero voxel ends at win.z0, past
+                        // win.zlast the value is zero and the next boundary
+                        // infinite.
+                        const TI* sbase = stage + (size_t)s * stage_elems + (pc - win.p0);
+                        const TI* ptr;
+                        int jabs;
+                        if (j0 >= win.z0) {
+                            jabs = j0;
+                            ptr = sbase + (size_t)(j0 - win.z0) * BP;
+                            vj = band_smem<TI, NB>(ptr, w, np);
+                        } else {
+                            jabs = win.z0 - 1;
+                            ptr = sbase - BP;  // address only, advanced before any read
+                            vj = 0.0f;
+                            jn = (float)(win.z0 - j0);
+                        }
+#pragma unroll
+                        for (int i = 0; i < R; ++i) {
+                            const float top = fmaf(bf, (float)(i + 1), f);
+                            float a = 0.0f;
+                            while (jn < top) {
+                                a = fmaf(jn - pos, vj, a);
+                                pos = jn;
+                                ++jabs;
+                                ptr += BP;
+                                if (jabs <= win.zlast) { vj = band_smem<TI, NB>(ptr, w, np); jn += 1.0f; }
+                                else { vj = 0.0f; jn = 3.0e38f; }
+                            }
+                            if (top > pos) { a = fmaf(top - pos, vj, a); pos = top; }
+                            acc[i] += a;
+                        }
+                    } else {
+                        // global fallback with bounds checks
+                        const TI* base = fbb + (size_t)L * pitch + pc;
+                        int j = j0;
+                        vj = ((unsigned)j < (unsigned)g.D) ? band_at(base + (size_t)j * fb_plane, w, np) : 0.0f;
+#pragma unroll
+                        for (int i = 0; i < R; ++i) {
+                            const float top = fmaf(bf, (float)(i + 1), f);
+                            float a = 0.0f;
+                            while (jn < top) {
+                                a = fmaf(jn - pos, vj, a);
+                                pos = jn;
+                                ++j;
+                                jn += 1.0f;
+                                vj = ((unsigned)j < (unsigned)g.D) ? band_at(base + (size_t)j * fb_plane, w, np) : 0.0f;
+                            }
+                            if (top > pos) { a = fmaf(top - pos, vj, a); pos = top; }
+                            acc[i] += a;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && L + 2 < nlines) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(L + 2, s);
+        }
+    }
+
+    if (!active) return;
+    const int col = h.keep ? k : Nu - 1 - k;
+    TO* out = sino + (((size_t)b * nview + v) * g.Nv) * Nu + col;
+    float E = 1.0f, F = 0.0f, M = 0.0f;
+    if (MODE == OP_A) {
+        const size_t oc = (size_t)v * Nu + k;
+        E = vt.colE[oc]; F = vt.colF[oc]; M = vt.colM[oc];
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int r = r0 + i;
+        if (r < g.Nv) {
+            float sv = acc[i];
+            if (MODE == OP_A) {
+                const float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+                sv *= E * sqrtf(F + zc * zc);
+            }
+            st(out + (size_t)r * Nu, sv);
+        }
+    }
+}
+
+}  // namespace xr

@@ -94,18 +94,62 @@ __device__ __forceinline__ void view_decisions(float ang, int& use_x, int& keep)
     keep = use_x ? (cf >= 0.0f) : (sf >= 0.0f);
 }
 
-__device__ __forceinline__ double sigma(int keep, double k, int nu) {
+// Fill the per-view header.  On the device the axis decision is taken as the
+// reference CPU path takes it (see view_decisions); on the host (only used
+// for sizing staging windows) plain float arithmetic is used.
+__host__ __device__ inline void make_view_hdr(const Geom& g, float ang, ViewHdr& h) {
+#ifdef __CUDA_ARCH__
+    view_decisions(ang, h.use_x, h.keep);
+#else
+    const float cf = (float)cos((double)ang), sf = (float)sin((double)ang);
+    h.use_x = cf * cf > 0.5f;
+    h.keep = h.use_x ? (cf >= 0.0f) : (sf >= 0.0f);
+#endif
+    h.beta = (double)ang;
+    h.s = sin(h.beta);
+    h.c = cos(h.beta);
+    h.sx = -h.s * g.sod;
+    h.sy = h.c * g.sod;
+    h.spar = h.use_x ? h.sx : h.sy;
+    h.sperp = h.use_x ? h.sy : h.sx;
+    h.nlines = h.use_x ? g.H : g.W;
+    h.npix = h.use_x ? g.W : g.H;
+    if (h.use_x) { h.perpA = (0.5 * g.H - 0.5) * g.dy + g.shy; h.perpB = -g.dy; }
+    else         { h.perpA = (0.5 - 0.5 * g.W) * g.dx + g.shx; h.perpB = g.dx; }
+    if (g.type == GEO_PARALLEL) { h.q0 = 1.0; h.q1 = 0.0; }
+    else { h.q0 = 1.0 - h.perpA / h.sperp; h.q1 = -h.perpB / h.sperp; }
+    h.dpix = h.use_x ? g.dx : g.dy;
+}
+
+// Column-centre z magnification M_k onto the axis plane (forward3d.cpp:258-297).
+__host__ __device__ inline double column_mag(const Geom& g, const ViewHdr& h, int k, double uscale) {
+    if (g.type == GEO_PARALLEL) return 1.0;
+    const double sgc = (h.keep ? ((double)k + 0.5 - 0.5 * g.Nu) : (0.5 * g.Nu - (double)k - 0.5));
+    double cx, cy;
+    if (g.type == GEO_FLAT) {
+        const double u = (sgc * g.du + g.shu) * uscale;
+        cx = u * h.c;
+        cy = u * h.s;
+    } else {
+        const double ac = sgc * g.du + g.shu + h.beta;
+        cx = sin(ac) * g.sdd + h.sx;
+        cy = -cos(ac) * g.sdd + h.sy;
+    }
+    return h.use_x ? h.sy / (h.sy - cy) : h.sx / (h.sx - cx);
+}
+
+__host__ __device__ __forceinline__ double sigma(int keep, double k, int nu) {
     return keep ? (k - 0.5 * nu) : (0.5 * nu - k);
 }
 
 // Intercept of the ray source -> point with the common axis (xrmath.h:8-22).
-__device__ __forceinline__ double map_point(const ViewHdr& h, double px, double py) {
+__host__ __device__ __forceinline__ double map_point(const ViewHdr& h, double px, double py) {
     if (h.use_x) return (h.sx * py - h.sy * px) / (py - h.sy);
     return (h.sy * px - h.sx * py) / (px - h.sx);
 }
 
 // Same for a ray leaving the source at angle a (xrmath.h:24-38).
-__device__ __forceinline__ double map_angle(const ViewHdr& h, double a) {
+__host__ __device__ __forceinline__ double map_angle(const ViewHdr& h, double a) {
     if (h.use_x) return h.sx + h.sy * tan(a);
     return h.sy + h.sx / tan(a);
 }
@@ -114,7 +158,7 @@ __device__ __forceinline__ double map_angle(const ViewHdr& h, double a) {
 //   flat: forward3d.cpp:229-243 (3D scales u by SOD/SDD; 2D du is already
 //         the isocentre spacing, projector.py:97) ; arc: forward3d.cpp:271-283 ;
 //   parallel: forward3d.cpp:53-56.
-__device__ __forceinline__ double boundary_axis(const Geom& g, const ViewHdr& h, double k, double uscale) {
+__host__ __device__ __forceinline__ double boundary_axis(const Geom& g, const ViewHdr& h, double k, double uscale) {
     const double sg = sigma(h.keep, k, g.Nu);
     if (g.type == GEO_FLAT) {
         const double u = (sg * g.du + g.shu) * uscale;
@@ -127,7 +171,7 @@ __device__ __forceinline__ double boundary_axis(const Geom& g, const ViewHdr& h,
 
 // Line-position coefficients of the ray through axis point D:
 // pos(L) = A + B * L in pixel units along line L.
-__device__ __forceinline__ void boundary_line_coeffs(const Geom& g, const ViewHdr& h, double D,
+__host__ __device__ __forceinline__ void boundary_line_coeffs(const Geom& g, const ViewHdr& h, double D,
                                                      double& A, double& B) {
     if (h.use_x) {
         const double pyA = (0.5 * g.H - 0.5) * g.dy + g.shy, pyB = -g.dy;

@@ -37,6 +37,16 @@ __device__ __forceinline__ float band_value(const TI* __restrict__ base, int j, 
     return s;
 }
 
+// Same sum at a pointer already positioned on voxel row j of the band.
+template <typename TI, int NB>
+__device__ __forceinline__ float band_at(const TI* __restrict__ p, const float (&w)[NB], int np) {
+    float s = w[0] * ld(p);
+#pragma unroll
+    for (int i = 1; i < NB; ++i)
+        if (i < np) s = fmaf(w[i], ld(p + i), s);
+    return s;
+}
+
 template <typename TI>
 __device__ __forceinline__ float row_value(const TI* __restrict__ colbase, int m, int Nv, int Nu) {
     if ((unsigned)m >= (unsigned)Nv) return 0.0f;
@@ -52,22 +62,7 @@ __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* _
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nview || k > g.Nu) return;
     ViewHdr h;
-    const float a = ang[v];
-    view_decisions(a, h.use_x, h.keep);
-    h.beta = (double)a;
-    h.s = sin(h.beta);
-    h.c = cos(h.beta);
-    h.sx = -h.s * g.sod;
-    h.sy = h.c * g.sod;
-    h.spar = h.use_x ? h.sx : h.sy;
-    h.sperp = h.use_x ? h.sy : h.sx;
-    h.nlines = h.use_x ? g.H : g.W;
-    h.npix = h.use_x ? g.W : g.H;
-    if (h.use_x) { h.perpA = (0.5 * g.H - 0.5) * g.dy + g.shy; h.perpB = -g.dy; }
-    else         { h.perpA = (0.5 - 0.5 * g.W) * g.dx + g.shx; h.perpB = g.dx; }
-    if (g.type == GEO_PARALLEL) { h.q0 = 1.0; h.q1 = 0.0; }
-    else { h.q0 = 1.0 - h.perpA / h.sperp; h.q1 = -h.perpB / h.sperp; }
-    h.dpix = h.use_x ? g.dx : g.dy;
+    make_view_hdr(g, ang[v], h);
     if (k == 0) vt.hdr[v] = h;
 
     const double uscale = (dim3d && g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
@@ -90,19 +85,7 @@ __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* _
         vt.colM[oc] = 0.0f;
         return;
     }
-    // Column centre and its z magnification: forward3d.cpp:258-297.
-    const double sgc = sigma(h.keep, (double)k + 0.5, g.Nu);
-    double cx, cy;
-    if (g.type == GEO_FLAT) {
-        const double u = (sgc * g.du + g.shu) * uscale;
-        cx = u * h.c;
-        cy = u * h.s;
-    } else {
-        const double ac = sgc * g.du + g.shu + h.beta;
-        cx = sin(ac) * g.sdd + h.sx;
-        cy = -cos(ac) * g.sdd + h.sy;
-    }
-    const double M = h.use_x ? h.sy / (h.sy - cy) : h.sx / (h.sx - cx);
+    const double M = column_mag(g, h, k, uscale);
     vt.colQ[oc] = M / g.dz;
     const double aa = 0.5 * (Dk + Dk1) - h.spar;
     const double F = aa * aa + h.sperp * h.sperp;
@@ -124,11 +107,11 @@ __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* _
 // that lines of the y-axis views (image columns) are contiguous in the
 // pixel coordinate p = H-1-iy.
 template <typename T>
-__global__ void transpose_flip_kernel(const T* __restrict__ in, T* __restrict__ out, int H, int W) {
+__global__ void transpose_flip_kernel(const T* __restrict__ in, T* __restrict__ out, int H, int W, int pitch) {
     __shared__ T tile[32][33];
     const size_t plane = (size_t)H * W;
     const T* src = in + (size_t)blockIdx.z * plane;
-    T* dst = out + (size_t)blockIdx.z * plane;
+    T* dst = out + (size_t)blockIdx.z * ((size_t)W * pitch);
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
     for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
         const int y = y0 + dy, x = x0 + threadIdx.x;
@@ -137,8 +120,19 @@ __global__ void transpose_flip_kernel(const T* __restrict__ in, T* __restrict__ 
     __syncthreads();
     for (int dx = threadIdx.y; dx < 32; dx += blockDim.y) {
         const int x = x0 + dx, y = y0 + threadIdx.x;
-        if (y < H && x < W) dst[(size_t)x * H + (H - 1 - y)] = tile[threadIdx.x][dx];
+        if (y < H && x < W) dst[(size_t)x * pitch + (H - 1 - y)] = tile[threadIdx.x][dx];
     }
+}
+
+// Copy image planes into a row pitch that is a multiple of 16 bytes (TMA
+// stride rule); the padding columns are never read inside the image.
+template <typename T>
+__global__ void pad_rows_kernel(const T* __restrict__ in, T* __restrict__ out, int W, int pitch, size_t nrows) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t row = i / W;
+    if (row >= nrows) return;
+    const int x = (int)(i % W);
+    out[row * pitch + x] = in[i];
 }
 
 // ------------------------------------------------------------- 3D kernels
@@ -148,7 +142,7 @@ __global__ void transpose_flip_kernel(const T* __restrict__ in, T* __restrict__ 
 // pixel band of its column (FP64 boundaries, FP32 weights) and merges the
 // z voxels of the band against its R rows in local coordinates.
 template <typename TI, typename TO, int R, int MODE>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ vol_rows,
                      const TI* __restrict__ vol_cols, TO* __restrict__ sino, const int nview,
                      const int view0, const double z0dz, const double zd0, const double dvv,
@@ -172,6 +166,7 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
 #pragma unroll
     for (int i = 0; i < R; ++i) acc[i] = 0.0f;
 
+    const float dpdz = (float)(h.dpix * g.dz);
     for (int L = 0; L < nlines; ++L) {
         const double pk = fma(bB0, (double)L, bA0);
         const double pk1 = fma(bB1, (double)L, bA1);
@@ -182,22 +177,29 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
         const double gq = Qk * q;
         const double t0 = fma(gq, zr0, -z0dz);
         const double bt = gq * dvv;
-        if (!(bt > 0.0 && bt < 1.0e6)) continue;
+        if (!(bt > 1.0e-4 && bt < 1.0e4)) continue;  // bounds every merge loop
         if (t0 + R * bt <= 0.0 || t0 >= (double)g.D) continue;
         const double jf = floor(t0);
         const int j0 = (int)jf;
         const float f = (float)(t0 - jf);
         const float bf = (float)bt;
-        const float lf = (MODE == OP_A) ? (float)(h.dpix * g.dz / (q * q)) : cw;
+        float lf = cw;
+        if (MODE == OP_A) {
+            const float qf = (float)q;
+            lf = dpdz / (qf * qf);
+        }
+        // band edges relative to the first pixel: small FP32 numbers
+        const float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
+        const TI* __restrict__ line = vol + (size_t)L * npix;
         for (int pc = pa; pc <= pb; pc += MAXB) {
             const int np = min(MAXB, pb - pc + 1);
+            const float off = (float)(pc - pa);
             float w[MAXB];
 #pragma unroll
             for (int i = 0; i < MAXB; ++i) {
                 float wi = 0.0f;
                 if (i < np) {
-                    const double pp = (double)(pc + i);
-                    wi = (float)(fmin(pp + 1.0, pk1) - fmax(pp, pk)) * lf;
+                    wi = (fminf(off + (float)(i + 1), u1) - fmaxf(off + (float)i, u0)) * lf;
                     if (MODE == OP_BWT) {
                         float px, py;
                         pixel_center(g, h, L, pc + i, px, py);
@@ -206,12 +208,25 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
                 }
                 w[i] = wi;
             }
-            const TI* __restrict__ base = vol + (size_t)L * npix + pc;
-            int m = 0;
+            // Voxel walk in local z coordinates (voxel j0+m spans [m, m+1]).
+            // Below the volume a single virtual zero voxel ends at voxel 0;
+            // past the top the value is zero and the next boundary infinite.
+            const TI* __restrict__ ptr;
+            int jabs;
+            float vj, jn;
             float pos = f;
-            if (j0 < 0) { m = -j0; pos = (float)m; }
-            float jn = (float)(m + 1);
-            float vj = band_value(base, j0 + m, plane, g.D, w, np);
+            if (j0 >= 0) {
+                jabs = j0;
+                ptr = line + (size_t)j0 * plane + pc;
+                vj = band_at(ptr, w, np);
+                jn = 1.0f;
+            } else {
+                // address of "voxel -1": only ever advanced to voxel 0, never read
+                jabs = -1;
+                ptr = line + pc - plane;
+                vj = 0.0f;
+                jn = (float)(-j0);
+            }
 #pragma unroll
             for (int i = 0; i < R; ++i) {
                 const float top = fmaf(bf, (float)(i + 1), f);
@@ -219,9 +234,10 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
                 while (jn < top) {
                     a = fmaf(jn - pos, vj, a);
                     pos = jn;
-                    ++m;
-                    jn += 1.0f;
-                    vj = band_value(base, j0 + m, plane, g.D, w, np);
+                    ++jabs;
+                    ptr += plane;
+                    if (jabs < g.D) { vj = band_at(ptr, w, np); jn += 1.0f; }
+                    else { vj = 0.0f; jn = 3.0e38f; }
                 }
                 if (top > pos) { a = fmaf(top - pos, vj, a); pos = top; }
                 acc[i] += a;
@@ -267,47 +283,90 @@ __global__ void prescale_at3d_kernel(const Geom g, const ViewTables vt, const TI
     out[idx] = ld(in + idx) * vt.colE[oc] * sqrtf(vt.colF[oc] + zc * zc);
 }
 
+// Float constants of the image grid and detector used by the FP32 column
+// guess and the FBP weight (exactness comes from the FP64 tables).
+struct GeomF {
+    float x0, y0;      // left / bottom image edge
+    float xc0, yc0;    // centre of column 0 / row 0 (row 0 is the top)
+    float dx, dy;
+    float sod, uscale, shu, du;
+    int H, Nu, type;
+};
+
+__device__ __forceinline__ float col_guess_f(const GeomF& gf, const ViewHdr& h, float x, float y) {
+    const float s = (float)h.s, c = (float)h.c;
+    float sg;
+    if (gf.type == GEO_FLAT) {
+        const float R = gf.sod;
+        const float u = R * (x * c + y * s) / (R + x * s - y * c);
+        sg = (u / gf.uscale - gf.shu) / gf.du;
+    } else if (gf.type == GEO_ARC) {
+        const float ac = (float)h.beta + gf.shu;
+        float dcx, dcy;
+        sincosf(ac, &dcx, &dcy);
+        dcy = -dcy;
+        const float ex = x - (float)h.sx, ey = y - (float)h.sy;
+        sg = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) / gf.du;
+    } else {
+        sg = (x * c + y * s - gf.shu) / gf.du;
+    }
+    return h.keep ? sg + 0.5f * gf.Nu : 0.5f * gf.Nu - sg;
+}
+
 // Voxel gather: lane = image column ix (32 consecutive), warp = run of R
 // voxels along z.  Each thread sweeps all views; per view it finds the
-// detector columns overlapping its pixel (FP32 guess, FP64 boundaries) and
-// merges its R voxels against the rows of each column.
+// detector columns overlapping its pixel (FP32 guess widened by one column
+// each side, exact FP64 boundaries) and merges its R voxels against the rows
+// of each column: voxels are the static loop, rows the dynamic one.  Below
+// the detector a single virtual zero row ends at row 0; past the top the
+// value is zero and the next boundary infinite.
 template <typename TI, typename TO, int R, int MODE>
 __global__ void __launch_bounds__(128)
-vox_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ sino, TO* __restrict__ vol,
-                    const int nview, const int nzg, const double z0dz, const double zd0, const double dvv,
-                    const float cw, const float uscale, const float atconst, const float oscale) {
+vox_gather3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const TI* __restrict__ sino,
+                    TO* __restrict__ vol, const int nview, const int nzg, const double z0dz, const double zd0,
+                    const double dvv, const float cw, const float atconst, const float oscale) {
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y;
     const int zg = blockIdx.z % nzg, b = blockIdx.z / nzg;
     const int j0 = (zg * blockDim.y + threadIdx.y) * R;
     if (ix >= g.W || j0 >= g.D) return;
     const int Nu = g.Nu, Nv = g.Nv;
+    const float dpdz = (float)(g.dz);
     float acc[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) acc[i] = 0.0f;
     const TI* __restrict__ sinob = sino + (size_t)b * nview * Nv * Nu;
+    const double dj0 = (double)j0;
 
     for (int v = 0; v < nview; ++v) {
-        const ViewHdr h = vt.hdr[v];
+        const ViewHdr& h = vt.hdr[v];
+        const int use_x = h.use_x, keep = h.keep;
         int L, p;
-        if (h.use_x) { L = iy; p = ix; } else { L = ix; p = g.H - 1 - iy; }
+        float xa, ya, xb, yb, px, py;
+        if (use_x) {
+            L = iy; p = ix;
+            ya = yb = py = gf.yc0 - (float)L * gf.dy;
+            xa = gf.x0 + (float)p * gf.dx;
+            xb = xa + gf.dx;
+            px = xa + 0.5f * gf.dx;
+        } else {
+            L = ix; p = g.H - 1 - iy;
+            xa = xb = px = gf.xc0 + (float)L * gf.dx;
+            ya = gf.y0 + (float)p * gf.dy;
+            yb = ya + gf.dy;
+            py = ya + 0.5f * gf.dy;
+        }
         const double q = fma(h.q1, (double)L, h.q0);
         float lf;
         if (MODE == OP_AT) {
-            lf = (g.type == GEO_PARALLEL) ? atconst : (float)(h.dpix * g.dz / (q * q));
+            if (g.type == GEO_PARALLEL) lf = atconst;
+            else { const float qf = (float)q; lf = (float)h.dpix * dpdz / (qf * qf); }
         } else {
             lf = cw;
-            if (MODE == OP_BW) {
-                float px, py;
-                pixel_center(g, h, L, p, px, py);
-                lf *= fbp_weight(g, h, px, py);
-            }
+            if (MODE == OP_BW) lf *= fbp_weight(g, h, px, py);
         }
         lf *= oscale;
-        float xa, ya, xb, yb;
-        line_point(g, h, L, (float)p, xa, ya);
-        line_point(g, h, L, (float)(p + 1), xb, yb);
-        float kf0 = col_guess(g, h, xa, ya, uscale), kf1 = col_guess(g, h, xb, yb, uscale);
+        const float kf0 = col_guess_f(gf, h, xa, ya), kf1 = col_guess_f(gf, h, xb, yb);
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const int ka = max(0, (int)floorf(lo) - 1);
@@ -317,29 +376,43 @@ vox_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ si
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
         const double* __restrict__ Q = vt.colQ + (size_t)v * Nu;
         const TI* __restrict__ sv = sinob + (size_t)v * Nv * Nu;
+        const double dp = (double)p;
         double pk = fma(bB[ka], (double)L, bA[ka]);
         for (int k = ka; k <= kb; ++k) {
             const double pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
-            const double wd = fmin((double)p + 1.0, pk1) - fmax((double)p, pk);
+            const float wf = (float)(fmin(dp + 1.0, pk1) - fmax(dp, pk));
             pk = pk1;
-            if (!(wd > 0.0)) continue;
+            if (!(wf > 0.0f)) continue;
             const double gq = Q[k] * q;
             const double T0 = fma(gq, zd0, -z0dz);
             const double bt = gq * dvv;
-            if (!(bt > 0.0 && bt < 1.0e6)) continue;
-            if (T0 >= (double)(j0 + R) || T0 + Nv * bt <= (double)j0) continue;
-            int rs = (int)floorf((float)((double)j0 - T0) / (float)bt);
-            double trs = fma((double)rs, bt, T0);
-            if (trs > (double)j0) { --rs; trs -= bt; }
-            else if (trs + bt <= (double)j0) { ++rs; trs += bt; }
-            const int col = h.keep ? k : Nu - 1 - k;
-            const TI* __restrict__ sc = sv + col;
-            const float wk = (float)wd * lf;
+            if (!(bt > 1.0e-4 && bt < 1.0e4)) continue;  // bounds every merge loop
+            if (T0 >= dj0 + R || T0 + Nv * bt <= dj0) continue;
             const float bf = (float)bt;
-            int m = rs;
+            const int col = keep ? k : Nu - 1 - k;
+            const TI* __restrict__ yp;
+            int m;
+            float y, rn;
+            if (T0 > dj0) {
+                // run starts below row 0: virtual zero row up to row 0
+                m = -1;
+                y = 0.0f;
+                rn = (float)(T0 - dj0);
+                yp = sv + col - Nu;  // address only; advanced to row 0 before any read
+            } else {
+                int rs = (int)floorf((float)(dj0 - T0) * __frcp_rn(bf));
+                double trs = fma((double)rs, bt, T0);
+                if (trs > dj0) { --rs; trs -= bt; }
+                else if (trs + bt <= dj0) { ++rs; trs += bt; }
+                if (rs > Nv - 1) { rs = Nv - 1; trs = fma((double)rs, bt, T0); }
+                if (rs < 0) { rs = 0; trs = T0; }
+                m = rs;
+                yp = sv + col + (size_t)rs * Nu;
+                y = ld(yp);
+                rn = (float)(trs - dj0) + bf;
+            }
+            const float wk = wf * lf;
             float pos = 0.0f;
-            float rn = (float)(trs - (double)j0) + bf;
-            float y = row_value(sc, m, Nv, Nu);
 #pragma unroll
             for (int i = 0; i < R; ++i) {
                 const float top = (float)(i + 1);
@@ -348,8 +421,9 @@ vox_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ si
                     a = fmaf(rn - pos, y, a);
                     pos = rn;
                     ++m;
-                    rn += bf;
-                    y = row_value(sc, m, Nv, Nu);
+                    yp += Nu;
+                    if (m < Nv) { y = ld(yp); rn += bf; }
+                    else { y = 0.0f; rn = 3.0e38f; }
                 }
                 a = fmaf(top - pos, y, a);
                 pos = top;

@@ -1,0 +1,72 @@
+// TMA (cp.async.bulk.tensor) and mbarrier helpers for sm_100a.
+//
+// Loads are plain tiled loads into this CTA's shared memory; no multicast
+// form is used anywhere.  Every wait on an mbarrier is bounded: after
+// XR_WAIT_LIMIT polls the wait gives up, records an error code in the
+// device-wide error word and returns false, so a kernel can never spin
+// forever on a transfer.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace xr {
+
+// Device-wide sticky error word (one per device that loads the library).
+// 0 = no error; kernels OR in a code when a bounded wait gives up.  Defined
+// here: the library is a single translation unit.
+__device__ unsigned int g_device_error = 0;
+
+constexpr unsigned XR_DEVERR_TMA_TIMEOUT = 1u;
+constexpr long long XR_WAIT_LIMIT = 1ll << 24;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Make barrier initialisation visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`; false (and the device error word
+// set) when the limit is reached.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    for (long long i = 0; i < XR_WAIT_LIMIT; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(&g_device_error, XR_DEVERR_TMA_TIMEOUT);
+    return false;
+}
+
+// 4D tiled TMA load of one box into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+}  // namespace xr
