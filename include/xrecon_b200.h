@@ -120,6 +120,25 @@ int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, in
  * kernels, so both paths can be compared. */
 int xr_set_plain_kernels(int on);
 
+/*
+ * Allocation-free variant of xr_dd2d (no reference counterpart: the
+ * reference allocates its outputs and scratch per call).  Same operators,
+ * layouts and results as xr_dd2d, but its scratch (per-view tables and the
+ * flipped image transpose) is a fixed static device array of
+ * XR_NOALLOC_SCRATCH_BYTES in the library, so the call never allocates or
+ * frees device memory.  Requests that need more scratch than that (see
+ * xr_dd2d_workspace_size) fail with XR_ERR_WORKSPACE.  Every scratch byte a
+ * call reads is first written by the same call, so nothing needs clearing.
+ * The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture.  There is one array per device: calls whose executions
+ * overlap (different streams, or threads) race on it and must be serialised
+ * by the caller.
+ */
+#define XR_NOALLOC_SCRATCH_BYTES (32u << 20)
+int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,
+                    const float* angles, int nbatch, int nview, void* stream);
+
 /* Human-readable message for the last non-OK status returned on this thread. */
 const char* xr_last_error(void);
 

@@ -58,6 +58,9 @@ def lib():
     L.xr_dd2d.argtypes = [c_int, ctypes.POINTER(Geom2d)] + common
     L.xr_dd3d.restype = c_int
     L.xr_dd3d.argtypes = [c_int, ctypes.POINTER(Geom3d)] + common
+    L.xr_dd2d_noalloc.restype = c_int
+    L.xr_dd2d_noalloc.argtypes = [c_int, ctypes.POINTER(Geom2d), c_void_p, c_int, c_void_p, c_int,
+                                  c_void_p, c_int, c_int, c_void_p]
     L.xr_fbp_filter.restype = c_int
     L.xr_fbp_filter.argtypes = [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int,
                                 c_void_p, c_void_p, c_void_p, c_void_p]

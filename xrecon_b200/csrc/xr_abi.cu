@@ -543,6 +543,28 @@ int apply(int dim3d, int op, const Geom& g, const void* in, int dti, void* out, 
     return dispatch_out<__half>(dim3d, op, g, in, out, dto, ang, nbatch, nview, ws, l, st, oscale);
 }
 
+// Fixed device scratch of xr_dd2d_noalloc.  Its address is looked up once per
+// device (cudaGetSymbolAddress) and cached; nothing is ever allocated for it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[XR_NOALLOC_SCRATCH_BYTES];
+
+int noalloc_scratch(void** ptr) {
+    static std::mutex mu;
+    static std::vector<void*> by_device;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(XR_ERR_CUDA, "cudaGetDevice failed");
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)by_device.size() <= dev) by_device.resize(dev + 1, nullptr);
+    if (!by_device[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(XR_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+        by_device[dev] = p;
+    }
+    *ptr = by_device[dev];
+    return XR_OK;
+}
+
 }  // namespace
 }  // namespace xr
 
@@ -634,6 +656,25 @@ int xr_device_error(unsigned int* code, int clear) {
             return xr::fail(XR_ERR_CUDA, "clearing the device error word failed");
     }
     return XR_OK;
+}
+
+int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,
+                    const float* angles, int nbatch, int nview, void* stream) {
+    if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
+    const xr::Geom g = xr::geom_from(geom);
+    if (int rc = xr::validate(g, 0, op, nbatch, nview)) return rc;
+    if (!xr::dtype_ok(dtype_in) || !xr::dtype_ok(dtype_out))
+        return xr::fail(XR_ERR_INVALID_ARGUMENT, "unsupported dtype (%d, %d)", dtype_in, dtype_out);
+    const size_t need = xr::layout(0, op, g, nbatch, nview, dtype_in).total;
+    if (need > (size_t)XR_NOALLOC_SCRATCH_BYTES)
+        return xr::fail(XR_ERR_WORKSPACE,
+                        "request needs %zu bytes of scratch; xr_dd2d_noalloc has a fixed %zu-byte scratch "
+                        "(use xr_dd2d with a caller workspace)",
+                        need, (size_t)XR_NOALLOC_SCRATCH_BYTES);
+    void* scratch = nullptr;
+    if (int rc = xr::noalloc_scratch(&scratch)) return rc;
+    return xr::apply(0, op, g, in, dtype_in, out, dtype_out, angles, nbatch, nview, scratch,
+                     (size_t)XR_NOALLOC_SCRATCH_BYTES, stream, 1.0f);
 }
 
 const char* xr_version(void) { return "xrecon_b200 0.1.0 (sm_100a)"; }
