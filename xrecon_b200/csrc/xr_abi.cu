@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "xr_cell_tma.cuh"
+#include "xr_vox_prefix.cuh"
 #include "../../include/xrecon_b200.h"
 
 
@@ -110,7 +111,7 @@ Geom geom_from(const xr_geom2d* p) {
 }
 
 struct Layout {
-    size_t hdr, bA, bB, colQ, colE, colF, colM, volT, volR, sinoS, total;
+    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, volT, volR, sinoS, total;
 };
 
 // ------------------------------------------------------ TMA staging plans
@@ -236,6 +237,7 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
     l.bA = o;    o = align256(o + V * (g.Nu + 1) * sizeof(double));
     l.bB = o;    o = align256(o + V * (g.Nu + 1) * sizeof(double));
     l.colQ = o;  o = align256(o + V * g.Nu * sizeof(double));
+    l.colR = o;  o = align256(o + V * g.Nu * sizeof(double));
     l.colE = o;  o = align256(o + V * g.Nu * sizeof(float));
     l.colF = o;  o = align256(o + V * g.Nu * sizeof(float));
     l.colM = o;  o = align256(o + V * g.Nu * sizeof(float));
@@ -255,9 +257,11 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
         if (dim3d && ((size_t)g.W * es) % 16 != 0)
             o = align256(o + (size_t)nbatch * g.D * g.H * round_up(g.W, 8) * es);
     }
+    // voxel-gather ops: the per-view row prefix tables (float2, Nv + 2 rows);
+    // the plain kernels' pre-scaled cone A^T sinogram reuses the region
     l.sinoS = o;
-    if (dim3d && eff == OP_AT && g.type != GEO_PARALLEL)
-        o = align256(o + (size_t)nbatch * V * g.Nv * g.Nu * sizeof(float));
+    if (dim3d && (eff == OP_AT || eff == OP_B || eff == OP_BW))
+        o = align256(o + (size_t)nbatch * V * (g.Nv + 2) * g.Nu * sizeof(float2));
     l.total = o;
     return l;
 }
@@ -268,6 +272,7 @@ ViewTables tables_at(char* ws, const Layout& l) {
     t.bA = reinterpret_cast<double*>(ws + l.bA);
     t.bB = reinterpret_cast<double*>(ws + l.bB);
     t.colQ = reinterpret_cast<double*>(ws + l.colQ);
+    t.colR = reinterpret_cast<double*>(ws + l.colR);
     t.colE = reinterpret_cast<float*>(ws + l.colE);
     t.colF = reinterpret_cast<float*>(ws + l.colF);
     t.colM = reinterpret_cast<float*>(ws + l.colM);
@@ -313,6 +318,8 @@ GeomF make_geomf(const Geom& g, int dim3d) {
 constexpr int CELL_R = 8;
 constexpr int VOX_R = 16;
 constexpr int VOX_NW = 4;
+constexpr int PFX_R = 16;
+constexpr int PFX_NWY = 8;
 
 template <typename T> constexpr int dtype_code();
 template <> constexpr int dtype_code<float>() { return DT_F32; }
@@ -438,6 +445,30 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
     dim3 block(32, VOX_NW);
     const GeomF gf = make_geomf(g, 1);
     const float atconst = (float)(g.dx * g.dy * g.dz / (g.du * g.dv));
+    if (!g_force_plain) {
+        float2* tab = reinterpret_cast<float2*>(ws + l.sinoS);
+        const int nbv = nbatch * nview;
+        dim3 pg((g.Nu + 127) / 128, std::min(nbv, 65535));
+        if (eff == OP_AT && g.type != GEO_PARALLEL)
+            row_prefix3d_kernel<TI, true><<<pg, 128, 0, st>>>(g, vt, in, tab, nview, nbv, zd0, dvv);
+        else
+            row_prefix3d_kernel<TI, false><<<pg, 128, 0, st>>>(g, vt, in, tab, nview, nbv, zd0, dvv);
+        if (int rc = check_cuda("row_prefix3d")) return rc;
+        const int nzp = (g.D + PFX_R - 1) / PFX_R;
+        if ((long long)nzp * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
+        dim3 pgrid((g.W + 31) / 32, (g.H + PFX_NWY - 1) / PFX_NWY, nzp * nbatch);
+        dim3 pblock(32, PFX_NWY);
+        if (eff == OP_AT)
+            vox_prefix3d_kernel<TO, PFX_R, PFX_NWY, OP_AT><<<pgrid, pblock, 0, st>>>(
+                g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, cw, atconst, oscale);
+        else if (eff == OP_B)
+            vox_prefix3d_kernel<TO, PFX_R, PFX_NWY, OP_B><<<pgrid, pblock, 0, st>>>(
+                g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, cw, atconst, oscale);
+        else
+            vox_prefix3d_kernel<TO, PFX_R, PFX_NWY, OP_BW><<<pgrid, pblock, 0, st>>>(
+                g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, cw, atconst, oscale);
+        return check_cuda("vox_prefix3d");
+    }
     if (eff == OP_AT) {
         if (g.type != GEO_PARALLEL) {
             float* sinoS = reinterpret_cast<float*>(ws + l.sinoS);

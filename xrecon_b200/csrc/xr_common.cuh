@@ -55,13 +55,14 @@ struct ViewHdr {
 // Per-view tables, structure of arrays, view-major.
 //   pos_k(L) = bA[k] + bB[k] * L : position of detector boundary k (traversal
 //              order) on line L in pixel units, k = 0..Nu
-//   colQ[k]  = M_k / dz (3D) ; colE, colF, colM: cell scale of A,
+//   colQ[k]  = M_k / dz (3D), colR[k] = 1 / colQ[k] ; colE, colF, colM: cell scale of A,
 //              s_A(k, r) = colE[k] * sqrt(colF[k] + (colM[k] * zc_r)^2)
 struct ViewTables {
     ViewHdr* hdr;
     double* bA;
     double* bB;
     double* colQ;
+    double* colR;
     float* colE;
     float* colF;
     float* colM;

@@ -80,6 +80,7 @@ __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* _
     if (g.type == GEO_PARALLEL) {
         // forward3d.cpp:58,98 (xy_scale / dv) and system_matrix2d.cpp:109.
         vt.colQ[oc] = 1.0 / g.dz;
+        vt.colR[oc] = g.dz;
         vt.colE[oc] = (float)(dim3d ? dperp / (g.du * g.dv) : dperp / g.du);
         vt.colF[oc] = 1.0f;
         vt.colM[oc] = 0.0f;
@@ -87,6 +88,7 @@ __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* _
     }
     const double M = column_mag(g, h, k, uscale);
     vt.colQ[oc] = M / g.dz;
+    vt.colR[oc] = g.dz / M;
     const double aa = 0.5 * (Dk + Dk1) - h.spar;
     const double F = aa * aa + h.sperp * h.sperp;
     if (dim3d) {

@@ -1,0 +1,206 @@
+// Voxel gather (B, Bw, A^T) through per-view row prefix tables.
+//
+// The z part of the DD backprojection of one (voxel column, detector column)
+// pair is the overlap integral of the detector column y[r] (rows mapped to
+// voxel z units at t_r = T0 + r*bt) with each voxel [j, j+1]:
+//     Z(j) = bt * (G(u(j+1)) - G(u(j))),   u(z) = (z - T0) / bt,
+//     G(u) = P[floor u] + (u - floor u) * y[floor u],  P[r] = sum_{r'<r} y[r'],
+// the same sum the reference forms by merging row and voxel boundaries
+// (include/cpu3d_common.h:48-202, backward3d_flat.cu:7-128), written as a
+// difference of a piecewise-linear primitive.  Every voxel boundary costs one
+// table lookup, independent of the data, so a warp never diverges on the
+// number of rows a voxel overlaps.
+//
+// Table layout (one per batch element and view), float2 {P, y} indexed
+// [row t = r + 1][physical column], rows t = 0 .. Nv + 1:
+//     t = 0      : {P[0], 0}     (everything below row 0)
+//     t = r + 1  : {P[r], y[r]}
+//     t = Nv + 1 : {P[Nv], 0}    (everything above the last row)
+// so clamping u to [-1, Nv] makes G exact outside the detector.  P is summed
+// in FP64 and stored relative to the middle row (P[Nv/2] = 0), which halves
+// the magnitude the FP32 differences cancel against.
+#pragma once
+
+#include "xr_kernels.cuh"
+
+namespace xr {
+
+// One thread per (batch element x view, physical column).  MODE OP_AT with a
+// cone geometry folds the projection's cell scale s_A(k, r) into y, as
+// prescale_at3d_kernel does.
+template <typename TI, bool PRESCALE>
+__global__ void __launch_bounds__(128)
+row_prefix3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ in, float2* __restrict__ tab,
+                    const int nview, const int nbv, const double zd0, const double dvv) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Nu = g.Nu, Nv = g.Nv;
+    if (c >= Nu) return;
+    for (int bv = blockIdx.y; bv < nbv; bv += gridDim.y) {
+        const int v = bv % nview;
+        const TI* __restrict__ src = in + (size_t)bv * Nv * Nu + c;
+        float2* __restrict__ dst = tab + (size_t)bv * (Nv + 2) * Nu + c;
+        float E = 1.0f, F = 0.0f, M = 0.0f;
+        if (PRESCALE) {
+            const int k = vt.hdr[v].keep ? c : Nu - 1 - c;
+            const size_t oc = (size_t)v * Nu + k;
+            E = vt.colE[oc]; F = vt.colF[oc]; M = vt.colM[oc];
+        }
+        auto value = [&](int r) -> float {
+            const float y = ld(src + (size_t)r * Nu);
+            if (!PRESCALE) return y;
+            const float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+            return y * E * sqrtf(F + zc * zc);
+        };
+        double half = 0.0;
+        for (int r = 0; r < Nv / 2; ++r) half += (double)value(r);
+        double run = -half;
+        dst[0] = make_float2((float)run, 0.0f);
+        for (int r = 0; r < Nv; ++r) {
+            const float y = value(r);
+            dst[(size_t)(r + 1) * Nu] = make_float2((float)run, y);
+            run += (double)y;
+        }
+        dst[(size_t)(Nv + 1) * Nu] = make_float2((float)run, 0.0f);
+    }
+}
+
+// FP32 detector-column guess for a point (traversal order, fractional
+// boundary index).  Only used to bracket the columns a pixel overlaps; the
+// overlaps themselves come from the FP64 boundary tables.  (dcx, dcy) is the
+// arc detector's central direction for this view.
+__device__ __forceinline__ float col_guess_fast(const GeomF& gf, const ViewHdr& h, float s, float c, float dcx,
+                                                float dcy, float x, float y) {
+    float sg;
+    if (gf.type == GEO_FLAT) {
+        const float R = gf.sod;
+        const float u = __fdividef(R * (x * c + y * s), R + x * s - y * c);
+        sg = (u / gf.uscale - gf.shu) / gf.du;
+    } else if (gf.type == GEO_ARC) {
+        const float ex = x - (float)h.sx, ey = y - (float)h.sy;
+        sg = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) / gf.du;
+    } else {
+        sg = (x * c + y * s - gf.shu) / gf.du;
+    }
+    return h.keep ? sg + 0.5f * gf.Nu : 0.5f * gf.Nu - sg;
+}
+
+// Voxel gather through the prefix tables.  CTA = 32 x NWY pixels of the image
+// plane (lane = x, warp = y) times one run of R voxels along z per thread, so
+// the warps of a CTA read overlapping parts of each view's table; the view
+// loop is inside the kernel, so each voxel is written once and no atomics are
+// needed.
+//   MODE OP_B  : T_vox weight cw / ((X_hi - X_lo) Mv dz) in pixel units
+//   MODE OP_BW : OP_B times the FBP distance weight of the voxel centre
+//   MODE OP_AT : adjoint of the projection (cone: the table holds the
+//                pre-scaled sinogram; the line factor dpix dz / q^2)
+template <typename TO, int R, int NWY, int MODE>
+__global__ void __launch_bounds__(32 * NWY)
+vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const float2* __restrict__ tab,
+                    TO* __restrict__ vol, const int nview, const int nzg, const double z0dz, const double zd0,
+                    const double dvv, const float cw, const float atconst, const float oscale) {
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * NWY + threadIdx.y;
+    const int zg = blockIdx.z % nzg, b = blockIdx.z / nzg;
+    const int j0 = zg * R;
+    if (ix >= g.W || iy >= g.H || j0 >= g.D) return;
+    const int Nu = g.Nu, Nv = g.Nv;
+    const size_t vstride = (size_t)(Nv + 2) * Nu;
+    const float2* __restrict__ tb = tab + (size_t)b * nview * vstride;
+    const double zs = (double)j0 + z0dz;  // run bottom, in voxel units from z = 0
+    const double zoff = zd0 / dvv;        // u0 = zs * (rows per voxel) - zoff
+    const float dpdz = (float)g.dz;
+    float acc[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = 0.0f;
+
+    for (int v = 0; v < nview; ++v) {
+        const ViewHdr& h = vt.hdr[v];
+        const int keep = h.keep;
+        int L, p;
+        float xa, ya, xb, yb, px, py;
+        if (h.use_x) {
+            L = iy; p = ix;
+            ya = yb = py = gf.yc0 - (float)L * gf.dy;
+            xa = gf.x0 + (float)p * gf.dx;
+            xb = xa + gf.dx;
+            px = xa + 0.5f * gf.dx;
+        } else {
+            L = ix; p = g.H - 1 - iy;
+            xa = xb = px = gf.xc0 + (float)L * gf.dx;
+            ya = gf.y0 + (float)p * gf.dy;
+            yb = ya + gf.dy;
+            py = ya + 0.5f * gf.dy;
+        }
+        const double q = fma(h.q1, (double)L, h.q0);
+        const double mvdv = __drcp_rn(q * dvv);  // rows per voxel = mvdv * colR[k]
+        float lf;
+        if (MODE == OP_AT) {
+            if (g.type == GEO_PARALLEL) lf = atconst;
+            else { const float qf = (float)q; lf = (float)h.dpix * dpdz / (qf * qf); }
+        } else {
+            lf = cw;
+            if (MODE == OP_BW) lf *= fbp_weight(g, h, px, py);
+        }
+        lf *= oscale;
+        const float sf = (float)h.s, cf = (float)h.c;
+        float dcx = 0.0f, dcy = 0.0f;
+        if (gf.type == GEO_ARC) {
+            sincosf((float)h.beta + gf.shu, &dcx, &dcy);
+            dcy = -dcy;
+        }
+        const float kf0 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xa, ya);
+        const float kf1 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xb, yb);
+        const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const int ka = max(0, (int)floorf(lo - 0.5f));
+        const int kb = min(Nu - 1, (int)floorf(hi + 0.5f));
+        if (ka > kb) continue;
+        const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
+        const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
+        const double* __restrict__ Rq = vt.colR + (size_t)v * Nu;
+        const float2* __restrict__ tv = tb + (size_t)v * vstride;
+        const double dp = (double)p;
+        float pkl = (float)(fma(bB[ka], (double)L, bA[ka]) - dp);  // boundary relative to the pixel
+        for (int k = ka; k <= kb; ++k) {
+            const float pk1 = (float)(fma(bB[k + 1], (double)L, bA[k + 1]) - dp);
+            const float wf = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
+            pkl = pk1;
+            if (!(wf > 0.0f)) continue;
+            const double ib = mvdv * Rq[k];  // detector rows per voxel
+            if (!(ib > 1.0e-4 && ib < 1.0e4)) continue;
+            const double u0 = fma(zs, ib, -zoff);
+            if (u0 >= (double)Nv || u0 + R * ib <= 0.0) continue;
+            const double fl = floor(u0);
+            const int r0 = (int)fl;
+            const float f0 = (float)(u0 - fl), fib = (float)ib;
+            const float ulo = (float)(-1 - r0), uhi = (float)(Nv - r0);
+            const int col = keep ? k : Nu - 1 - k;
+            // table row of local row 0 (absolute row r0) in this column
+            const float2* __restrict__ tc = tv + (ptrdiff_t)(r0 + 1) * Nu + col;
+            const float wk = wf * lf * __frcp_rn(fib);
+            float gprev;
+            {
+                const float uc = fminf(fmaxf(f0, ulo), uhi);
+                const float rl = floorf(uc);
+                const float2 e = __ldg(tc + (ptrdiff_t)((int)rl) * Nu);
+                gprev = fmaf(uc - rl, e.y, e.x);
+            }
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const float uc = fminf(fmaxf(fmaf((float)(i + 1), fib, f0), ulo), uhi);
+                const float rl = floorf(uc);
+                const float2 e = __ldg(tc + (ptrdiff_t)((int)rl) * Nu);
+                const float gi = fmaf(uc - rl, e.y, e.x);
+                acc[i] = fmaf(wk, gi - gprev, acc[i]);
+                gprev = gi;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int j = j0 + i;
+        if (j < g.D) st(vol + (((size_t)b * g.D + j) * g.H + iy) * g.W + ix, acc[i]);
+    }
+}
+
+}  // namespace xr
