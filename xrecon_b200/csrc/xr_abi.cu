@@ -445,7 +445,9 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
     dim3 block(32, VOX_NW);
     const GeomF gf = make_geomf(g, 1);
     const float atconst = (float)(g.dx * g.dy * g.dz / (g.du * g.dv));
-    if (!g_force_plain) {
+    // the prefix kernel addresses one view's table with 32-bit byte offsets
+    const bool prefix_ok = (double)(g.Nv + 2) * g.Nu * sizeof(float2) < 2147483648.0;
+    if (!g_force_plain && prefix_ok) {
         float2* tab = reinterpret_cast<float2*>(ws + l.sinoS);
         const int nbv = nbatch * nview;
         dim3 pg((g.Nu + 127) / 128, std::min(nbv, 65535));

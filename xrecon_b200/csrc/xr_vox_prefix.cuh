@@ -11,14 +11,18 @@
 // table lookup, independent of the data, so a warp never diverges on the
 // number of rows a voxel overlaps.
 //
-// Table layout (one per batch element and view), float2 {P, y} indexed
+// Table layout (one per batch element and view), float2 {C, y} indexed
 // [row t = r + 1][physical column], rows t = 0 .. Nv + 1:
-//     t = 0      : {P[0], 0}     (everything below row 0)
-//     t = r + 1  : {P[r], y[r]}
-//     t = Nv + 1 : {P[Nv], 0}    (everything above the last row)
-// so clamping u to [-1, Nv] makes G exact outside the detector.  P is summed
-// in FP64 and stored relative to the middle row (P[Nv/2] = 0), which halves
-// the magnitude the FP32 differences cancel against.
+//     t = 0      : {P[0], 0}                (everything below row 0)
+//     t = r + 1  : {P[r] + y[r] / 2, y[r]}  (primitive at the row's middle)
+//     t = Nv + 1 : {P[Nv], 0}               (everything above the last row)
+// so that G(u) = C[n] + (u - 1/2 - n) * y[n] for any n with |u - 1/2 - n| <= 1/2:
+// the row index may be taken as round-to-nearest(u - 1/2), which an FP32 add
+// of 1.5 * 2^23 yields on the FMA pipe (ties pick either neighbour; both give
+// the same G).  Clamping u - 1/2 to [-1, Nv - 1/2] makes G exact outside the
+// detector.  P is summed in FP64 and stored relative to the middle row
+// (P[Nv/2] = 0), which halves the magnitude the FP32 differences cancel
+// against.
 #pragma once
 
 #include "xr_kernels.cuh"
@@ -57,7 +61,7 @@ row_prefix3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ in
         dst[0] = make_float2((float)run, 0.0f);
         for (int r = 0; r < Nv; ++r) {
             const float y = value(r);
-            dst[(size_t)(r + 1) * Nu] = make_float2((float)run, y);
+            dst[(size_t)(r + 1) * Nu] = make_float2((float)(run + 0.5 * (double)y), y);
             run += (double)y;
         }
         dst[(size_t)(Nv + 1) * Nu] = make_float2((float)run, 0.0f);
@@ -104,10 +108,11 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
     const int j0 = zg * R;
     if (ix >= g.W || iy >= g.H || j0 >= g.D) return;
     const int Nu = g.Nu, Nv = g.Nv;
+    const unsigned Nu8 = (unsigned)Nu * 8u;
     const size_t vstride = (size_t)(Nv + 2) * Nu;
     const float2* __restrict__ tb = tab + (size_t)b * nview * vstride;
     const double zs = (double)j0 + z0dz;  // run bottom, in voxel units from z = 0
-    const double zoff = zd0 / dvv;        // u0 = zs * (rows per voxel) - zoff
+    const double zoffh = -zd0 / dvv - 0.5;  // u0 = zs * (rows per voxel) + zoffh
     const float dpdz = (float)g.dz;
     float acc[R];
 #pragma unroll
@@ -158,42 +163,72 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
         const double* __restrict__ Rq = vt.colR + (size_t)v * Nu;
-        const float2* __restrict__ tv = tb + (size_t)v * vstride;
-        const double dp = (double)p;
-        float pkl = (float)(fma(bB[ka], (double)L, bA[ka]) - dp);  // boundary relative to the pixel
-        for (int k = ka; k <= kb; ++k) {
-            const float pk1 = (float)(fma(bB[k + 1], (double)L, bA[k + 1]) - dp);
-            const float wf = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
+        const char* __restrict__ tvb = reinterpret_cast<const char*>(tb + (size_t)v * vstride);
+        const double dp = (double)p, dL = (double)L;
+        // first column whose right boundary lies right of the pixel's left edge
+        // (boundaries relative to the pixel, in pixel units)
+        int k = ka;
+        float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
+        float pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+        while (!(pk1 > 0.0f) && k < kb) {
+            ++k;
             pkl = pk1;
-            if (!(wf > 0.0f)) continue;
-            const double ib = mvdv * Rq[k];  // detector rows per voxel
-            if (!(ib > 1.0e-4 && ib < 1.0e4)) continue;
-            const double u0 = fma(zs, ib, -zoff);
-            if (u0 >= (double)Nv || u0 + R * ib <= 0.0) continue;
-            const double fl = floor(u0);
-            const int r0 = (int)fl;
-            const float f0 = (float)(u0 - fl), fib = (float)ib;
-            const float ulo = (float)(-1 - r0), uhi = (float)(Nv - r0);
-            const int col = keep ? k : Nu - 1 - k;
-            // table row of local row 0 (absolute row r0) in this column
-            const float2* __restrict__ tc = tv + (ptrdiff_t)(r0 + 1) * Nu + col;
-            const float wk = wf * lf * __frcp_rn(fib);
-            float gprev;
-            {
-                const float uc = fminf(fmaxf(f0, ulo), uhi);
-                const float rl = floorf(uc);
-                const float2 e = __ldg(tc + (ptrdiff_t)((int)rl) * Nu);
-                gprev = fmaf(uc - rl, e.y, e.x);
-            }
+            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+        }
+        // lanes now walk their overlapping columns in step, one per iteration
+        for (;;) {
+            const float wf = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
+            do {
+                if (!(wf > 0.0f)) break;
+                const double ib = mvdv * Rq[k];  // detector rows per voxel
+                if (!(ib > 1.0e-4 && ib < 1.0e4)) break;
+                // row coordinate of the run's bottom boundary, minus half a row
+                const double u0 = fma(zs, ib, zoffh);
+                if (u0 >= (double)Nv - 0.5 || u0 + R * ib <= -0.5) break;
+                const double t0 = u0 + 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer
+                const double n0 = t0 - 6755399441055744.0;
+                const int r0 = __double2loint(t0);
+                const float f0 = (float)(u0 - n0), fib = (float)ib;
+                const int col = keep ? k : Nu - 1 - k;
+                // Byte offset of the entry for local row n is
+                //   ((r0 + 1 + n) * Nu + col) * 8 = bits(n + 1.5 * 2^23) * Nu8 + K
+                // in 32-bit arithmetic (the table of one view is < 2 GiB).
+                const unsigned K = (unsigned)(r0 + 1) * Nu8 + (unsigned)col * 8u - 0x4B400000u * Nu8;
+                const float wk = wf * lf * __frcp_rn(fib);
+                // rows the run reaches (local), inside [0, Nv - 1] in every active lane?
+                const bool inside = (u0 >= 0.0) && (u0 + R * ib <= (double)Nv - 1.0);
+                float gprev = 0.0f;
+                if (__all_sync(__activemask(), inside)) {
 #pragma unroll
-            for (int i = 0; i < R; ++i) {
-                const float uc = fminf(fmaxf(fmaf((float)(i + 1), fib, f0), ulo), uhi);
-                const float rl = floorf(uc);
-                const float2 e = __ldg(tc + (ptrdiff_t)((int)rl) * Nu);
-                const float gi = fmaf(uc - rl, e.y, e.x);
-                acc[i] = fmaf(wk, gi - gprev, acc[i]);
-                gprev = gi;
-            }
+                    for (int i = 0; i <= R; ++i) {
+                        const float uc = fmaf((float)i, fib, f0);
+                        const float tr = uc + 12582912.0f;  // 1.5 * 2^23: round to nearest integer
+                        const float nf = tr - 12582912.0f;
+                        const float2 e = __ldg(reinterpret_cast<const float2*>(
+                            tvb + ((unsigned)__float_as_int(tr) * Nu8 + K)));
+                        const float gi = fmaf(uc - nf, e.y, e.x);
+                        if (i > 0) acc[i - 1] = fmaf(wk, gi - gprev, acc[i - 1]);
+                        gprev = gi;
+                    }
+                } else {
+                    const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
+#pragma unroll
+                    for (int i = 0; i <= R; ++i) {
+                        const float uc = fminf(fmaxf(fmaf((float)i, fib, f0), ulo), uhi);
+                        const float tr = uc + 12582912.0f;
+                        const float nf = tr - 12582912.0f;
+                        const float2 e = __ldg(reinterpret_cast<const float2*>(
+                            tvb + ((unsigned)__float_as_int(tr) * Nu8 + K)));
+                        const float gi = fmaf(uc - nf, e.y, e.x);
+                        if (i > 0) acc[i - 1] = fmaf(wk, gi - gprev, acc[i - 1]);
+                        gprev = gi;
+                    }
+                }
+            } while (false);
+            if (++k > kb) break;
+            pkl = pk1;
+            if (pkl >= 1.0f) break;  // column k starts right of the pixel
+            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
         }
     }
 #pragma unroll
