@@ -318,8 +318,14 @@ GeomF make_geomf(const Geom& g, int dim3d) {
 constexpr int CELL_R = 8;
 constexpr int VOX_R = 16;
 constexpr int VOX_NW = 4;
-constexpr int PFX_R = 16;
-constexpr int PFX_NWY = 8;
+#ifndef XR_PFX_R
+#define XR_PFX_R 16
+#endif
+#ifndef XR_PFX_NWY
+#define XR_PFX_NWY 8
+#endif
+constexpr int PFX_R = XR_PFX_R;      // z voxels per thread of the prefix backprojection
+constexpr int PFX_NWY = XR_PFX_NWY;  // image lines (warps) per CTA
 
 template <typename T> constexpr int dtype_code();
 template <> constexpr int dtype_code<float>() { return DT_F32; }

@@ -97,8 +97,11 @@ __device__ __forceinline__ float col_guess_fast(const GeomF& gf, const ViewHdr& 
 //   MODE OP_BW : OP_B times the FBP distance weight of the voxel centre
 //   MODE OP_AT : adjoint of the projection (cone: the table holds the
 //                pre-scaled sinogram; the line factor dpix dz / q^2)
+#ifndef XR_PFX_MINB
+#define XR_PFX_MINB 4
+#endif
 template <typename TO, int R, int NWY, int MODE>
-__global__ void __launch_bounds__(32 * NWY)
+__global__ void __launch_bounds__(32 * NWY, XR_PFX_MINB)
 vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const float2* __restrict__ tab,
                     TO* __restrict__ vol, const int nview, const int nzg, const double z0dz, const double zd0,
                     const double dvv, const float cw, const float atconst, const float oscale) {
