@@ -150,9 +150,10 @@ def test_edges_odd_shapes_and_empty(cuda):
 
 @pytest.mark.parametrize("scan", ["flat", "arc", "parallel"])
 def test_tma_and_plain_paths_match_oracle(cuda, scan):
-    """The TMA-staged projection kernels and the plain kernels both match
-    the oracle (windows clamped at the image edges, detector wider and
-    narrower than the image, shifted geometries)."""
+    """The staged kernels (TMA line windows for A/B^T/Bw^T, row prefix tables
+    for A^T/B/Bw) and the plain kernels both match the oracle (windows clamped
+    at the image edges, detector wider and narrower than the image, rows
+    finer and coarser than voxels, shifted geometries)."""
     from xrecon_b200 import _native
     cases = [
         _opts3d(96, 80, 40, 128, 48, 1.0, 1.0, 1.0, 1.2, 1.2, 400., 800., (0.5, -0.3, 0.7), 0.3, -0.4, scan),
@@ -166,12 +167,14 @@ def test_tma_and_plain_paths_match_oracle(cuda, scan):
         for opts in cases:
             D, H, W = int(opts[2]), int(opts[1]), int(opts[0])
             img = rng.random((1, 1, D, H, W)).astype(np.float32)
-            for op in ("A", "BT", "BWT"):
-                exact = O.dd3d(op, img, opts, ang)
+            sino = rng.random((1, 1, ang.size, int(opts[4]), int(opts[3]))).astype(np.float32)
+            for op in ("A", "BT", "BWT", "AT", "B", "BW"):
+                x = img if op in ("A", "BT", "BWT") else sino
+                exact = O.dd3d(op, x, opts, ang)
                 _native.set_plain_kernels(False)
-                tma = run(3, op, img, opts, ang, cuda)
+                tma = run(3, op, x, opts, ang, cuda)
                 _native.set_plain_kernels(True)
-                plain = run(3, op, img, opts, ang, cuda)
+                plain = run(3, op, x, opts, ang, cuda)
                 assert rel_l2(tma, exact) < 1e-5, (scan, op, "tma")
                 assert rel_l2(plain, exact) < 1e-5, (scan, op, "plain")
     finally:

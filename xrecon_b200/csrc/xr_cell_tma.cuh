@@ -210,7 +210,36 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         w[i] = wi;
                     }
                     float pos = f, jn = 1.0f, vj;
-                    if (win.ok) {
+                    if (win.ok && bf < 0.999f) {
+                        // Rows shorter than a voxel: each row crosses at most
+                        // one voxel boundary, so the walk is a fixed sequence
+                        // of R steps with one predicated advance each.  t is
+                        // clamped to the staged voxels win.z0 .. win.zlast
+                        // (rows -1 and D of the volume arrive as zeros, and
+                        // the window covers every t of the CTA otherwise).
+                        const float tlo = (float)(win.z0 - j0);
+                        const float thi = (float)(win.zlast - j0) + 0.999f;
+                        float tcur = fminf(fmaxf(f, tlo), thi);
+                        const float jlf = floorf(tcur);
+                        float jn = jlf + 1.0f;
+                        const TI* ptr = stage + (size_t)s * stage_elems + (pc - win.p0) +
+                                        (size_t)(j0 + (int)jlf - win.z0) * BP;
+                        float bcur = band_smem<TI, NB>(ptr, w, np);
+#pragma unroll
+                        for (int i = 0; i < R; ++i) {
+                            const float t1 = fminf(fmaxf(fmaf(bf, (float)(i + 1), f), tlo), thi);
+                            const float sp = fminf(t1, jn);
+                            float a = bcur * (sp - tcur);
+                            if (t1 > jn) {
+                                ptr += BP;
+                                bcur = band_smem<TI, NB>(ptr, w, np);
+                                jn += 1.0f;
+                                a = fmaf(bcur, t1 - sp, a);
+                            }
+                            acc[i] += a;
+                            tcur = t1;
+                        }
+                    } else if (win.ok) {
                         // Staged voxels win.z0 .. win.zlast; below the window a
                         // single virtual zero voxel ends at win.z0, past
                         // win.zlast the value is zero and the next boundary
