@@ -40,6 +40,13 @@ __device__ __forceinline__ float band_smem(const TI* p, const float (&w)[NB], in
     return s;
 }
 
+// Elements of one stage of the TMA cell gather: BZ + 1 rows of BP, rounded
+// up to 128 bytes.
+template <typename TI>
+__host__ __device__ inline int cell_stage_elems(int BP, int BZ) {
+    return (int)(((size_t)BP * (BZ + 1) * sizeof(TI) + 127) / 128 * 128 / sizeof(TI));
+}
+
 struct CellWindow {
     int p0, z0, zlast, empty, ok;
 };
@@ -89,10 +96,13 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                   TO* __restrict__ sino, const int nview, const int view0, const double z0dz, const double zd0,
                   const double dvv, const float cw, const int BP, const int BZ) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // each stage starts on a 128-byte boundary (TMA destination alignment)
-    const int stage_elems = (int)(((size_t)BP * BZ * sizeof(TI) + 127) / 128 * 128 / sizeof(TI));
+    // each stage starts on a 128-byte boundary (TMA destination alignment) and
+    // holds BZ + 1 rows: the spare row absorbs the look-ahead read of the
+    // branch-free walk (never used in a result)
+    const int stage_elems = cell_stage_elems<TI>(BP, BZ);
     TI* stage = reinterpret_cast<TI*>(smem_raw);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)2 * stage_elems * sizeof(TI));
+    int4* winfo = reinterpret_cast<int4*>(bar + 2);  // window of the line in each stage
 
     const int lane = threadIdx.x, tid = threadIdx.y * 32 + threadIdx.x;
     const int Nu = g.Nu;
@@ -140,6 +150,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
 
     auto issue = [&](int L, int s) {
         const CellWindow w = cell_window(cg, h, L, z0dz, npix, g.D, BP, BZ);
+        winfo[s] = make_int4(w.p0, w.z0, w.zlast, w.empty | (w.ok << 1));
         if (w.ok) {
             mbar_arrive_expect_tx(&bar[s], box_bytes);
             tma_load_4d(stage + (size_t)s * stage_elems, map, w.p0, L, w.z0, b, &bar[s]);
@@ -168,8 +179,12 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     for (int L = 0; L < nlines; ++L) {
         const int s = L & 1;
         const unsigned parity = (unsigned)((L >> 1) & 1);
-        const CellWindow win = cell_window(cg, h, L, z0dz, npix, g.D, BP, BZ);
         mbar_wait_bounded(&bar[s], parity);
+        CellWindow win;
+        {
+            const int4 wi = winfo[s];
+            win.p0 = wi.x; win.z0 = wi.y; win.zlast = wi.z; win.empty = wi.w & 1; win.ok = wi.w >> 1;
+        }
         if (active) {
             const double pk = fma(bB0, (double)L, bA0);
             const double pk1 = fma(bB1, (double)L, bA1);
@@ -189,7 +204,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                 float lf = cw;
                 if (MODE == OP_A) {
                     const float qf = (float)q;
-                    lf = dpdz / (qf * qf);
+                    lf = __fdividef(dpdz, qf * qf);
                 }
                 const float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
                 for (int pc = pa; pc <= pb; pc += NB) {
@@ -225,17 +240,18 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         const TI* ptr = stage + (size_t)s * stage_elems + (pc - win.p0) +
                                         (size_t)(j0 + (int)jlf - win.z0) * BP;
                         float bcur = band_smem<TI, NB>(ptr, w, np);
+                        float bnext = band_smem<TI, NB>(ptr + BP, w, np);
 #pragma unroll
                         for (int i = 0; i < R; ++i) {
                             const float t1 = fminf(fmaxf(fmaf(bf, (float)(i + 1), f), tlo), thi);
                             const float sp = fminf(t1, jn);
-                            float a = bcur * (sp - tcur);
-                            if (t1 > jn) {
-                                ptr += BP;
-                                bcur = band_smem<TI, NB>(ptr, w, np);
-                                jn += 1.0f;
-                                a = fmaf(bcur, t1 - sp, a);
-                            }
+                            // the second term vanishes unless the row crosses jn
+                            const float a = fmaf(bnext, t1 - sp, bcur * (sp - tcur));
+                            const bool adv = t1 > jn;
+                            bcur = adv ? bnext : bcur;
+                            jn = adv ? jn + 1.0f : jn;
+                            ptr = adv ? ptr + BP : ptr;
+                            bnext = band_smem<TI, NB>(ptr + BP, w, np);
                             acc[i] += a;
                             tcur = t1;
                         }
