@@ -164,6 +164,10 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
         mbar_init(&bar[1], 1);
         fence_barrier_init();
     }
+    // The spare row BZ of each stage is never written by TMA; the look-ahead
+    // read multiplies it by zero, so it must hold finite values (zeros).
+    for (int i = tid; i < 2 * BP; i += blockDim.x * blockDim.y)
+        stage[(size_t)(i / BP) * stage_elems + (size_t)BZ * BP + (i % BP)] = TI(0.0f);
     __syncthreads();
     if (tid == 0) {
         issue(0, 0);

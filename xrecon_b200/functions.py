@@ -10,6 +10,7 @@ options tensor (reference calling convention) or a
 """
 from __future__ import annotations
 
+import torch
 from torch.autograd import Function
 
 from . import backend as _B
@@ -54,3 +55,61 @@ WeightedBackProjection3d = _make("WeightedBackProjection3d", _B.weighted_backwar
 WeightedBackProjectionTranspose3d = _make("WeightedBackProjectionTranspose3d",
                                           _B.weighted_backward_projection_transpose3d,
                                           _B.weighted_backward_projection3d)
+
+
+class ProjectionLeastSquares(Function):
+    """``0.5 * ||A x - y||^2`` summed over the batch, with A the projection
+    (2D or 3D by the rank of ``x``), evaluated over chunks of views.
+
+    Forward projects one chunk of ``view_chunk`` views at a time and keeps
+    only the scalar; backward recomputes each chunk's residual
+    ``r_c = A_c x - y_c`` and accumulates ``A_c^T r_c``, the hand-written
+    transpose that is the backward of ``Projection2d/3d``.  Nothing of
+    sinogram size is saved between forward and backward, and at most one
+    chunk's sinogram is alive, so batched 3D gradients need
+    O(volume + view_chunk * detector) memory instead of O(views * detector).
+    Sums are accumulated in FP64.
+
+    ``y`` is not differentiated (the measured data).
+    """
+
+    @staticmethod
+    def forward(ctx, x, y, option, angles, view_chunk: int):
+        dim = x.dim() - 2
+        fwd = _B.forward_projection2d if dim == 2 else _B.forward_projection3d
+        xc = _c(x)
+        V = angles.numel()
+        total = torch.zeros((), dtype=torch.float64, device=x.device)
+        for v0 in range(0, V, view_chunk):
+            v1 = min(V, v0 + view_chunk)
+            r = fwd(xc, option, angles[v0:v1].contiguous()) - y[:, :, v0:v1]
+            total += r.double().square().sum()
+        ctx.option = option
+        ctx.view_chunk = view_chunk
+        ctx.save_for_backward(x, y, angles)
+        return (0.5 * total).to(x.dtype)
+
+    @staticmethod
+    def backward(ctx, grad_output):
+        x, y, angles = ctx.saved_tensors
+        dim = x.dim() - 2
+        fwd = _B.forward_projection2d if dim == 2 else _B.forward_projection3d
+        adj = _B.projection_transpose2d if dim == 2 else _B.projection_transpose3d
+        xc = _c(x)
+        V = angles.numel()
+        grad = None
+        for v0 in range(0, V, ctx.view_chunk):
+            v1 = min(V, v0 + ctx.view_chunk)
+            a = angles[v0:v1].contiguous()
+            r = fwd(xc, ctx.option, a) - y[:, :, v0:v1]
+            g = adj(_c(r), ctx.option, a)
+            grad = g if grad is None else grad.add_(g)
+        return grad * grad_output, None, None, None, None
+
+
+def projection_least_squares(x, y, option, angles, view_chunk: int = 32):
+    """Differentiable ``0.5 * ||A x - y||^2`` with view-chunked recomputation
+    (see :class:`ProjectionLeastSquares`)."""
+    if view_chunk < 1:
+        raise ValueError("view_chunk must be >= 1")
+    return ProjectionLeastSquares.apply(x, y, option, angles, int(view_chunk))

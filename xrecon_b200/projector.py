@@ -73,6 +73,54 @@ def parker_weights(angles: Tensor, gamma: Tensor, num_det: int) -> Tensor:
     return w.clamp_(0.0, 1.0)
 
 
+class _FilterRows(torch.autograd.Function):
+    """Differentiable FBP pre-filter: ``out = corr_u(s * weight * parker, filt)``
+    with the fused kernel, in FP32 without TF32.
+
+    The adjoint of the correlation with ``filt`` is the correlation with the
+    reversed filter, so the sinogram gradient runs through the same kernel;
+    the (rarely trained) weight and filter gradients are reduced in FP64.
+    """
+
+    @staticmethod
+    def forward(ctx, s, weight, filt, parker, nview, rows_per_view):
+        Nu = s.shape[-1]
+        sc = s.contiguous()
+        out = _native.fbp_filter(sc, nview=nview, rows_per_view=rows_per_view,
+                                 cosw=weight.detach().reshape(-1), filt=filt.detach().reshape(-1),
+                                 parker=None if parker is None else parker.detach().reshape(nview, Nu))
+        ctx.save_for_backward(sc, weight, filt, parker)
+        ctx.nview, ctx.rows_per_view = nview, rows_per_view
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        s, weight, filt, parker = ctx.saved_tensors
+        Nu = s.shape[-1]
+        h = _native.fbp_filter(g.contiguous(), nview=ctx.nview, rows_per_view=ctx.rows_per_view, cosw=None,
+                               filt=filt.detach().reshape(-1).flip(0), parker=None)
+        w = weight.detach().to(h.dtype)
+        pk = None if parker is None else parker.detach()  # broadcasts against the sinogram
+        gs = gw = gf = None
+        if ctx.needs_input_grad[0]:
+            gs = h * w if pk is None else h * w * pk
+        if ctx.needs_input_grad[1]:
+            t = (h.double() * s.double()) if pk is None else (h.double() * s.double() * pk.double())
+            gw = t.reshape(-1, Nu).sum(0).reshape(weight.shape).to(weight.dtype)
+        if ctx.needs_input_grad[2]:
+            # d out[i] / d filt[m] = sw[i + m - (Nu - 1)]
+            sw = s.double() * w.double() if pk is None else s.double() * w.double() * pk.double()
+            a = sw.reshape(-1, Nu)
+            b = g.double().reshape(-1, Nu)
+            n = 4 * Nu
+            fa = torch.fft.rfft(a, n=n)
+            fb = torch.fft.rfft(b, n=n)
+            cc = torch.fft.irfft((fa * fb.conj()).sum(0), n=n)  # cc[k] = sum_i b[i] a[i + k]
+            idx = torch.arange(2 * Nu - 1, device=cc.device) - (Nu - 1)
+            gf = cc[idx % n].reshape(filt.shape).to(filt.dtype)
+        return gs, gw, gf, None, None, None
+
+
 class _ProjectorBase(nn.Module):
     _dim = 0
 
@@ -112,16 +160,8 @@ class _ProjectorBase(nn.Module):
         needs_grad = torch.is_grad_enabled() and (
             sino.requires_grad or (isinstance(filt, Tensor) and filt.requires_grad) or wt.requires_grad)
         if needs_grad:
-            s = sino.to(torch.float32)
-            if pw is not None:
-                s = s * pw.to(device=s.device, dtype=s.dtype)
-            s = s * wt.to(device=s.device, dtype=s.dtype)
-            f = filt.to(device=s.device, dtype=s.dtype)
-            with torch.backends.cudnn.flags(enabled=True, allow_tf32=False):
-                if self._dim == 2:
-                    filtered = nn.functional.conv2d(s, f.reshape(1, 1, 1, -1), padding=(0, Nu - 1))
-                else:
-                    filtered = nn.functional.conv3d(s, f.reshape(1, 1, 1, 1, -1), padding=(0, 0, Nu - 1))
+            pw_t = None if pw is None else pw.to(device=sino.device, dtype=torch.float32)
+            filtered = _FilterRows.apply(sino.to(torch.float32), wt, filt, pw_t, angles.numel(), rows_per_view)
             recon = self.backprojection_weighted(filtered.contiguous(), angles)
             return recon * scale.to(device=recon.device, dtype=recon.dtype)
         with torch.no_grad():
