@@ -59,9 +59,14 @@ def make_projector():
                           xr.ConeBeam3d(xr.Detector3d((WL["Nu"], WL["Nv"]), WL["du"]), WL["sod"], WL["sdd"], "flat"))
 
 
-def angles_np():
+def angles_np(nviews=None):
+    """The workload's views, uniform over 2 pi; with ``nviews`` an evenly
+    strided subset (profiling cases)."""
     import numpy as np
-    return (np.arange(WL["V"]) * (2 * np.pi / WL["V"])).astype(np.float32)
+    a = (np.arange(WL["V"]) * (2 * np.pi / WL["V"])).astype(np.float32)
+    if nviews is None or nviews >= WL["V"]:
+        return a
+    return a[:: WL["V"] // nviews][:nviews].copy()
 
 
 # ---------------------------------------------------------------- clocks
@@ -193,7 +198,8 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
     D, H, W = WL["D"], WL["H"], WL["W"]
     vol = ellipsoid_volume_torch((D, H, W), random_ellipsoids3d(20, seed=rank, density=(0.0, 1.0)), dev)
     vol = vol[None, None].contiguous()
-    ang = torch.from_numpy(angles_np()).to(dev)
+    ang = torch.from_numpy(angles_np(args.views)).to(dev)
+    nv = ang.numel()
 
     def step(x):
         s = P.projection(x, ang)
@@ -216,6 +222,8 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
     barrier()
     torch.cuda.synchronize()
     clocks.start()
+    from xrecon_b200 import _native
+    launches0 = _native.launch_count()
     e0.record(stream)
     for i in range(args.steps):
         ev[i][0].record(stream)
@@ -225,6 +233,7 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         ev[i][2].record(stream)
         del s, r
     e1.record(stream)
+    launches = _native.launch_count() - launches0
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier()
@@ -236,29 +245,31 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         t = torch.tensor([t_step], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_step = float(t.item())
-    value = world * nvox() * WL["V"] / t_step / 1e9
+    value = world * nvox() * nv / t_step / 1e9
 
     # end-to-end through the public API with host buffers
-    host_vol = vol.cpu().pin_memory()
-    host_out = torch.empty_like(host_vol).pin_memory()
-    dvol = torch.empty_like(vol)
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(1, min(args.steps, 3))
-    barrier()
-    torch.cuda.synchronize()
-    f0.record(stream)
-    for _ in range(e2e_steps):
-        dvol.copy_(host_vol, non_blocking=True)
-        out = step(dvol)
-        host_out.copy_(out, non_blocking=True)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    t_e2e = f0.elapsed_time(f1) / 1e3 / e2e_steps
-    if world > 1:
-        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e_value = world * nvox() * WL["V"] / t_e2e / 1e9
+    e2e_value = None
+    if not args.no_e2e:
+        host_vol = vol.cpu().pin_memory()
+        host_out = torch.empty_like(host_vol).pin_memory()
+        dvol = torch.empty_like(vol)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2e_steps = max(1, min(args.steps, 3))
+        barrier()
+        torch.cuda.synchronize()
+        f0.record(stream)
+        for _ in range(e2e_steps):
+            dvol.copy_(host_vol, non_blocking=True)
+            out = step(dvol)
+            host_out.copy_(out, non_blocking=True)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        t_e2e = f0.elapsed_time(f1) / 1e3 / e2e_steps
+        if world > 1:
+            t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e_value = world * nvox() * nv / t_e2e / 1e9
     vol_bytes = vol.numel() * 4
 
     # BF16-stored form of the same step (volume and sinogram in BF16, FP32
@@ -279,33 +290,39 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         t16 = g0.elapsed_time(g1) / 1e3 / nb
         ref32 = step(vol)
         rel = float((out16.float() - ref32).norm() / ref32.norm())
-        bf = {"value": world * nvox() * WL["V"] / t16 / 1e9, "unit": UNIT, "ms_per_step": t16 * 1e3,
+        bf = {"value": world * nvox() * nv / t16 / 1e9, "unit": UNIT, "ms_per_step": t16 * 1e3,
               "rel_l2_vs_fp32": rel}
         del vol16, out16, ref32
 
     hbm, src = peaks()
     dom_t = max(t_a, t_b)
-    dom = "cell_gather3d (projection A)" if t_a >= t_b else "vox_gather3d (backprojection B)"
-    achieved = algo_bytes_op() / dom_t / 1e9
+    dom = "cell_tma3d_kernel (projection A)" if t_a >= t_b else "vox_prefix3d_kernel (backprojection B)"
+    wl = dict(WL, V=nv)
+    achieved = algo_bytes_op(wl) / dom_t / 1e9
     traffic = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
-        traffic = json.loads(tp.read_text()).get("A" if t_a >= t_b else "B")
+        tj = json.loads(tp.read_text())
+        full = tj.get("A" if t_a >= t_b else "B")
+        # recorded at the full view count; scaled for a profiling subset
+        traffic = None if full is None else full * nv / tj.get("views", WL["V"])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random ellipsoids)",
-        "config": {"workload": WORKLOAD_NAME, "volume": [WL["D"], WL["H"], WL["W"]], "views": WL["V"],
+        "config": {"workload": WORKLOAD_NAME if nv == WL["V"] else f"{WORKLOAD_NAME} (profiling subset: {nv} views)",
+                   "volume": [WL["D"], WL["H"], WL["W"]], "views": nv,
                    "detector": [WL["Nv"], WL["Nu"]], "ms_projection": t_a * 1e3,
                    "ms_backprojection": t_b * 1e3,
                    "l2": "inputs larger than L2 (volume 256 MiB, sinogram 1.41 GiB)",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": algo_bytes_op()},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": vol_bytes, "d2h_bytes_per_step": vol_bytes},
-        "gpu_launches": 5 * args.steps,
+                     "algorithmic_bytes_per_launch": algo_bytes_op(wl)},
+        "e2e": None if e2e_value is None else {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": vol_bytes,
+                                               "d2h_bytes_per_step": vol_bytes},
+        "gpu_launches": launches,
         "clocks": clk,
     }
     if bf:
@@ -326,6 +343,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-bf16", action="store_true", help="skip the BF16-storage measurement")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
+    ap.add_argument("--views", type=int, default=None,
+                    help="profiling: an evenly strided subset of the workload's views")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

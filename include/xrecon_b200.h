@@ -139,6 +139,10 @@ int xr_set_plain_kernels(int on);
 int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,
                     const float* angles, int nbatch, int nview, void* stream);
 
+/* Number of CUDA kernels this library has launched in this process (all
+ * devices and threads). */
+unsigned long long xr_launch_count(void);
+
 /* Human-readable message for the last non-OK status returned on this thread. */
 const char* xr_last_error(void);
 

@@ -71,6 +71,8 @@ def lib():
     L.xr_set_plain_kernels.restype = c_int
     L.xr_set_plain_kernels.argtypes = [c_int]
     L.xr_last_error.restype = ctypes.c_char_p
+    L.xr_launch_count.restype = ctypes.c_ulonglong
+    L.xr_launch_count.argtypes = []
     L.xr_version.restype = ctypes.c_char_p
     _lib = L
     return L
@@ -229,6 +231,11 @@ def cell_plan(geom: Geom3d) -> dict:
 def set_plain_kernels(on: bool) -> None:
     """Route operators through the plain (non-TMA) kernels (testing aid)."""
     lib().xr_set_plain_kernels(int(bool(on)))
+
+
+def launch_count() -> int:
+    """Kernels launched by the library so far in this process."""
+    return int(lib().xr_launch_count())
 
 
 def version() -> str:

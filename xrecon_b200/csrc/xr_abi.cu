@@ -8,6 +8,7 @@
 
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <cstring>
 #include <type_traits>
 #include <map>
@@ -37,7 +38,12 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
+// Kernels launched by this library (process-wide; every launch site is
+// followed by exactly one check_cuda).
+std::atomic<unsigned long long> g_launches{0};
+
 int check_cuda(const char* what) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(XR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
     return XR_OK;
@@ -715,6 +721,8 @@ int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in,
     return xr::apply(0, op, g, in, dtype_in, out, dtype_out, angles, nbatch, nview, scratch,
                      (size_t)XR_NOALLOC_SCRATCH_BYTES, stream, 1.0f);
 }
+
+unsigned long long xr_launch_count(void) { return xr::g_launches.load(std::memory_order_relaxed); }
 
 const char* xr_version(void) { return "xrecon_b200 0.1.0 (sm_100a)"; }
 
