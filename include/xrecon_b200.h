@@ -139,6 +139,49 @@ int xr_set_plain_kernels(int on);
 int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,
                     const float* angles, int nbatch, int nview, void* stream);
 
+/*
+ * Ragged batch of 2D reconstructions: projection then FBP for many
+ * instances with different geometries, image sizes, view counts and
+ * detectors, in one persistent cooperative kernel launch (no reference
+ * counterpart: the reference runs each instance through Projector2d,
+ * projector.py:176-206, with one launch per operator).  Buffers hold the
+ * instances back to back; offsets are in elements:
+ *   images / recon : [H][W] at img_offset         (recon: the FBP output)
+ *   sino           : [nview][Nu] at sino_offset   (the projection output)
+ *   angles         : [nview] at ang_offset
+ *   filt           : [2 Nu - 1] filter taps at filt_offset (as xr_fbp_filter)
+ *   cosw           : [Nu] cosine weight at cosw_offset
+ * recon = scale * Bw(corr_u(sino * cosw, filt)) per instance.
+ */
+typedef struct {
+    xr_geom2d geom;
+    int nview;
+    long long img_offset, sino_offset, ang_offset, filt_offset, cosw_offset;
+    float scale;
+} xr_ragged2d_instance;
+
+typedef struct xr_ragged2d_plan xr_ragged2d_plan;
+
+/* Validate the instances and lay out the device workspace (host only). */
+int xr_ragged2d_plan_create(const xr_ragged2d_instance* inst, int ninst, xr_ragged2d_plan** plan,
+                            size_t* workspace_bytes);
+/* Bind buffers and workspace: uploads the per-instance descriptors
+ * (synchronous; call before any stream capture). */
+int xr_ragged2d_plan_bind(xr_ragged2d_plan* plan, const float* images, float* sino, float* recon,
+                          const float* angles, const float* filt, const float* cosw, void* workspace,
+                          size_t workspace_bytes);
+/* One persistent launch over the whole batch (capturable in a CUDA graph).
+ * project = 0 skips the projection (sino is then an input).  Tile shape:
+ * 32 << a_cols_log2 detector columns per projection tile, 1 << view_split_log2
+ * threads per pixel in the backprojection (both 0..3).  Calls on one plan
+ * must not overlap (they share the workspace's tile counters). */
+int xr_ragged2d_run(const xr_ragged2d_plan* plan, int project, int a_cols_log2, int view_split_log2, void* stream);
+/* Grid size of the persistent launch and the tile counts of its ten tile
+ * lists (tables, filter rows, projection per a_cols, backprojection per
+ * view split). */
+int xr_ragged2d_plan_info(const xr_ragged2d_plan* plan, int* grid, int* tiles10);
+void xr_ragged2d_plan_destroy(xr_ragged2d_plan* plan);
+
 /* Number of CUDA kernels this library has launched in this process (all
  * devices and threads). */
 unsigned long long xr_launch_count(void);

@@ -8,6 +8,7 @@
 
 #include <cudaTypedefs.h>
 
+#include <array>
 #include <atomic>
 #include <cstring>
 #include <type_traits>
@@ -17,6 +18,7 @@
 
 #include "xr_cell_tma.cuh"
 #include "xr_vox_prefix.cuh"
+#include "xr_ragged.cuh"
 #include "../../include/xrecon_b200.h"
 
 
@@ -588,6 +590,43 @@ int apply(int dim3d, int op, const Geom& g, const void* in, int dti, void* out, 
     return dispatch_out<__half>(dim3d, op, g, in, out, dto, ang, nbatch, nview, ws, l, st, oscale);
 }
 
+// ------------------------------------------------------ ragged 2D batches
+
+struct RaggedLayout {
+    size_t desc, sync;
+    std::vector<size_t> hdr, bA, bB, colQ, colR, colE, colF, colM, imgT, filt;
+    size_t total;
+};
+
+}  // namespace
+}  // namespace xr
+
+struct xr_ragged2d_plan {
+    std::vector<xr_ragged2d_instance> inst;
+    std::vector<xr::Geom> geom;
+    xr::RaggedLayout lay;
+    int t0[10][1];  // unused placeholder (tile starts live in the device descriptors)
+    std::vector<std::array<int, 10>> starts;  // per instance
+    int totals[10];
+    int max_nu;
+    int device;
+    int grid;
+    size_t smem;
+    void* workspace;
+};
+
+namespace xr {
+namespace {
+
+int ragged_tiles(const Geom& g, int nview, int list) {
+    const int hw = g.H * g.W;
+    if (list == 0) return nview + (hw + 1023) / 1024;
+    if (list == 1) return nview;
+    if (list < 6) return nview * ((g.Nu + (32 << (list - 2)) - 1) / (32 << (list - 2)));
+    const int px = 256 / (1 << (list - 6));
+    return (hw + px - 1) / px;
+}
+
 // Fixed device scratch of xr_dd2d_noalloc.  Its address is looked up once per
 // device (cudaGetSymbolAddress) and cached; nothing is ever allocated for it.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[XR_NOALLOC_SCRATCH_BYTES];
@@ -723,6 +762,149 @@ int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in,
 }
 
 unsigned long long xr_launch_count(void) { return xr::g_launches.load(std::memory_order_relaxed); }
+
+int xr_ragged2d_plan_create(const xr_ragged2d_instance* inst, int ninst, xr_ragged2d_plan** plan,
+                            size_t* workspace_bytes) {
+    using namespace xr;
+    if (!inst || !plan || !workspace_bytes || ninst < 1) return fail(XR_ERR_INVALID_ARGUMENT, "bad ragged plan arguments");
+    auto* P = new xr_ragged2d_plan();
+    P->inst.assign(inst, inst + ninst);
+    P->max_nu = 0;
+    size_t o = 0;
+    RaggedLayout& L = P->lay;
+    L.desc = o; o = align256(o + (size_t)ninst * sizeof(RaggedDev));
+    L.sync = o; o = align256(o + 64);
+    long long tot[10] = {0};
+    for (int i = 0; i < ninst; ++i) {
+        const Geom g = geom_from(&inst[i].geom);
+        const int V = inst[i].nview;
+        if (int rc = validate(g, 0, OP_A, 1, V)) { delete P; return rc; }
+        if (V < 1) { delete P; return fail(XR_ERR_INVALID_ARGUMENT, "instance %d has no views", i); }
+        if ((long long)g.H * g.W > (1ll << 30)) { delete P; return fail(XR_ERR_UNSUPPORTED, "instance %d image too large", i); }
+        P->geom.push_back(g);
+        P->max_nu = std::max(P->max_nu, g.Nu);
+        std::array<int, 10> st{};
+        for (int l = 0; l < 10; ++l) {
+            st[l] = (int)tot[l];
+            tot[l] += ragged_tiles(g, V, l);
+        }
+        P->starts.push_back(st);
+        const size_t Vs = (size_t)V;
+        L.hdr.push_back(o);  o = align256(o + Vs * sizeof(ViewHdr));
+        L.bA.push_back(o);   o = align256(o + Vs * (g.Nu + 1) * sizeof(double));
+        L.bB.push_back(o);   o = align256(o + Vs * (g.Nu + 1) * sizeof(double));
+        L.colQ.push_back(o); o = align256(o + Vs * g.Nu * sizeof(double));
+        L.colR.push_back(o); o = align256(o + Vs * g.Nu * sizeof(double));
+        L.colE.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
+        L.colF.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
+        L.colM.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
+        L.imgT.push_back(o); o = align256(o + (size_t)g.H * g.W * sizeof(float));
+        L.filt.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
+    }
+    for (int l = 0; l < 10; ++l) {
+        if (tot[l] > 0x7fffffffll) { delete P; return fail(XR_ERR_UNSUPPORTED, "ragged batch too large"); }
+        P->totals[l] = (int)tot[l];
+    }
+    L.total = o;
+    P->smem = std::max<size_t>(256, 3 * (size_t)P->max_nu + 16) * sizeof(float);
+    if (P->smem > 200 * 1024) { delete P; return fail(XR_ERR_UNSUPPORTED, "detector too wide for the ragged kernel"); }
+    if (cudaGetDevice(&P->device) != cudaSuccess) { delete P; return fail(XR_ERR_CUDA, "cudaGetDevice failed"); }
+    if (P->smem > 48 * 1024 &&
+        cudaFuncSetAttribute(ragged2d_fbp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->smem) != cudaSuccess) {
+        delete P; return fail(XR_ERR_CUDA, "cannot reserve shared memory");
+    }
+    int per_sm = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ragged2d_fbp_kernel, 256, P->smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P->device) != cudaSuccess || per_sm < 1) {
+        delete P; return fail(XR_ERR_CUDA, "occupancy query failed");
+    }
+    P->grid = per_sm * nsm;
+    P->workspace = nullptr;
+    *plan = P;
+    *workspace_bytes = L.total;
+    return XR_OK;
+}
+
+int xr_ragged2d_plan_bind(xr_ragged2d_plan* P, const float* images, float* sino, float* recon, const float* angles,
+                          const float* filt, const float* cosw, void* workspace, size_t workspace_bytes) {
+    using namespace xr;
+    if (!P || !images || !sino || !recon || !angles || !filt || !cosw || !workspace)
+        return fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
+    if (workspace_bytes < P->lay.total) return fail(XR_ERR_WORKSPACE, "workspace of %zu bytes required", P->lay.total);
+    if (reinterpret_cast<uintptr_t>(workspace) % 256) return fail(XR_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    char* ws = static_cast<char*>(workspace);
+    const RaggedLayout& L = P->lay;
+    std::vector<RaggedDev> d(P->inst.size());
+    for (size_t i = 0; i < d.size(); ++i) {
+        const xr_ragged2d_instance& in = P->inst[i];
+        RaggedDev& r = d[i];
+        r.g = P->geom[i];
+        r.vt.hdr = reinterpret_cast<ViewHdr*>(ws + L.hdr[i]);
+        r.vt.bA = reinterpret_cast<double*>(ws + L.bA[i]);
+        r.vt.bB = reinterpret_cast<double*>(ws + L.bB[i]);
+        r.vt.colQ = reinterpret_cast<double*>(ws + L.colQ[i]);
+        r.vt.colR = reinterpret_cast<double*>(ws + L.colR[i]);
+        r.vt.colE = reinterpret_cast<float*>(ws + L.colE[i]);
+        r.vt.colF = reinterpret_cast<float*>(ws + L.colF[i]);
+        r.vt.colM = reinterpret_cast<float*>(ws + L.colM[i]);
+        r.nview = in.nview;
+        r.cw = column_width(r.g, 0);
+        r.scale = in.scale;
+        r.img = images + in.img_offset;
+        r.imgT = reinterpret_cast<float*>(ws + L.imgT[i]);
+        r.sino = sino + in.sino_offset;
+        r.filt_out = reinterpret_cast<float*>(ws + L.filt[i]);
+        r.recon = recon + in.img_offset;
+        r.ang = angles + in.ang_offset;
+        r.filt = filt + in.filt_offset;
+        r.cosw = cosw + in.cosw_offset;
+        for (int l = 0; l < 10; ++l) r.t0[l] = P->starts[i][l];
+    }
+    if (cudaMemcpy(ws + L.desc, d.data(), d.size() * sizeof(RaggedDev), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(ws + L.sync, 0, 64) != cudaSuccess)
+        return fail(XR_ERR_CUDA, "descriptor upload failed");
+    P->workspace = workspace;
+    return XR_OK;
+}
+
+int xr_ragged2d_run(const xr_ragged2d_plan* P, int project, int a_cols_log2, int view_split_log2, void* stream) {
+    using namespace xr;
+    if (!P || !P->workspace) return fail(XR_ERR_INVALID_ARGUMENT, "plan not bound to a workspace");
+    if (a_cols_log2 < 0 || a_cols_log2 > 3 || view_split_log2 < 0 || view_split_log2 > 3)
+        return fail(XR_ERR_INVALID_ARGUMENT, "tile parameters out of range");
+    char* ws = static_cast<char*>(P->workspace);
+    const RaggedDev* desc = reinterpret_cast<const RaggedDev*>(ws + P->lay.desc);
+    unsigned* bar = reinterpret_cast<unsigned*>(ws + P->lay.sync);
+    int* ctr = reinterpret_cast<int*>(ws + P->lay.sync + 16);
+    const int4 totals = make_int4(P->totals[0], project ? P->totals[2 + a_cols_log2] : 0, P->totals[1],
+                                  P->totals[6 + view_split_log2]);
+    const int4 lists = make_int4(0, 2 + a_cols_log2, 1, 6 + view_split_log2);
+    const int ninst = (int)P->inst.size();
+    const int CW = 32 << a_cols_log2, VS = 1 << view_split_log2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P->grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = P->smem;
+    cfg.stream = static_cast<cudaStream_t>(stream);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, ragged2d_fbp_kernel, desc, ninst, totals, lists, project, CW, VS, bar, ctr) !=
+        cudaSuccess)
+        return check_cuda("ragged2d_fbp (cooperative launch)");
+    return check_cuda("ragged2d_fbp");
+}
+
+int xr_ragged2d_plan_info(const xr_ragged2d_plan* P, int* grid, int* tiles10) {
+    if (!P || !grid || !tiles10) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
+    *grid = P->grid;
+    for (int l = 0; l < 10; ++l) tiles10[l] = P->totals[l];
+    return XR_OK;
+}
+
+void xr_ragged2d_plan_destroy(xr_ragged2d_plan* plan) { delete plan; }
 
 const char* xr_version(void) { return "xrecon_b200 0.1.0 (sm_100a)"; }
 

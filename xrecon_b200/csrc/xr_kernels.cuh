@@ -56,13 +56,22 @@ __device__ __forceinline__ float row_value(const TI* __restrict__ colbase, int m
 // ------------------------------------------------------------------ setup
 
 // One thread per (view, boundary k in 0..Nu).  FP64 throughout.
+__device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d, const float angle, const int v,
+                                                 const int k, const ViewTables& vt);
+
 __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* __restrict__ ang,
                                    const int nview, const ViewTables vt) {
     const int v = blockIdx.y;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nview || k > g.Nu) return;
+    setup_view_entry(g, dim3d, ang[v], v, k, vt);
+}
+
+// Per-view tables of view v, boundary / column k (k = 0..Nu).
+__device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d, const float angle, const int v,
+                                                 const int k, const ViewTables& vt) {
     ViewHdr h;
-    make_view_hdr(g, ang[v], h);
+    make_view_hdr(g, angle, h);
     if (k == 0) vt.hdr[v] = h;
 
     const double uscale = (dim3d && g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
@@ -443,6 +452,15 @@ vox_gather3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const TI*
 // ------------------------------------------------------------- 2D kernels
 
 // Cell gather, 2D: one thread per (view, column).
+template <typename TI, int MODE>
+__device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt, const ViewHdr& h,
+                                            const TI* __restrict__ img_rows, const TI* __restrict__ img_cols,
+                                            const int v, const int k, const float cw, const int l0, const int ls);
+template <typename TI, int MODE>
+__device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, const TI* __restrict__ sinob,
+                                           const int ix, const int iy, const float cw, const int v0,
+                                           const int v1, const int vs);
+
 template <typename TI, typename TO, int MODE>
 __global__ void __launch_bounds__(128)
 cell_gather2d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ img_rows,
@@ -453,12 +471,26 @@ cell_gather2d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ i
     const int Nu = g.Nu;
     if (k >= Nu) return;
     const ViewHdr h = vt.hdr[v];
+    const size_t plane = (size_t)g.W * g.H;
+    const float acc = cell2d_sum<TI, MODE>(g, vt, h, img_rows + b * plane, img_cols + b * plane, v, k, cw, 0, 1);
+    const int col = h.keep ? k : Nu - 1 - k;
+    st(sino + ((size_t)b * nview + v) * Nu + col, acc);
+}
+
+// Cell k of view v (traversal order), lines L = l0, l0 + ls, ...: the 2D DD
+// line sum, times the cell scale colE for MODE OP_A (applied by the caller
+// when the lines are split over threads: pass ls > 1 and scale afterwards).
+template <typename TI, int MODE>
+__device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt, const ViewHdr& h,
+                                            const TI* __restrict__ img_rows, const TI* __restrict__ img_cols,
+                                            const int v, const int k, const float cw, const int l0, const int ls) {
+    const int Nu = g.Nu;
     const size_t ob = (size_t)v * (Nu + 1) + k;
     const double bA0 = vt.bA[ob], bB0 = vt.bB[ob], bA1 = vt.bA[ob + 1], bB1 = vt.bB[ob + 1];
     const int nlines = h.nlines, npix = h.npix;
-    const TI* __restrict__ img = (h.use_x ? img_rows : img_cols) + (size_t)b * nlines * npix;
+    const TI* __restrict__ img = h.use_x ? img_rows : img_cols;
     float acc = 0.0f;
-    for (int L = 0; L < nlines; ++L) {
+    for (int L = l0; L < nlines; L += ls) {
         const double pk = fma(bB0, (double)L, bA0);
         const double pk1 = fma(bB1, (double)L, bA1);
         const int pa = max((int)floor(pk), 0);
@@ -478,9 +510,8 @@ cell_gather2d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ i
             acc = fmaf(w, ld(line + pp), acc);
         }
     }
-    if (MODE == OP_A) acc *= vt.colE[(size_t)v * Nu + k];
-    const int col = h.keep ? k : Nu - 1 - k;
-    st(sino + ((size_t)b * nview + v) * Nu + col, acc);
+    if (MODE == OP_A && ls == 1) acc *= vt.colE[(size_t)v * Nu + k];
+    return acc;
 }
 
 // Voxel gather, 2D: one thread per pixel, sweeping the views.
@@ -492,10 +523,19 @@ vox_gather2d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ si
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     const int b = blockIdx.z;
     if (ix >= g.W || iy >= g.H) return;
+    const float acc = pix2d_sum<TI, MODE>(g, vt, sino + (size_t)b * nview * g.Nu, ix, iy, cw, 0, nview, 1);
+    st(img + ((size_t)b * g.H + iy) * g.W + ix, acc * oscale);
+}
+
+// Pixel (ix, iy): the 2D DD backprojection sum over views v = v0, v0 + vs, ...
+// < v1 of the sinogram sinob [nview][Nu].
+template <typename TI, int MODE>
+__device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, const TI* __restrict__ sinob,
+                                           const int ix, const int iy, const float cw, const int v0,
+                                           const int v1, const int vs) {
     const int Nu = g.Nu;
-    const TI* __restrict__ sinob = sino + (size_t)b * nview * Nu;
     float acc = 0.0f;
-    for (int v = 0; v < nview; ++v) {
+    for (int v = v0; v < v1; v += vs) {
         const ViewHdr h = vt.hdr[v];
         int L, p;
         if (h.use_x) { L = iy; p = ix; } else { L = ix; p = g.H - 1 - iy; }
@@ -534,7 +574,7 @@ vox_gather2d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ si
             acc = fmaf(w, ld(sv + col), acc);
         }
     }
-    st(img + ((size_t)b * g.H + iy) * g.W + ix, acc * oscale);
+    return acc;
 }
 
 // -------------------------------------------------------------- FBP filter
