@@ -195,7 +195,8 @@ CellPlan plan_cell(const Geom& g) {
     }
     p.BP = round_up(std::max(maxspan, 8), 8);
     p.BZ = (int)maxnz;
-    p.ok = p.BP <= 256 && p.BZ <= 256 && p.BZ >= 1 && (size_t)2 * p.BP * (p.BZ + 1) * 4 <= 200 * 1024;
+    p.ok = p.BP <= 256 && p.BZ <= 256 && p.BZ >= 1 &&
+           (size_t)2 * p.BP * (p.BZ + 1) * 4 + (size_t)std::max(g.W, g.H) * 16 + 16 <= 200 * 1024;
     std::lock_guard<std::mutex> lk(mu);
     cache[key] = p;
     return p;
@@ -345,7 +346,8 @@ int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr
                          const TI* rows, const TI* cols, int pitch_r, int pitch_c, TO* out, int nbatch, int nview,
                          const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
     auto kern = cell_tma3d_kernel<TI, TO, R, 2, MODE>;
-    const size_t smem = 2 * (size_t)cell_stage_elems<TI>(p.BP, p.BZ) * sizeof(TI) + 16 + 2 * sizeof(int4);
+    const int maxlines = std::max(g.W, g.H);
+    const size_t smem = 2 * (size_t)cell_stage_elems<TI>(p.BP, p.BZ) * sizeof(TI) + 16 + (size_t)maxlines * sizeof(int4);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
     const int RG = CELL_NW * R;

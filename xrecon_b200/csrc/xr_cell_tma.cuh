@@ -102,7 +102,8 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     const int stage_elems = cell_stage_elems<TI>(BP, BZ);
     TI* stage = reinterpret_cast<TI*>(smem_raw);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)2 * stage_elems * sizeof(TI));
-    int4* winfo = reinterpret_cast<int4*>(bar + 2);  // window of the line in each stage
+    // window of every line of this CTA (computed once, below)
+    int4* wins = reinterpret_cast<int4*>(bar + 2);
 
     const int lane = threadIdx.x, tid = threadIdx.y * 32 + threadIdx.x;
     const int Nu = g.Nu;
@@ -149,11 +150,10 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     const unsigned box_bytes = (unsigned)((size_t)BP * BZ * sizeof(TI));
 
     auto issue = [&](int L, int s) {
-        const CellWindow w = cell_window(cg, h, L, z0dz, npix, g.D, BP, BZ);
-        winfo[s] = make_int4(w.p0, w.z0, w.zlast, w.empty | (w.ok << 1));
-        if (w.ok) {
+        const int4 w = wins[L];
+        if (w.w >> 1) {
             mbar_arrive_expect_tx(&bar[s], box_bytes);
-            tma_load_4d(stage + (size_t)s * stage_elems, map, w.p0, L, w.z0, b, &bar[s]);
+            tma_load_4d(stage + (size_t)s * stage_elems, map, w.x, L, w.y, b, &bar[s]);
         } else {
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar[s])) : "memory");
         }
@@ -163,6 +163,11 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         fence_barrier_init();
+    }
+    // the line windows, evaluated by all threads in parallel (FP64)
+    for (int L = tid; L < nlines; L += blockDim.x * blockDim.y) {
+        const CellWindow w = cell_window(cg, h, L, z0dz, npix, g.D, BP, BZ);
+        wins[L] = make_int4(w.p0, w.z0, w.zlast, w.empty | (w.ok << 1));
     }
     // The spare row BZ of each stage is never written by TMA; the look-ahead
     // read multiplies it by zero, so it must hold finite values (zeros).
@@ -186,7 +191,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
         mbar_wait_bounded(&bar[s], parity);
         CellWindow win;
         {
-            const int4 wi = winfo[s];
+            const int4 wi = wins[L];
             win.p0 = wi.x; win.z0 = wi.y; win.zlast = wi.z; win.empty = wi.w & 1; win.ok = wi.w >> 1;
         }
         if (active) {
