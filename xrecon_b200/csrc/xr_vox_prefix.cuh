@@ -193,25 +193,47 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                 const int r0 = __double2loint(t0);
                 const float f0 = (float)(u0 - n0), fib = (float)ib;
                 const int col = keep ? k : Nu - 1 - k;
-                // Byte offset of the entry for local row n is
-                //   ((r0 + 1 + n) * Nu + col) * 8 = bits(n + 1.5 * 2^23) * Nu8 + K
-                // in 32-bit arithmetic (the table of one view is < 2 GiB).
-                const unsigned K = (unsigned)(r0 + 1) * Nu8 + (unsigned)col * 8u - 0x4B400000u * Nu8;
+                // Address of the entry for local row n:
+                //   tvb + ((r0 + 1 + n) Nu + col) 8 = cb + bits(n + 1.5 * 2^23) Nu8
+                // with bits() read as unsigned: one wide multiply-add per lookup.
+                const char* cb = reinterpret_cast<const char*>(
+                    reinterpret_cast<uintptr_t>(tvb) +
+                    (uintptr_t)((long long)(r0 + 1) * Nu8 + (long long)col * 8 - 0x4B400000ll * (long long)Nu8));
                 const float wk = wf * lf * __frcp_rn(fib);
                 // rows the run reaches (local), inside [0, Nv - 1] in every active lane?
                 const bool inside = (u0 >= 0.0) && (u0 + R * ib <= (double)Nv - 1.0);
                 float gprev = 0.0f;
                 if (__all_sync(__activemask(), inside)) {
+                    // boundaries in pairs: the index arithmetic on packed FP32x2
+                    const float2 fib2 = make_float2(fib, fib), f02 = make_float2(f0, f0);
+                    const float2 mg2 = make_float2(12582912.0f, 12582912.0f);  // 1.5 * 2^23
+                    const float2 nmg2 = make_float2(-12582912.0f, -12582912.0f);
+                    const float2 neg2 = make_float2(-1.0f, -1.0f);
 #pragma unroll
-                    for (int i = 0; i <= R; ++i) {
-                        const float uc = fmaf((float)i, fib, f0);
-                        const float tr = uc + 12582912.0f;  // 1.5 * 2^23: round to nearest integer
-                        const float nf = tr - 12582912.0f;
-                        const float2 e = __ldg(reinterpret_cast<const float2*>(
-                            tvb + ((unsigned)__float_as_int(tr) * Nu8 + K)));
-                        const float gi = fmaf(uc - nf, e.y, e.x);
-                        if (i > 0) acc[i - 1] = fmaf(wk, gi - gprev, acc[i - 1]);
-                        gprev = gi;
+                    for (int i = 0; i <= R; i += 2) {
+                        if (i + 1 <= R) {
+                            const float2 u2 = __ffma2_rn(make_float2((float)i, (float)(i + 1)), fib2, f02);
+                            const float2 tr2 = __fadd2_rn(u2, mg2);   // round to nearest integer
+                            const float2 nf2 = __fadd2_rn(tr2, nmg2);
+                            const float2 fr2 = __ffma2_rn(nf2, neg2, u2);  // u - n
+                            const float2 ea = __ldg(reinterpret_cast<const float2*>(
+                                cb + (size_t)(unsigned)__float_as_int(tr2.x) * Nu8));
+                            const float2 eb = __ldg(reinterpret_cast<const float2*>(
+                                cb + (size_t)(unsigned)__float_as_int(tr2.y) * Nu8));
+                            const float ga = fmaf(fr2.x, ea.y, ea.x);
+                            const float gb = fmaf(fr2.y, eb.y, eb.x);
+                            if (i > 0) acc[i - 1] = fmaf(wk, ga - gprev, acc[i - 1]);
+                            acc[i] = fmaf(wk, gb - ga, acc[i]);
+                            gprev = gb;
+                        } else {
+                            const float uc = fmaf((float)i, fib, f0);
+                            const float tr = uc + 12582912.0f;
+                            const float nf = tr - 12582912.0f;
+                            const float2 e = __ldg(reinterpret_cast<const float2*>(
+                                cb + (size_t)(unsigned)__float_as_int(tr) * Nu8));
+                            const float gi = fmaf(uc - nf, e.y, e.x);
+                            acc[i - 1] = fmaf(wk, gi - gprev, acc[i - 1]);
+                        }
                     }
                 } else {
                     const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
@@ -221,7 +243,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                         const float tr = uc + 12582912.0f;
                         const float nf = tr - 12582912.0f;
                         const float2 e = __ldg(reinterpret_cast<const float2*>(
-                            tvb + ((unsigned)__float_as_int(tr) * Nu8 + K)));
+                            cb + (size_t)(unsigned)__float_as_int(tr) * Nu8));
                         const float gi = fmaf(uc - nf, e.y, e.x);
                         if (i > 0) acc[i - 1] = fmaf(wk, gi - gprev, acc[i - 1]);
                         gprev = gi;
