@@ -318,6 +318,8 @@ GeomF make_geomf(const Geom& g, int dim3d) {
     f.uscale = (dim3d && g.type == GEO_FLAT) ? (float)(g.sod / g.sdd) : 1.0f;
     f.shu = (float)g.shu;
     f.du = (float)g.du;
+    f.inv_uscale = 1.0f / f.uscale;
+    f.inv_du = (float)(1.0 / g.du);
     f.H = g.H;
     f.Nu = g.Nu;
     f.type = g.type;

@@ -301,6 +301,7 @@ struct GeomF {
     float xc0, yc0;    // centre of column 0 / row 0 (row 0 is the top)
     float dx, dy;
     float sod, uscale, shu, du;
+    float inv_uscale, inv_du;  // reciprocals for the column guess
     int H, Nu, type;
 };
 

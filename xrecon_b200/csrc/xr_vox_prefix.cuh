@@ -78,12 +78,12 @@ __device__ __forceinline__ float col_guess_fast(const GeomF& gf, const ViewHdr& 
     if (gf.type == GEO_FLAT) {
         const float R = gf.sod;
         const float u = __fdividef(R * (x * c + y * s), R + x * s - y * c);
-        sg = (u / gf.uscale - gf.shu) / gf.du;
+        sg = (u * gf.inv_uscale - gf.shu) * gf.inv_du;
     } else if (gf.type == GEO_ARC) {
         const float ex = x - (float)h.sx, ey = y - (float)h.sy;
-        sg = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) / gf.du;
+        sg = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * gf.inv_du;
     } else {
-        sg = (x * c + y * s - gf.shu) / gf.du;
+        sg = (x * c + y * s - gf.shu) * gf.inv_du;
     }
     return h.keep ? sg + 0.5f * gf.Nu : 0.5f * gf.Nu - sg;
 }
@@ -184,7 +184,10 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             do {
                 if (!(wf > 0.0f)) break;
                 const double ib = mvdv * Rq[k];  // detector rows per voxel
-                if (!(ib > 1.0e-4 && ib < 1.0e4)) break;
+                // keeps every local row index below 2^17, where the FP32
+                // round-to-nearest below is exact (geometries this extreme
+                // are far outside any scanner's)
+                if (!((float)ib < 4096.0f)) break;
                 // row coordinate of the run's bottom boundary, minus half a row
                 const double u0 = fma(zs, ib, zoffh);
                 if (u0 >= (double)Nv - 0.5 || u0 + R * ib <= -0.5) break;
