@@ -121,19 +121,28 @@ int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, in
 int xr_set_plain_kernels(int on);
 
 /*
- * Allocation-free variant of xr_dd2d (no reference counterpart: the
- * reference allocates its outputs and scratch per call).  Same operators,
- * layouts and results as xr_dd2d, but its scratch (per-view tables and the
- * flipped image transpose) is a fixed static device array of
- * XR_NOALLOC_SCRATCH_BYTES in the library, so the call never allocates or
- * frees device memory.  Requests that need more scratch than that (see
+ * Allocation-free variant of xr_dd2d.  It has no counterpart in the
+ * reference, which allocates its outputs and scratch on every call.
+ *
+ * Who needs it: a caller that cannot allocate device memory while it runs,
+ * such as a reconstruction service that reserves its whole device-memory
+ * budget at start-up, or code running inside a host framework that owns the
+ * device allocator.  For such callers a cudaMalloc in mid-run can fail, or
+ * stall the device while it waits for free memory.
+ *
+ * Same operators, layouts and results as xr_dd2d.  The caller still passes
+ * its inputs and outputs; the scratch (per-view tables and the flipped image
+ * transpose) lives in a fixed static device array of
+ * XR_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU that loads
+ * the library until the process exits.  No call allocates or frees device
+ * memory.  Requests that need more scratch than that (see
  * xr_dd2d_workspace_size) fail with XR_ERR_WORKSPACE.  Every scratch byte a
  * call reads is first written by the same call, so nothing needs clearing.
- * The first call on a device looks up the array's address
+ * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) and caches it; make that first call before any
  * stream capture.  There is one array per device: calls whose executions
- * overlap (different streams, or threads) race on it and must be serialised
- * by the caller.
+ * overlap on the GPU (different streams, or threads) race on it and must be
+ * serialised by the caller.
  */
 #define XR_NOALLOC_SCRATCH_BYTES (32u << 20)
 int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,

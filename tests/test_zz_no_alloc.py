@@ -1,7 +1,10 @@
-"""xr_dd2d_noalloc: the allocation-free 2D entry point, whose scratch is a
-fixed static device array inside the library.  Called through the C ABI and
-compared with xr_dd2d (caller workspace) on consecutive calls.  Named to be
-collected last, so it also runs after every other test has used the library.
+"""xr_dd2d_noalloc: the 2D entry point for callers that cannot allocate
+device memory while they run (a service with a device-memory budget fixed at
+start-up, or code inside a host framework that owns the device allocator).
+Its scratch is a fixed static device array inside the library.  Called
+through the C ABI and compared with xr_dd2d (caller workspace) on
+consecutive calls.  Named to be collected last, so that it also runs after
+every other test has used the library.
 """
 import ctypes
 import math

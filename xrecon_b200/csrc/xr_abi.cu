@@ -631,8 +631,11 @@ int ragged_tiles(const Geom& g, int nview, int list) {
     return (hw + px - 1) / px;
 }
 
-// Fixed device scratch of xr_dd2d_noalloc.  Its address is looked up once per
-// device (cudaGetSymbolAddress) and cached; nothing is ever allocated for it.
+// Fixed device scratch of xr_dd2d_noalloc, the entry for callers that cannot
+// allocate device memory mid-run.  Host code only sees a stand-in for this
+// name, so its device address is looked up once per device, with that
+// device current (cudaGetSymbolAddress), cached, and passed to the kernels;
+// nothing is ever allocated for it.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[XR_NOALLOC_SCRATCH_BYTES];
 
 int noalloc_scratch(void** ptr) {
