@@ -113,8 +113,9 @@ int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, i
 int xr_device_error(unsigned int* code, int clear);
 
 /* Staging plan of the 3D projection kernel for this geometry: whether the
- * TMA line windows are used and their box size (pixels x z voxels). */
-int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, int* rows_per_thread);
+ * TMA line windows are used, their box size (pixels x z voxels), and whether
+ * the fine-row kernel (detector rows shorter than a voxel) is chosen. */
+int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, int* rows_per_thread, int* fine);
 
 /* Testing aid: nonzero routes every operator through the plain (non-TMA)
  * kernels, so both paths can be compared. */

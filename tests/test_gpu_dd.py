@@ -163,6 +163,11 @@ def test_tma_and_plain_paths_match_oracle(cuda, scan):
     ang = (np.arange(0, 24) * (2 * np.pi / 24) + 0.02).astype(np.float32)
     ang = np.concatenate([ang, np.array([np.pi / 4, 3 * np.pi / 4], np.float32)])
     rng = np.random.default_rng(9)
+    if scan != "parallel":
+        # both projection kernels are exercised: rows finer than voxels in the
+        # first case, coarser in the second
+        plans = [_native.cell_plan(_native.geom3d_from_values(o.tolist())) for o in cases]
+        assert plans[0]["fine"] and not plans[1]["fine"], plans
     try:
         for opts in cases:
             D, H, W = int(opts[2]), int(opts[1]), int(opts[0])

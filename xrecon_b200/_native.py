@@ -67,7 +67,7 @@ def lib():
     L.xr_device_error.restype = c_int
     L.xr_device_error.argtypes = [ctypes.POINTER(ctypes.c_uint), c_int]
     L.xr_cell_plan.restype = c_int
-    L.xr_cell_plan.argtypes = [ctypes.POINTER(Geom3d)] + [ctypes.POINTER(c_int)] * 4
+    L.xr_cell_plan.argtypes = [ctypes.POINTER(Geom3d)] + [ctypes.POINTER(c_int)] * 5
     L.xr_set_plain_kernels.restype = c_int
     L.xr_set_plain_kernels.argtypes = [c_int]
     L.xr_last_error.restype = ctypes.c_char_p
@@ -220,12 +220,12 @@ def device_error(clear: bool = True) -> int:
 
 def cell_plan(geom: Geom3d) -> dict:
     """Staging plan of the 3D projection kernel (TMA box size) for a geometry."""
-    vals = [c_int(0) for _ in range(4)]
+    vals = [c_int(0) for _ in range(5)]
     rc = lib().xr_cell_plan(ctypes.byref(geom), *[ctypes.byref(v) for v in vals])
     if rc != 0:
         _raise(rc, "xr_cell_plan")
     return dict(ok=bool(vals[0].value), box_pixels=vals[1].value, box_z=vals[2].value,
-                rows_per_thread=vals[3].value)
+                rows_per_thread=vals[3].value, fine=bool(vals[4].value))
 
 
 def set_plain_kernels(on: bool) -> None:

@@ -127,6 +127,7 @@ struct Layout {
 struct CellPlan {
     bool ok;
     int BP, BZ, R;
+    bool fine;  // rows longer than a voxel are rare: the fine-only kernel
 };
 
 constexpr int CELL_NW = 8;
@@ -149,7 +150,8 @@ CellPlan plan_cell(const Geom& g) {
         auto it = cache.find(key);
         if (it != cache.end()) return it->second;
     }
-    CellPlan p{false, 0, 0, cell_rows_per_thread(g)};
+    CellPlan p{false, 0, 0, cell_rows_per_thread(g), false};
+    double coarse = 0.0, pairs = 0.0;
     const int RG = CELL_NW * p.R;
     const double uscale = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
     const double rs = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
@@ -173,6 +175,21 @@ CellPlan plan_cell(const Geom& g) {
             boundary_line_coeffs(g, h, D, A[k], B[k]);
         }
         for (int k = 0; k < g.Nu; ++k) Q[k] = column_mag(g, h, k, uscale) / g.dz;
+        {
+            // row length in voxels bt = Q_k q(L) dvv, q linear in L: the
+            // fraction of this view's (column, line) pairs with bt >= 0.999
+            const double n = (double)h.nlines;
+            for (int k = 0; k < g.Nu; ++k) {
+                const double a0 = std::fabs(Q[k] * dvv * h.q0);
+                const double a1 = std::fabs(Q[k] * dvv * (h.q0 + h.q1 * (n - 1.0)));
+                double f;
+                if (a0 >= 0.999 && a1 >= 0.999) f = 1.0;
+                else if (a0 < 0.999 && a1 < 0.999) f = 0.0;
+                else f = (std::max(a0, a1) - 0.999) / std::fabs(a1 - a0);
+                coarse += f;
+                pairs += 1.0;
+            }
+        }
         for (int k0 = 0; k0 < g.Nu; k0 += 32) {
             const int kend = std::min(k0 + 32, g.Nu);
             CellCtaGeo c;
@@ -193,6 +210,7 @@ CellPlan plan_cell(const Geom& g) {
             }
         }
     }
+    p.fine = pairs > 0.0 && coarse < 0.05 * pairs;
     p.BP = round_up(std::max(maxspan, 8), 8);
     p.BZ = (int)maxnz;
     p.ok = p.BP <= 256 && p.BZ <= 256 && p.BZ >= 1 &&
@@ -347,7 +365,7 @@ template <typename TI, typename TO, int R, int MODE>
 int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr, const CUtensorMap& mc,
                          const TI* rows, const TI* cols, int pitch_r, int pitch_c, TO* out, int nbatch, int nview,
                          const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
-    auto kern = cell_tma3d_kernel<TI, TO, R, 2, MODE>;
+    auto kern = p.fine ? cell_tma3d_kernel<TI, TO, R, 2, MODE, true> : cell_tma3d_kernel<TI, TO, R, 2, MODE, false>;
     const int maxlines = std::max(g.W, g.H);
     const size_t smem = 2 * (size_t)cell_stage_elems<TI>(p.BP, p.BZ) * sizeof(TI) + 16 + (size_t)maxlines * sizeof(int4);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -719,8 +737,8 @@ int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, i
 
 const char* xr_last_error(void) { return xr::g_last_error.c_str(); }
 
-int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, int* rows_per_thread) {
-    if (!geom || !ok || !box_pixels || !box_z || !rows_per_thread)
+int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, int* rows_per_thread, int* fine) {
+    if (!geom || !ok || !box_pixels || !box_z || !rows_per_thread || !fine)
         return xr::fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
     const xr::Geom g = xr::geom_from(geom);
     if (int rc = xr::validate(g, 1, 0, 1, 1)) return rc;
@@ -729,6 +747,7 @@ int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, in
     *box_pixels = p.BP;
     *box_z = p.BZ;
     *rows_per_thread = p.R;
+    *fine = p.fine;
     return XR_OK;
 }
 

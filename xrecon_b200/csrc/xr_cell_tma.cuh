@@ -88,7 +88,10 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
     return w;
 }
 
-template <typename TI, typename TO, int R, int NB, int MODE>
+// FINE: the geometry's detector rows are (nearly) all shorter than a voxel,
+// so only the fine-row walk is compiled; lines where it does not apply take
+// the global path.  Less code and fewer live registers than the full kernel.
+template <typename TI, typename TO, int R, int NB, int MODE, bool FINE>
 __global__ void __launch_bounds__(256, 2)
 cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUtensorMap map_rows,
                   const __grid_constant__ CUtensorMap map_cols, const TI* __restrict__ fb_rows,
@@ -264,7 +267,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                             acc[i] += a;
                             tcur = t1;
                         }
-                    } else if (win.ok) {
+                    } else if (!FINE && win.ok) {
                         // Staged voxels win.z0 .. win.zlast; below the window a
                         // single virtual zero voxel ends at win.z0, past
                         // win.zlast the value is zero and the next boundary
