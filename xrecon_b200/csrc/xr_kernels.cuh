@@ -490,6 +490,7 @@ __device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt,
     const double bA0 = vt.bA[ob], bB0 = vt.bB[ob], bA1 = vt.bA[ob + 1], bB1 = vt.bB[ob + 1];
     const int nlines = h.nlines, npix = h.npix;
     const TI* __restrict__ img = h.use_x ? img_rows : img_cols;
+    const float dpixf = (float)h.dpix;
     float acc = 0.0f;
     for (int L = l0; L < nlines; L += ls) {
         const double pk = fma(bB0, (double)L, bA0);
@@ -498,11 +499,14 @@ __device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt,
         const int pb = min((int)ceil(pk1) - 1, npix - 1);
         if (pa > pb) continue;
         float lf;
-        if (MODE == OP_A) lf = (float)(h.dpix / fma(h.q1, (double)L, h.q0));
+        if (MODE == OP_A) lf = __fdividef(dpixf, (float)fma(h.q1, (double)L, h.q0));
         else lf = cw;
         const TI* __restrict__ line = img + (size_t)L * npix;
+        // boundaries relative to the first pixel, so FP32 keeps them exact
+        const float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
         for (int pp = pa; pp <= pb; ++pp) {
-            float w = (float)(fmin((double)pp + 1.0, pk1) - fmax((double)pp, pk)) * lf;
+            const float o = (float)(pp - pa);
+            float w = (fminf(o + 1.0f, u1) - fmaxf(o, u0)) * lf;
             if (MODE == OP_BWT) {
                 float px, py;
                 pixel_center(g, h, L, pp, px, py);
@@ -535,41 +539,77 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
                                            const int ix, const int iy, const float cw, const int v0,
                                            const int v1, const int vs) {
     const int Nu = g.Nu;
+    // This pixel's edges and centre in world coordinates (the values
+    // line_point and pixel_center give), hoisted out of the view loop.
+    const float dxf = (float)g.dx, dyf = (float)g.dy;
+    const float xa_x = (float)(-0.5 * g.W * g.dx + g.shx) + (float)ix * dxf;   // x-axis views: x edges
+    const float yc_x = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);          //   and line centre
+    const float xc_y = (float)((ix - 0.5 * g.W + 0.5) * g.dx + g.shx);          // y-axis views: line centre
+    const float ya_y = (float)(-0.5 * g.H * g.dy + g.shy) + (float)(g.H - 1 - iy) * dyf;  //   and y edges
+    float pcx = 0.0f, pcy = 0.0f;
+    if (MODE == OP_BW) {
+        pcx = (float)((ix - 0.5 * g.W + 0.5) * g.dx + g.shx);
+        pcy = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);
+    }
+    const float sodf = (float)g.sod, shuf = (float)g.shu, inv_du = (float)(1.0 / g.du);
     float acc = 0.0f;
     for (int v = v0; v < v1; v += vs) {
-        const ViewHdr h = vt.hdr[v];
+        const ViewHdr& h = vt.hdr[v];
         int L, p;
-        if (h.use_x) { L = iy; p = ix; } else { L = ix; p = g.H - 1 - iy; }
+        float xa, ya, xb, yb;
+        if (h.use_x) {
+            L = iy; p = ix;
+            xa = xa_x; xb = xa_x + dxf; ya = yb = yc_x;
+        } else {
+            L = ix; p = g.H - 1 - iy;
+            xa = xb = xc_y; ya = ya_y; yb = ya_y + dyf;
+        }
         float lf;
         if (MODE == OP_AT) {
-            lf = (float)(h.dpix / fma(h.q1, (double)L, h.q0));
+            lf = __fdividef((float)h.dpix, (float)fma(h.q1, (double)L, h.q0));
         } else {
             lf = cw;
-            if (MODE == OP_BW) {
-                float px, py;
-                pixel_center(g, h, L, p, px, py);
-                lf *= fbp_weight(g, h, px, py);
-            }
+            if (MODE == OP_BW) lf *= fbp_weight(g, h, pcx, pcy);
         }
-        float xa, ya, xb, yb;
-        line_point(g, h, L, (float)p, xa, ya);
-        line_point(g, h, L, (float)(p + 1), xb, yb);
-        const float kf0 = col_guess(g, h, xa, ya, 1.0f), kf1 = col_guess(g, h, xb, yb, 1.0f);
+        // FP32 column guess (brackets the overlapped columns; the overlaps
+        // themselves come from the FP64 boundary tables)
+        const float sf = (float)h.s, cf = (float)h.c;
+        float kf0, kf1;
+        if (g.type == GEO_FLAT) {
+            kf0 = (__fdividef(sodf * (xa * cf + ya * sf), sodf + xa * sf - ya * cf) - shuf) * inv_du;
+            kf1 = (__fdividef(sodf * (xb * cf + yb * sf), sodf + xb * sf - yb * cf) - shuf) * inv_du;
+        } else if (g.type == GEO_ARC) {
+            float dcx, dcy;
+            sincosf((float)(h.beta + g.shu), &dcx, &dcy);
+            dcy = -dcy;
+            const float sxf = (float)h.sx, syf = (float)h.sy;
+            float ex = xa - sxf, ey = ya - syf;
+            kf0 = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
+            ex = xb - sxf; ey = yb - syf;
+            kf1 = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
+        } else {
+            kf0 = (xa * cf + ya * sf - shuf) * inv_du;
+            kf1 = (xb * cf + yb * sf - shuf) * inv_du;
+        }
+        if (h.keep) { kf0 += 0.5f * Nu; kf1 += 0.5f * Nu; }
+        else { kf0 = 0.5f * Nu - kf0; kf1 = 0.5f * Nu - kf1; }
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
-        const int ka = max(0, (int)floorf(lo) - 1);
-        const int kb = min(Nu - 1, (int)floorf(hi) + 1);
+        const int ka = max(0, (int)floorf(lo - 0.5f));
+        const int kb = min(Nu - 1, (int)floorf(hi + 0.5f));
         if (ka > kb) continue;
         const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
         const TI* __restrict__ sv = sinob + (size_t)v * Nu;
-        double pk = fma(bB[ka], (double)L, bA[ka]);
+        const double dp = (double)p, dL = (double)L;
+        // boundaries relative to the pixel (pixel units)
+        float pkl = (float)(fma(bB[ka], dL, bA[ka]) - dp);
         for (int k = ka; k <= kb; ++k) {
-            const double pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
-            const double wd = fmin((double)p + 1.0, pk1) - fmax((double)p, pk);
-            pk = pk1;
-            if (!(wd > 0.0)) continue;
-            float w = (float)wd * lf;
+            const float pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            const float wd = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
+            pkl = pk1;
+            if (!(wd > 0.0f)) continue;
+            float w = wd * lf;
             if (MODE == OP_AT) w *= vt.colE[(size_t)v * Nu + k];
             const int col = h.keep ? k : Nu - 1 - k;
             acc = fmaf(w, ld(sv + col), acc);
