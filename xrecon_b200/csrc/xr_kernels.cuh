@@ -552,6 +552,8 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
         pcy = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);
     }
     const float sodf = (float)g.sod, shuf = (float)g.shu, inv_du = (float)(1.0 / g.du);
+    // column bracket margin: half a column, plus the arc guess's angle error
+    const float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * inv_du : 0.0f);
     float acc = 0.0f;
     for (int v = v0; v < v1; v += vs) {
         const ViewHdr& h = vt.hdr[v];
@@ -584,9 +586,9 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
             dcy = -dcy;
             const float sxf = (float)h.sx, syf = (float)h.sy;
             float ex = xa - sxf, ey = ya - syf;
-            kf0 = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
+            kf0 = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
             ex = xb - sxf; ey = yb - syf;
-            kf1 = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
+            kf1 = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
         } else {
             kf0 = (xa * cf + ya * sf - shuf) * inv_du;
             kf1 = (xb * cf + yb * sf - shuf) * inv_du;
@@ -595,8 +597,8 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
         else { kf0 = 0.5f * Nu - kf0; kf1 = 0.5f * Nu - kf1; }
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
-        const int ka = max(0, (int)floorf(lo - 0.5f));
-        const int kb = min(Nu - 1, (int)floorf(hi + 0.5f));
+        const int ka = max(0, (int)floorf(lo - margin));
+        const int kb = min(Nu - 1, (int)floorf(hi + margin));
         if (ka > kb) continue;
         const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);

@@ -81,7 +81,7 @@ __device__ __forceinline__ float col_guess_fast(const GeomF& gf, const ViewHdr& 
         sg = (u * gf.inv_uscale - gf.shu) * gf.inv_du;
     } else if (gf.type == GEO_ARC) {
         const float ex = x - (float)h.sx, ey = y - (float)h.sy;
-        sg = atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * gf.inv_du;
+        sg = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * gf.inv_du;
     } else {
         sg = (x * c + y * s - gf.shu) * gf.inv_du;
     }
@@ -117,6 +117,8 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
     const double zs = (double)j0 + z0dz;  // run bottom, in voxel units from z = 0
     const double zoffh = -zd0 / dvv - 0.5;  // u0 = zs * (rows per voxel) + zoffh
     const float dpdz = (float)g.dz;
+    // column bracket margin: half a column, plus the arc guess's angle error
+    const float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * gf.inv_du : 0.0f);
     float acc[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) acc[i] = 0.0f;
@@ -160,8 +162,8 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         const float kf1 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xb, yb);
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
-        const int ka = max(0, (int)floorf(lo - 0.5f));
-        const int kb = min(Nu - 1, (int)floorf(hi + 0.5f));
+        const int ka = max(0, (int)floorf(lo - margin));
+        const int kb = min(Nu - 1, (int)floorf(hi + margin));
         if (ka > kb) continue;
         const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
