@@ -50,6 +50,7 @@ struct ViewHdr {
     double perpA, perpB;    // perpendicular coordinate of line L = perpA + perpB * L
     double q0, q1;          // 1 / Mv(L) = q0 + q1 * L   (1 for parallel)
     double dpix;            // pixel size along the line (dx or dy)
+    float dcx, dcy;         // arc detector: central ray direction (column guesses)
 };
 
 // Per-view tables, structure of arrays, view-major.
@@ -120,6 +121,8 @@ __host__ __device__ inline void make_view_hdr(const Geom& g, float ang, ViewHdr&
     if (g.type == GEO_PARALLEL) { h.q0 = 1.0; h.q1 = 0.0; }
     else { h.q0 = 1.0 - h.perpA / h.sperp; h.q1 = -h.perpB / h.sperp; }
     h.dpix = h.use_x ? g.dx : g.dy;
+    h.dcx = (float)sin(h.beta + g.shu);
+    h.dcy = (float)(-cos(h.beta + g.shu));
 }
 
 // Column-centre z magnification M_k onto the axis plane (forward3d.cpp:258-297).
@@ -263,13 +266,13 @@ __device__ __forceinline__ void line_point(const Geom& g, const ViewHdr& h, int 
 __device__ __forceinline__ float fbp_weight(const Geom& g, const ViewHdr& h, float px, float py) {
     if (g.type == GEO_FLAT) {
         const float R = (float)g.sod;
-        const float d = ((float)h.sx * px + (float)h.sy * py) / R;
+        const float d = __fdividef((float)h.sx * px + (float)h.sy * py, R);
         const float den = R - d;
-        return R * R / (den * den);
+        return __fdividef(R * R, den * den);
     }
     if (g.type == GEO_ARC) {
         const float ex = (float)h.sx - px, ey = (float)h.sy - py;
-        return 1.0f / (ex * ex + ey * ey);
+        return __fdividef(1.0f, ex * ex + ey * ey);
     }
     return 1.0f;
 }

@@ -581,9 +581,7 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
             kf0 = (__fdividef(sodf * (xa * cf + ya * sf), sodf + xa * sf - ya * cf) - shuf) * inv_du;
             kf1 = (__fdividef(sodf * (xb * cf + yb * sf), sodf + xb * sf - yb * cf) - shuf) * inv_du;
         } else if (g.type == GEO_ARC) {
-            float dcx, dcy;
-            sincosf((float)(h.beta + g.shu), &dcx, &dcy);
-            dcy = -dcy;
+            const float dcx = h.dcx, dcy = h.dcy;
             const float sxf = (float)h.sx, syf = (float)h.sy;
             float ex = xa - sxf, ey = ya - syf;
             kf0 = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;

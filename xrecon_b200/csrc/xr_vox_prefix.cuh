@@ -153,11 +153,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         }
         lf *= oscale;
         const float sf = (float)h.s, cf = (float)h.c;
-        float dcx = 0.0f, dcy = 0.0f;
-        if (gf.type == GEO_ARC) {
-            sincosf((float)h.beta + gf.shu, &dcx, &dcy);
-            dcy = -dcy;
-        }
+        const float dcx = h.dcx, dcy = h.dcy;
         const float kf0 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xa, ya);
         const float kf1 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xb, yb);
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
