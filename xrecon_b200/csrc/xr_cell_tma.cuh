@@ -91,8 +91,11 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
 // FINE: the geometry's detector rows are (nearly) all shorter than a voxel,
 // so only the fine-row walk is compiled; lines where it does not apply take
 // the global path.  Less code and fewer live registers than the full kernel.
+#ifndef XR_CELL_MINB
+#define XR_CELL_MINB 2  // CTAs per SM the register budget is sized for
+#endif
 template <typename TI, typename TO, int R, int NB, int MODE, bool FINE>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, XR_CELL_MINB)
 cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUtensorMap map_rows,
                   const __grid_constant__ CUtensorMap map_cols, const TI* __restrict__ fb_rows,
                   const TI* __restrict__ fb_cols, const int pitch_rows, const int pitch_cols,
