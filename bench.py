@@ -211,6 +211,34 @@ def run_reference_arm(args, rank: int):
 
 # ---------------------------------------------------------------- GPU arm
 
+def operator_times(P, vol, ang, nv, reps: int = 2):
+    """Every operator and the FDK on the same workload (FP32), each timed
+    alone with CUDA events: ms per application and Gvoxel-views/s."""
+    import torch
+    sino = P.projection(vol, ang)
+    ops = {
+        "projection_t (A^T)": lambda: P.projection_t(sino, ang),
+        "backprojection_weighted (Bw)": lambda: P.backprojection_weighted(sino, ang),
+        "backprojection_t (B^T)": lambda: P.backprojection_t(vol, ang),
+        "backprojection_weighted_t (Bw^T)": lambda: P.backprojection_weighted_t(vol, ang),
+        "filtered_backprojection (FDK)": lambda: P.filtered_backprojection(sino, ang),
+    }
+    out = {}
+    for name, fn in ops.items():
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": ms, "gvoxel_views_per_s": nvox() * nv / (ms / 1e3) / 1e9}
+    del sino
+    return out
+
+
 def ragged_measure(dev, reps: int = 5):
     """The 64-instance ragged fan-arc batch: projection + FBP of every
     instance as one autotuned persistent launch replayed from a CUDA graph,
@@ -393,6 +421,8 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
     }
     if bf:
         line["bf16"] = bf
+    if not args.no_ops:
+        line["operators"] = operator_times(P, vol, ang, nv)
     if not args.no_ragged and world == 1:
         line["ragged_fan_arc_batch"] = ragged_measure(dev)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -413,6 +443,7 @@ def main():
     ap.add_argument("--no-bf16", action="store_true", help="skip the BF16-storage measurement")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged 2D batch measurement")
+    ap.add_argument("--no-ops", action="store_true", help="skip the per-operator timings")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
     args = ap.parse_args()

@@ -715,22 +715,25 @@ int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, i
     if (nrows == 0) return XR_OK;
     if (!xr::dtype_ok(dtype_in)) return xr::fail(XR_ERR_INVALID_ARGUMENT, "unsupported dtype %d", dtype_in);
     constexpr int OUTS = 8;
-    const size_t smem = (size_t)(3 * Nu + 2 * OUTS) * sizeof(float);
+    // threads per row (a warp multiple covering Nu / 8 outputs), rows per CTA
+    const int tpr = std::min(256, ((Nu + OUTS - 1) / OUTS + 31) / 32 * 32);
+    const int rpc = std::max(1, 256 / tpr);
+    const size_t smem = ((size_t)(xr::filt_taps_smem(Nu) + 3) / 4 * 4 + (size_t)rpc * xr::filt_row_pitch(Nu)) * sizeof(float);
     if (smem > 200 * 1024) return xr::fail(XR_ERR_UNSUPPORTED, "detector width %d too large for the filter kernel", Nu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int grid = std::min(nrows, 148 * 8);
+    const int grid = std::min((nrows + rpc - 1) / rpc, 148 * 8);
     if (dtype_in == xr::DT_F32) {
         auto k = xr::fbp_filter_kernel<float, OUTS>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, 256, smem, st>>>(static_cast<const float*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker);
+        k<<<grid, 256, smem, st>>>(static_cast<const float*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker, tpr, rpc);
     } else if (dtype_in == xr::DT_BF16) {
         auto k = xr::fbp_filter_kernel<__nv_bfloat16, OUTS>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, 256, smem, st>>>(static_cast<const __nv_bfloat16*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker);
+        k<<<grid, 256, smem, st>>>(static_cast<const __nv_bfloat16*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker, tpr, rpc);
     } else {
         auto k = xr::fbp_filter_kernel<__half, OUTS>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, 256, smem, st>>>(static_cast<const __half*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker);
+        k<<<grid, 256, smem, st>>>(static_cast<const __half*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker, tpr, rpc);
     }
     return xr::check_cuda("fbp_filter");
 }

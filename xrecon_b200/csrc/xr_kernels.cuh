@@ -621,53 +621,77 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
 // -------------------------------------------------------------- FBP filter
 
 // out[row, i] = sum_j x[row, j] * filt[j - i + Nu - 1], x = in * cosw * parker.
-// One CTA per detector row at a time; each thread produces OUTS consecutive
-// outputs with the filter window kept in registers.
+// A CTA takes `rpc` rows at a time; `tpr` threads per row, each producing 8
+// consecutive outputs.  The inner loop runs over blocks of 8 inputs (two
+// float4 loads of the row, broadcast to the warp) against a 15-tap register
+// window of the filter that advances 8 taps per block: 64 FMAs per 10 shared
+// loads.  Taps and rows are zero-padded in shared memory, so the loop has no
+// bounds checks.  Neighbouring lanes' windows start 8 taps apart, so the taps
+// are stored with one padding float after every 32 (tap i at i + i / 32):
+// lanes 4 apart then fall one bank apart instead of on the same bank.
+constexpr int XR_FILT_PAD = 32;  // zero taps on each side of the filter
+
+__host__ __device__ inline int filt_row_pitch(int Nu) { return (Nu + 7) / 8 * 8 + 8; }
+__host__ __device__ inline int filt_taps_len(int Nu) { return 2 * ((Nu + 7) / 8 * 8) + 2 * XR_FILT_PAD + 16; }
+// shared-memory floats holding filt_taps_len taps in the padded layout
+__host__ __device__ inline int filt_taps_smem(int Nu) { const int n = filt_taps_len(Nu); return n + n / 32 + 1; }
+__device__ __forceinline__ int tap_pos(int i) { return i + (i >> 5); }
+
 template <typename TI, int OUTS>
 __global__ void __launch_bounds__(256)
 fbp_filter_kernel(const TI* __restrict__ in, float* __restrict__ out, const int nrows, const int Nu,
                   const int nview, const int rows_per_view, const float* __restrict__ cosw,
-                  const float* __restrict__ filt, const float* __restrict__ parker) {
-    extern __shared__ float smem[];
-    float* f = smem;              // 2*Nu - 1 (+ OUTS padding)
-    float* x = smem + 2 * Nu + OUTS;  // Nu (+ OUTS padding)
+                  const float* __restrict__ filt, const float* __restrict__ parker, const int tpr, const int rpc) {
+    static_assert(OUTS == 8, "the register window below is written for 8 outputs per thread");
+    extern __shared__ __align__(16) float smem[];
     const int nf = 2 * Nu - 1;
-    for (int i = threadIdx.x; i < nf + OUTS + 1; i += blockDim.x) f[i] = (i < nf) ? filt[i] : 0.0f;
-    for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
-        const int view = (row / rows_per_view) % nview;
-        const TI* src = in + (size_t)row * Nu;
+    const int ntap = filt_taps_len(Nu);
+    const int pitch = filt_row_pitch(Nu);
+    float* fp = smem;                               // fp[tap_pos(XR_FILT_PAD + m)] = filt[m]
+    float* xs = smem + (filt_taps_smem(Nu) + 3) / 4 * 4;  // rpc rows of `pitch` floats
+    for (int i = threadIdx.x; i < ntap; i += blockDim.x) {
+        const int m = i - XR_FILT_PAD;
+        fp[tap_pos(i)] = (m >= 0 && m < nf) ? filt[m] : 0.0f;
+    }
+    const int r = threadIdx.x / tpr, tl = threadIdx.x - r * tpr;
+    for (int row0 = blockIdx.x * rpc; row0 < nrows; row0 += gridDim.x * rpc) {
         __syncthreads();
-        for (int j = threadIdx.x; j < Nu + OUTS; j += blockDim.x) {
+        for (int e = threadIdx.x; e < rpc * pitch; e += blockDim.x) {
+            const int rr = e / pitch, j = e - rr * pitch;
+            const int row = row0 + rr;
             float val = 0.0f;
-            if (j < Nu) {
-                val = ld(src + j);
+            if (j < Nu && row < nrows) {
+                val = ld(in + (size_t)row * Nu + j);
                 if (cosw) val *= cosw[j];
-                if (parker) val *= parker[(size_t)view * Nu + j];
+                if (parker) val *= parker[(size_t)((row / rows_per_view) % nview) * Nu + j];
             }
-            x[j] = val;
+            xs[e] = val;
         }
         __syncthreads();
-        for (int i0 = threadIdx.x * OUTS; i0 < Nu; i0 += blockDim.x * OUTS) {
-            // out[i0 + t] = sum_j x[j] * f[j + Nu - 1 - i0 - t]
+        const int row = row0 + r;
+        if (r >= rpc || row >= nrows) continue;
+        const float* xr = xs + r * pitch;
+        for (int i0 = tl * OUTS; i0 < Nu; i0 += tpr * OUTS) {
+            // out[i0 + t] = sum_j x[j] fb[j - t],  fb[m] = filt[m + Nu - 1 - i0]
+            const int fb0 = XR_FILT_PAD + (Nu - 1 - i0);  // tap index of fb[0]
             float acc[OUTS];
-            float win[OUTS];
 #pragma unroll
             for (int t = 0; t < OUTS; ++t) acc[t] = 0.0f;
-            // window for j = 0: win[t] = f[Nu - 1 - i0 - t] (index may be < 0 -> treat as 0)
+            float w[15];  // w[k] = fb[jb - 7 + k]
 #pragma unroll
-            for (int t = 0; t < OUTS; ++t) {
-                const int fi = Nu - 1 - i0 - t;
-                win[t] = (fi >= 0) ? f[fi] : 0.0f;
-            }
-            for (int j = 0; j < Nu; ++j) {
-                const float xj = x[j];
+            for (int k = 0; k < 7; ++k) w[k] = fp[tap_pos(fb0 + k - 7)];
+            for (int jb = 0; jb < Nu; jb += 8) {
+                const float4 xa = *reinterpret_cast<const float4*>(xr + jb);
+                const float4 xb = *reinterpret_cast<const float4*>(xr + jb + 4);
+                const float x8[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
 #pragma unroll
-                for (int t = 0; t < OUTS; ++t) acc[t] = fmaf(xj, win[t], acc[t]);
-                // shift: next j uses f[j + 1 + Nu - 1 - i0 - t] = old win[t - 1]
+                for (int k = 0; k < 8; ++k) w[7 + k] = fp[tap_pos(fb0 + jb + k)];
 #pragma unroll
-                for (int t = OUTS - 1; t > 0; --t) win[t] = win[t - 1];
-                const int fi = j + Nu - i0;  // = (j + 1) + Nu - 1 - i0 - 0
-                win[0] = (fi < nf) ? f[fi] : 0.0f;
+                for (int jj = 0; jj < 8; ++jj)
+#pragma unroll
+                    for (int t = 0; t < OUTS; ++t) acc[t] = fmaf(x8[jj], w[jj - t + 7], acc[t]);
+#pragma unroll
+                for (int k = 0; k < 7; ++k) w[k] = w[k + 8];
             }
 #pragma unroll
             for (int t = 0; t < OUTS; ++t)
