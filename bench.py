@@ -239,6 +239,31 @@ def operator_times(P, vol, ang, nv, reps: int = 2):
     return out
 
 
+def sysmat_measure(dev, reps: int = 3):
+    """Sparse projection-matrix export (count, scan, fill, coalesce) of the
+    2D fan-flat geometry: 256x256 image of 1 mm, 720 views over 2 pi, 256
+    cells of 2 mm, SOD 500, SDD 1000."""
+    import numpy as np
+    import torch
+    from xrecon_b200 import geometry as G
+    from xrecon_b200.projector import Projector2d
+    P = Projector2d(G.Volume2d(256, 1.0), G.FanBeam2d(G.Detector2d(256, 2.0), 500.0, 1000.0, "flat")).to(dev)
+    ang = torch.from_numpy((np.arange(720) * (2 * np.pi / 720)).astype(np.float32)).to(dev)
+    M = P.system_matrix(ang)
+    nnz = M._nnz()
+    del M
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        M = P.system_matrix(ang)
+        del M
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return {"nnz": nnz, "ms": ms, "gnnz_per_s": nnz / (ms / 1e3) / 1e9}
+
+
 def ragged_measure(dev, reps: int = 5):
     """The 64-instance ragged fan-arc batch: projection + FBP of every
     instance as one autotuned persistent launch replayed from a CUDA graph,
@@ -425,6 +450,8 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         line["operators"] = operator_times(P, vol, ang, nv)
     if not args.no_ragged and world == 1:
         line["ragged_fan_arc_batch"] = ragged_measure(dev)
+    if not args.no_sysmat and world == 1:
+        line["system_matrix_2d_fan_flat"] = sysmat_measure(dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         sample = cpu_reference_sample(4, vol.cpu().numpy())
         line["cpu_baseline"] = {k: v for k, v in sample.items() if k != "seconds"} if sample else None
@@ -444,6 +471,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged 2D batch measurement")
     ap.add_argument("--no-ops", action="store_true", help="skip the per-operator timings")
+    ap.add_argument("--no-sysmat", action="store_true", help="skip the system-matrix export timing")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
     args = ap.parse_args()

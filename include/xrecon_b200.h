@@ -150,6 +150,28 @@ int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in,
                     const float* angles, int nbatch, int nview, void* stream);
 
 /*
+ * Sparse export of the projection matrix A (replaces system_matrix2d /
+ * system_matrix3d, torch_binding.cpp:353-405, which build it on the CPU with
+ * src/cpu/system_matrix2d.cpp and src/cpu/system_matrix3d.cpp).  Two passes
+ * over the cells, numbered c = (view * Nv + det_row) * Nu + k with k the
+ * traversal-order column (2D: Nv = 1):
+ *   offsets == NULL : counts[c] = number of nonzero weights of cell c;
+ *   offsets != NULL : the weights of cell c are written at rows/cols/vals
+ *                     [offsets[c], offsets[c] + counts[c]) (offsets is the
+ *                     exclusive scan of counts).
+ * Entries: row = (view * Nv + det_row) * Nu + physical column, col = voxel
+ * index (iz * H + iy) * W + ix, value = the projection's weight (FP32), so
+ * that the matrix times the flattened image equals xr_dd*d(XR_PROJECTION).
+ * Zero weights are skipped, as in the reference.  angles: device [nview].
+ */
+size_t xr_sysmat2d_workspace_size(const xr_geom2d* geom, int nview);
+size_t xr_sysmat3d_workspace_size(const xr_geom3d* geom, int nview);
+int xr_sysmat2d(const xr_geom2d* geom, const float* angles, int nview, const long long* offsets, long long* counts,
+                long long* rows, long long* cols, float* vals, void* workspace, size_t workspace_bytes, void* stream);
+int xr_sysmat3d(const xr_geom3d* geom, const float* angles, int nview, const long long* offsets, long long* counts,
+                long long* rows, long long* cols, float* vals, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * Ragged batch of 2D reconstructions: projection then FBP for many
  * instances with different geometries, image sizes, view counts and
  * detectors, in one persistent cooperative kernel launch (no reference

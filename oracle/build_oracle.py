@@ -2,12 +2,12 @@
 
 * ``oracle/lib/libxr_oracle.so`` -- the FP64 C restatement ``dd_oracle.c``.
 * ``oracle/_ref/libxrecon_ref_cpu.so`` -- the reference's own CPU operators
-  (XRecon ``src/cpu/{forward2d,backward2d,system_matrix2d,forward3d,
-  backward3d}.cpp``) compiled in place from the reference sources together with
+  (XRecon ``src/cpu/{forward2d,backward2d,system_matrix2d,system_matrix3d,
+  forward3d,backward3d}.cpp``) compiled in place from the reference sources together with
   ``ref_shim.cpp``.  Built only where the reference tree is present; the
   resulting .so travels with the repository snapshot (it is git-ignored).
 
-The reference's own build system is not used: its CPU path is five C++ files
+The reference's own build system is not used: its CPU path is six C++ files
 that only need the reference ``include/`` directory and the CUDA headers for
 the ``__host__ __device__`` qualifiers of ``include/types.h``.
 """
@@ -24,7 +24,7 @@ REF_DIR = HERE / "_ref"
 ORACLE_SO = LIB_DIR / "libxr_oracle.so"
 REF_SO = REF_DIR / "libxrecon_ref_cpu.so"
 REFERENCE_ROOT = Path(os.environ.get("XRECON_REFERENCE_ROOT", "/root/reference"))
-REF_CPU_SOURCES = ["forward2d.cpp", "backward2d.cpp", "system_matrix2d.cpp",
+REF_CPU_SOURCES = ["forward2d.cpp", "backward2d.cpp", "system_matrix2d.cpp", "system_matrix3d.cpp",
                    "forward3d.cpp", "backward3d.cpp"]
 CUDA_INCLUDE = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "include"
 

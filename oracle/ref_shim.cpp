@@ -8,6 +8,8 @@
 // builds the reference's Volume/Geometry structs (include/types.h:35-119)
 // from plain scalars, exactly as the reference binding does after unpacking
 // the options tensor (src/api/torch_binding.cpp:62-124).
+#include <vector>
+
 #include "types.h"
 #include "functions.h"
 
@@ -77,6 +79,36 @@ int xr_ref_dd3d(int op, float* image, float* proj, float* ang,
     case 5: xrecon::weighted_backward3d_t_cpu(proj, image, ang, vol, geo, nbatch, nview); return 0;
     default: return 1;
     }
+}
+
+// System matrix of the projection (system_matrix2d_cpu /
+// system_matrix3d_cpu, include/functions.h:92-118): fills at most `cap`
+// triplets and returns their total count (call again with a larger buffer
+// when the count exceeds cap), or -1 on an unknown geometry.
+long long xr_ref_sysmat2d(float* ang, int W, int H, float dx, float dy, float shx, float shy, int type, int Nu,
+                          float du, float shu, float sod, float sdd, int nview, long long* rows, long long* cols,
+                          float* vals, long long cap)
+{
+    if (type < 0 || type > 2) return -1;
+    std::vector<int64_t> r, c;
+    std::vector<float> v;
+    xrecon::system_matrix2d_cpu(r, c, v, ang, make_vol2d(W, H, dx, dy, shx, shy),
+                                make_geo2d(type, Nu, du, shu, sod, sdd), nview);
+    const long long n = (long long)v.size();
+    for (long long i = 0; i < n && i < cap; ++i) { rows[i] = r[i]; cols[i] = c[i]; vals[i] = v[i]; }
+    return n;
+}
+
+long long xr_ref_sysmat3d(float* ang, const int* ni, const float* fv, const float* fg, int type, int nview,
+                          long long* rows, long long* cols, float* vals, long long cap)
+{
+    if (type < 0 || type > 2) return -1;
+    std::vector<int64_t> r, c;
+    std::vector<float> v;
+    xrecon::system_matrix3d_cpu(r, c, v, ang, make_vol3d(ni, fv), make_geo3d(type, ni + 3, fg), nview);
+    const long long n = (long long)v.size();
+    for (long long i = 0; i < n && i < cap; ++i) { rows[i] = r[i]; cols[i] = c[i]; vals[i] = v[i]; }
+    return n;
 }
 
 }  // extern "C"

@@ -44,6 +44,16 @@ def _load():
         lib.xr_ref_dd3d.argtypes = ([ctypes.c_int] + [ctypes.POINTER(ctypes.c_float)] * 3 +
                                     [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
                                      ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int, ctypes.c_int])
+        lib.xr_ref_sysmat2d.restype = ctypes.c_longlong
+        lib.xr_ref_sysmat2d.argtypes = ([ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int] +
+                                        [ctypes.c_float] * 4 + [ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 4 +
+                                        [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_longlong])
+        lib.xr_ref_sysmat3d.restype = ctypes.c_longlong
+        lib.xr_ref_sysmat3d.argtypes = ([ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_longlong])
         _lib = lib
     return _lib
 
@@ -123,3 +133,35 @@ class RefXreconC:
     def weighted_backward_projection3d(self, x, o, a): return self._wrap(dd3d, "BW", x, o, a)
     def backward_projection_transpose3d(self, x, o, a): return self._wrap(dd3d, "BT", x, o, a)
     def weighted_backward_projection_transpose3d(self, x, o, a): return self._wrap(dd3d, "BWT", x, o, a)
+
+
+def system_matrix(dim: int, options, angles):
+    """The reference's system_matrix2d_cpu / system_matrix3d_cpu triplets
+    (rows, cols, vals) as numpy arrays, unsorted, and the matrix shape."""
+    ang = np.ascontiguousarray(angles, dtype=np.float32)
+    V = ang.shape[0]
+    L = _load()
+    cap = 0
+    while True:
+        rows = np.zeros(max(cap, 1), np.int64)
+        cols = np.zeros(max(cap, 1), np.int64)
+        vals = np.zeros(max(cap, 1), np.float32)
+        args = (rows.ctypes.data, cols.ctypes.data, vals.ctypes.data, cap)
+        if dim == 2:
+            g = unpack2d(options)
+            n = L.xr_ref_sysmat2d(_fp(ang), g["W"], g["H"], g["dx"], g["dy"], g["shx"], g["shy"], g["type"],
+                                  g["Nu"], g["du"], g["shu"], g["SOD"], g["SDD"], V, *args)
+            shape = (V * g["Nu"], g["H"] * g["W"])
+        else:
+            g = unpack3d(options)
+            ni = np.array([g["W"], g["H"], g["D"], g["Nu"], g["Nv"]], dtype=np.int32)
+            fv = np.array([g["dx"], g["dy"], g["dz"], g["shx"], g["shy"], g["shz"]], dtype=np.float32)
+            fg = np.array([g["du"], g["dv"], g["shu"], g["shv"], g["SOD"], g["SDD"]], dtype=np.float32)
+            n = L.xr_ref_sysmat3d(_fp(ang), ni.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _fp(fv), _fp(fg),
+                                  g["type"], V, *args)
+            shape = (V * g["Nv"] * g["Nu"], g["D"] * g["H"] * g["W"])
+        if n < 0:
+            raise RuntimeError("reference system matrix failed")
+        if n <= cap:
+            return rows[:n], cols[:n], vals[:n], shape
+        cap = int(n)

@@ -17,7 +17,10 @@ from the reference's code path on CPU:
 * fbp2d_<case>.npz / fdk3d_<case>.npz: Projector.filtered_backprojection
   results (TF32 is irrelevant: this is the CPU conv path);
 * options.npz: the packed options vectors of Projector2d/3d for the benchmark
-  geometries; filters.npz: the filter tables.
+  geometries; filters.npz: the filter tables;
+* sysmat{2,3}d_<geom>.npz: the reference's sparse projection matrices
+  (system_matrix2d_cpu / system_matrix3d_cpu) for small shifted geometries
+  (``python tests/golden/make_golden.py sysmat`` writes only these).
 """
 from __future__ import annotations
 
@@ -153,5 +156,30 @@ def main():
     print("fixtures written to", HERE)
 
 
+def make_sysmat():
+    """sysmat{2,3}d_<geom>.npz: the reference's system_matrix2d/3d triplets
+    (its own CPU code through oracle/_ref) for small shifted geometries."""
+    P2, P3, G, F = import_reference()
+    ang = angles_set(10, 0.2)
+    for scan in ("parallel", "flat", "arc"):
+        if scan == "parallel":
+            geo2 = G.ParallelBeam2d(G.Detector2d(32, 1.1, 0.4))
+            geo3 = G.ParallelBeam3d(G.Detector3d((16, 6), (1.1, 0.9), (0.3, -0.4)))
+        else:
+            geo2 = G.FanBeam2d(G.Detector2d(32, 2.0, 0.4), 300.0, 600.0, scan)
+            geo3 = G.ConeBeam3d(G.Detector3d((16, 6), (1.6, 1.4), (0.3, -0.4)), 300.0, 600.0, scan)
+        for dim, P in ((2, P2(G.Volume2d((24, 20), (1.0, 1.1), (0.5, -0.5)), geo2)),
+                       (3, P3(G.Volume3d((12, 10, 6), (1.0, 1.1, 1.2), (0.5, -0.5, 0.5)), geo3))):
+            opts = P.options.numpy()
+            r, c, v, shape = refcpu.system_matrix(dim, opts, ang)
+            np.savez_compressed(HERE / f"sysmat{dim}d_{scan}.npz", options=opts, angles=ang, rows=r, cols=c,
+                                vals=v, shape=np.array(shape, np.int64))
+    print("system-matrix fixtures written to", HERE)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["sysmat"]:
+        make_sysmat()
+    else:
+        main()
+        make_sysmat()

@@ -75,3 +75,21 @@ def test_oracle_reference_library_when_present():
     a = O.dd3d("A", x, g["options"], g["angles"])
     b = refcpu.dd3d("A", x, g["options"], g["angles"])
     assert rel_l2(b, a) < 1e-5
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_reference_system_matrix_is_the_oracle_projection(dim, scan):
+    """The reference's sparse projection matrix (fixture) times an image is
+    the oracle's projection: pins the matrix conventions (rows: view, detector
+    row, physical column; columns: flattened voxels)."""
+    g = load_golden(f"sysmat{dim}d_{scan}")
+    shape = tuple(int(s) for s in g["shape"])
+    M = np.zeros(shape)
+    np.add.at(M, (g["rows"], g["cols"]), g["vals"])
+    rng = np.random.default_rng(4)
+    o = g["options"]
+    img_shape = (1, 1, int(o[1]), int(o[0])) if dim == 2 else (1, 1, int(o[2]), int(o[1]), int(o[0]))
+    x = rng.random(img_shape)
+    exact = (O.dd2d if dim == 2 else O.dd3d)("A", x, o, g["angles"]).reshape(-1)
+    assert rel_l2(M @ x.reshape(-1), exact) < TOL[scan]

@@ -71,6 +71,13 @@ def lib():
     L.xr_set_plain_kernels.restype = c_int
     L.xr_set_plain_kernels.argtypes = [c_int]
     L.xr_last_error.restype = ctypes.c_char_p
+    for d, G in ((2, Geom2d), (3, Geom3d)):
+        ws = getattr(L, f"xr_sysmat{d}d_workspace_size")
+        ws.restype = c_size_t
+        ws.argtypes = [ctypes.POINTER(G), c_int]
+        fn = getattr(L, f"xr_sysmat{d}d")
+        fn.restype = c_int
+        fn.argtypes = [ctypes.POINTER(G), c_void_p, c_int] + [c_void_p] * 5 + [c_void_p, c_size_t, c_void_p]
     L.xr_launch_count.restype = ctypes.c_ulonglong
     L.xr_launch_count.argtypes = []
     L.xr_version.restype = ctypes.c_char_p
@@ -207,6 +214,44 @@ def fbp_filter(sino: torch.Tensor, nview: int, rows_per_view: int, cosw: torch.T
     if rc != 0:
         _raise(rc, "xr_fbp_filter")
     return out
+
+
+def system_matrix(dim: int, geom, angles: torch.Tensor, device) -> torch.Tensor:
+    """Sparse COO matrix of the projection (rows: view, detector row, column;
+    columns: voxels), built on ``device`` in two passes (count, scan, fill)
+    and coalesced, as the reference's system_matrix2d/3d returns it."""
+    L = lib()
+    dev = torch.device(device)
+    ang = _angles(angles, dev)
+    V = ang.numel()
+    if V == 0:
+        raise RuntimeError("system matrix needs at least one view")
+    Nv = geom.Nv if dim == 3 else 1
+    D = geom.D if dim == 3 else 1
+    ncell = V * Nv * geom.Nu
+    with torch.cuda.device(dev):
+        nbytes = getattr(L, f"xr_sysmat{dim}d_workspace_size")(ctypes.byref(geom), V)
+        ws = _workspace(nbytes, dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        fn = getattr(L, f"xr_sysmat{dim}d")
+        counts = torch.empty(ncell, dtype=torch.int64, device=dev)
+        rc = fn(ctypes.byref(geom), ang.data_ptr(), V, None, counts.data_ptr(), None, None, None,
+                ws.data_ptr(), ws.numel(), stream)
+        if rc != 0:
+            _raise(rc, f"xr_sysmat{dim}d (count)")
+        ends = torch.cumsum(counts, 0)
+        nnz = int(ends[-1].item())
+        offsets = ends - counts
+        rows = torch.empty(nnz, dtype=torch.int64, device=dev)
+        cols = torch.empty(nnz, dtype=torch.int64, device=dev)
+        vals = torch.empty(nnz, dtype=torch.float32, device=dev)
+        if nnz:
+            rc = fn(ctypes.byref(geom), ang.data_ptr(), V, offsets.data_ptr(), counts.data_ptr(), rows.data_ptr(),
+                    cols.data_ptr(), vals.data_ptr(), ws.data_ptr(), ws.numel(), stream)
+            if rc != 0:
+                _raise(rc, f"xr_sysmat{dim}d (fill)")
+        shape = (V * Nv * geom.Nu, D * geom.H * geom.W)
+        return torch.sparse_coo_tensor(torch.stack([rows, cols]), vals, shape, check_invariants=False).coalesce()
 
 
 def device_error(clear: bool = True) -> int:

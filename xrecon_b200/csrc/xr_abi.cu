@@ -19,6 +19,7 @@
 #include "xr_cell_tma.cuh"
 #include "xr_vox_prefix.cuh"
 #include "xr_ragged.cuh"
+#include "xr_sysmat.cuh"
 #include "../../include/xrecon_b200.h"
 
 
@@ -612,6 +613,43 @@ int apply(int dim3d, int op, const Geom& g, const void* in, int dti, void* out, 
     return dispatch_out<__half>(dim3d, op, g, in, out, dto, ang, nbatch, nview, ws, l, st, oscale);
 }
 
+// ------------------------------------------------------ system matrix export
+
+// Layout of the per-view tables alone (no operator-specific regions).
+Layout tables_layout(int dim3d, const Geom& g, int nview) { return layout(dim3d, -1, g, 1, nview, DT_F32); }
+
+int sysmat(int dim3d, const Geom& g, const float* ang, int nview, const long long* offsets, long long* counts,
+           long long* rows, long long* cols, float* vals, void* workspace, size_t ws_bytes, void* stream) {
+    if (int rc = validate(g, dim3d, OP_A, 1, nview)) return rc;
+    if (nview < 1 || !ang) return fail(XR_ERR_INVALID_ARGUMENT, "need at least one view and its angle");
+    if (!offsets && !counts) return fail(XR_ERR_INVALID_ARGUMENT, "count pass needs the counts buffer");
+    if (offsets && (!rows || !cols || !vals)) return fail(XR_ERR_INVALID_ARGUMENT, "fill pass needs rows, cols, vals");
+    const Layout l = tables_layout(dim3d, g, nview);
+    if (!workspace || ws_bytes < l.total)
+        return fail(XR_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", l.total, ws_bytes);
+    if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+        return fail(XR_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const ViewTables vt = tables_at(static_cast<char*>(workspace), l);
+    {
+        dim3 grid((g.Nu + 1 + 127) / 128, nview);
+        setup_views_kernel<<<grid, 128, 0, st>>>(g, dim3d, ang, nview, vt);
+        if (int rc = check_cuda("setup_views")) return rc;
+    }
+    double zd0 = 0.0, dvv = 1.0, z0dz = 0.0;
+    if (dim3d) row_params(g, zd0, dvv, z0dz);
+    const long long ncell = (long long)nview * (dim3d ? g.Nv : 1) * g.Nu;
+    const unsigned blocks = (unsigned)((ncell + 127) / 128);
+    if (dim3d) {
+        if (offsets) sysmat_kernel<true, true><<<blocks, 128, 0, st>>>(g, vt, nview, counts, offsets, rows, cols, vals, z0dz, zd0, dvv);
+        else sysmat_kernel<false, true><<<blocks, 128, 0, st>>>(g, vt, nview, counts, offsets, rows, cols, vals, z0dz, zd0, dvv);
+    } else {
+        if (offsets) sysmat_kernel<true, false><<<blocks, 128, 0, st>>>(g, vt, nview, counts, offsets, rows, cols, vals, z0dz, zd0, dvv);
+        else sysmat_kernel<false, false><<<blocks, 128, 0, st>>>(g, vt, nview, counts, offsets, rows, cols, vals, z0dz, zd0, dvv);
+    }
+    return check_cuda("sysmat");
+}
+
 // ------------------------------------------------------ ragged 2D batches
 
 struct RaggedLayout {
@@ -791,6 +829,30 @@ int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in,
 }
 
 unsigned long long xr_launch_count(void) { return xr::g_launches.load(std::memory_order_relaxed); }
+
+size_t xr_sysmat2d_workspace_size(const xr_geom2d* geom, int nview) {
+    if (!geom) return 0;
+    return xr::tables_layout(0, xr::geom_from(geom), nview).total;
+}
+
+size_t xr_sysmat3d_workspace_size(const xr_geom3d* geom, int nview) {
+    if (!geom) return 0;
+    return xr::tables_layout(1, xr::geom_from(geom), nview).total;
+}
+
+int xr_sysmat2d(const xr_geom2d* geom, const float* angles, int nview, const long long* offsets, long long* counts,
+                long long* rows, long long* cols, float* vals, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
+    return xr::sysmat(0, xr::geom_from(geom), angles, nview, offsets, counts, rows, cols, vals, workspace,
+                      workspace_bytes, stream);
+}
+
+int xr_sysmat3d(const xr_geom3d* geom, const float* angles, int nview, const long long* offsets, long long* counts,
+                long long* rows, long long* cols, float* vals, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
+    return xr::sysmat(1, xr::geom_from(geom), angles, nview, offsets, counts, rows, cols, vals, workspace,
+                      workspace_bytes, stream);
+}
 
 int xr_ragged2d_plan_create(const xr_ragged2d_instance* inst, int ninst, xr_ragged2d_plan** plan,
                             size_t* workspace_bytes) {

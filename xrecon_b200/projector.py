@@ -277,7 +277,13 @@ class Projector2d(_ProjectorBase):
     weighted_backprojection_transpose = backprojection_weighted_t
 
     def system_matrix(self, angles: Tensor) -> Tensor:
-        raise NotImplementedError("the sparse system-matrix export is not part of this library")
+        """Sparse COO projection matrix [V * Nv * Nu, D * H * W] (2D: [V * Nu,
+        H * W]); the reference builds it on the CPU (system_matrix2d/3d,
+        torch_binding.cpp:353-405).  Built here on the GPU; returned on the
+        angles' device, so CPU angles give a CPU matrix as in the reference."""
+        dev = angles.device if angles.is_cuda else torch.device("cuda", torch.cuda.current_device())
+        m = _native.system_matrix(self._dim, self._host_geom.struct, angles, dev)
+        return m if angles.is_cuda else m.cpu()
 
     get_sys_matrix = system_matrix
 
@@ -416,7 +422,13 @@ class Projector3d(_ProjectorBase):
         return WeightedBackProjectionTranspose3d.apply(image, self._host(), self._prepare_angles(angles, image))
 
     def system_matrix(self, angles: Tensor) -> Tensor:
-        raise NotImplementedError("the sparse system-matrix export is not part of this library")
+        """Sparse COO projection matrix [V * Nv * Nu, D * H * W] (2D: [V * Nu,
+        H * W]); the reference builds it on the CPU (system_matrix2d/3d,
+        torch_binding.cpp:353-405).  Built here on the GPU; returned on the
+        angles' device, so CPU angles give a CPU matrix as in the reference."""
+        dev = angles.device if angles.is_cuda else torch.device("cuda", torch.cuda.current_device())
+        m = _native.system_matrix(self._dim, self._host_geom.struct, angles, dev)
+        return m if angles.is_cuda else m.cpu()
 
     get_sys_matrix = system_matrix
     projection_transpose = projection_t
