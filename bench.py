@@ -264,6 +264,44 @@ def sysmat_measure(dev, reps: int = 3):
     return {"nnz": nnz, "ms": ms, "gnnz_per_s": nnz / (ms / 1e3) / 1e9}
 
 
+def rebin_measure(P, vol, ang, reps: int = 3):
+    """Fan -> parallel rebinning of the workload's sinogram (1440 views,
+    256 rows, 1024 flat columns of 0.8 mm at SDD, i.e. 0.4387 mm at the
+    isocentre) to 1024 parallel bins: this library's kernel, the same pass
+    fused with a ramp filter, and torch.nn.functional.grid_sample on the
+    same grid (the call the reference's rebinning makes)."""
+    import torch
+    import torch.nn.functional as F
+    from xrecon_b200.filters import filter_generate
+    from xrecon_b200.rebin import fan_to_parallel_rebin, rebin_grid
+    sino = P.projection(vol, ang)
+    du_iso = WL["du"] * WL["sod"] / WL["sdd"]
+    args = (WL["sod"], du_iso, 0.0, "flat")
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    _, _, t = fan_to_parallel_rebin(sino, ang, *args)
+    filt = filter_generate(WL["Nu"], float(t[1] - t[0]), "ramp", torch.float32).to(sino.device)
+    ms = timed(lambda: fan_to_parallel_rebin(sino, ang, *args))
+    ms_fused = timed(lambda: fan_to_parallel_rebin(sino, ang, *args, filt=filt))
+    grid, _ = rebin_grid(ang, WL["Nu"], WL["sod"], du_iso, 0.0, "flat", ang, WL["Nu"], None, 0.0)
+    src = sino.permute(0, 1, 3, 2, 4).reshape(WL["Nv"], 1, WL["V"], WL["Nu"])
+    g4 = grid[None].expand(WL["Nv"], -1, -1, -1)
+    ms_torch = timed(lambda: F.grid_sample(src, g4, mode="bilinear", padding_mode="zeros", align_corners=True))
+    del sino, src
+    return {"ms": ms, "ms_fused_with_ramp_filter": ms_fused, "torch_grid_sample_ms": ms_torch,
+            "samples": WL["V"] * WL["Nv"] * WL["Nu"]}
+
+
 def ragged_measure(dev, reps: int = 5):
     """The 64-instance ragged fan-arc batch: projection + FBP of every
     instance as one autotuned persistent launch replayed from a CUDA graph,
@@ -452,6 +490,8 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         line["ragged_fan_arc_batch"] = ragged_measure(dev)
     if not args.no_sysmat and world == 1:
         line["system_matrix_2d_fan_flat"] = sysmat_measure(dev)
+    if not args.no_rebin and world == 1:
+        line["rebin_fan_to_parallel"] = rebin_measure(P, vol, ang)
     if rank == 0 and world == 1 and not args.no_cpu:
         sample = cpu_reference_sample(4, vol.cpu().numpy())
         line["cpu_baseline"] = {k: v for k, v in sample.items() if k != "seconds"} if sample else None
@@ -472,6 +512,7 @@ def main():
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged 2D batch measurement")
     ap.add_argument("--no-ops", action="store_true", help="skip the per-operator timings")
     ap.add_argument("--no-sysmat", action="store_true", help="skip the system-matrix export timing")
+    ap.add_argument("--no-rebin", action="store_true", help="skip the rebinning timing")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
     args = ap.parse_args()

@@ -150,6 +150,20 @@ int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in,
                     const float* angles, int nbatch, int nview, void* stream);
 
 /*
+ * Fan/cone -> parallel rebinning along the detector columns (replaces the
+ * grid_sample step of fan_to_parallel_rebin, xrecon/utils/rebin.py:10-95).
+ *   in   : [nbatch][nview][Nv][Nu] fan sinogram (xr_dtype dtype_in)
+ *   grid : device float [nview_out][Nt][2], the reference's normalized
+ *          sampling grid (x: detector column, y: view), align_corners=True
+ *   out  : float [nbatch][nview_out][Nv][Nt]; bilinear samples with zero
+ *          padding (grid_sample semantics)
+ *   filt : NULL, or [2 Nt - 1] filter taps: the rebinned rows are then
+ *          filtered in the same pass (as xr_fbp_filter, no weights).
+ */
+int xr_rebin_parallel(const void* in, int dtype_in, float* out, int nbatch, int nview, int Nv, int Nu,
+                      const float* grid, int nview_out, int Nt, const float* filt, void* stream);
+
+/*
  * Sparse export of the projection matrix A (replaces system_matrix2d /
  * system_matrix3d, torch_binding.cpp:353-405, which build it on the CPU with
  * src/cpu/system_matrix2d.cpp and src/cpu/system_matrix3d.cpp).  Two passes

@@ -182,3 +182,72 @@ def rel_l2(a, b) -> float:
     b = np.asarray(b, dtype=np.float64)
     den = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
+
+
+# ---------------------------------------------------------------- rebinning
+
+def rebin_grid(angles, Nu, iso_source, det_spacing, det_shift, detector_type, output_angles, Nt,
+               output_det_spacing, output_det_shift):
+    """Sampling grid of fan_to_parallel_rebin (xrecon/utils/rebin.py:67-95),
+    in the reference's float32 arithmetic: [Vout, Nt, 2] (x: column, y: view)
+    normalized for align_corners=True, and the bin centres t [Nt]."""
+    f32 = np.float32
+    a = np.asarray(angles, f32)
+    oa = np.asarray(output_angles, f32)
+    u = (np.arange(-Nu / 2 + 0.5, Nu / 2, 1.0).astype(f32) * f32(det_spacing) + f32(det_shift)).astype(f32)
+    if detector_type == "arc":
+        gext = np.abs(u).max()
+    else:
+        gext = np.arctan2(np.abs(u).max(), f32(iso_source)).astype(f32)
+    max_t = f32(iso_source) * np.sin(gext).astype(f32)
+    if output_det_spacing is None:
+        output_det_spacing = float(f32(2.0) * max_t / f32(Nt)) if Nt > 0 else 1.0
+    t = (np.arange(-Nt / 2 + 0.5, Nt / 2, 1.0).astype(f32) * f32(output_det_spacing) + f32(output_det_shift)).astype(f32)
+    ratio = np.clip(t / f32(iso_source), f32(-1.0 + 1e-6), f32(1.0 - 1e-6)).astype(f32)
+    gamma = np.arcsin(ratio).astype(f32)
+    beta = (oa[:, None] - gamma[None, :]).astype(f32)
+    uq = gamma if detector_type == "arc" else (np.tan(gamma).astype(f32) * f32(iso_source)).astype(f32)
+    V = a.size
+    step = f32(1.0) if V < 2 else np.diff(a).mean(dtype=f32)
+    bidx = ((beta - a[0]) / step).astype(f32)
+    ucoord = ((uq - f32(det_shift)) / f32(det_spacing) + f32(Nu / 2 - 0.5)).astype(f32)
+    gy = (f32(2.0) * bidx / f32(max(V - 1, 1)) - f32(1.0)).astype(f32)
+    gx = (f32(2.0) * ucoord[None, :] / f32(max(Nu - 1, 1)) - f32(1.0)).astype(f32)
+    return np.stack([np.broadcast_to(gx, gy.shape), gy], axis=-1), t
+
+
+def grid_sample_rows(sino5, grid):
+    """Bilinear sampling of every [V, Nu] plane of sino5 [B, C, V, Nv, Nu] at
+    grid [Vout, Nt, 2] (align_corners=True, zero padding), FP64:
+    [B, C, Vout, Nv, Nt]."""
+    s = np.asarray(sino5, np.float64)
+    B, C, V, Nv, Nu = s.shape
+    g = np.asarray(grid, np.float64)
+    ix = (g[..., 0] + 1.0) / 2.0 * (Nu - 1)
+    iy = (g[..., 1] + 1.0) / 2.0 * (V - 1)
+    x0, y0 = np.floor(ix).astype(np.int64), np.floor(iy).astype(np.int64)
+    out = np.zeros((B, C, g.shape[0], Nv, g.shape[1]))
+    for dy, wy in ((0, y0 + 1 - iy), (1, iy - y0)):
+        for dx, wx in ((0, x0 + 1 - ix), (1, ix - x0)):
+            yy, xx = y0 + dy, x0 + dx
+            ok = (yy >= 0) & (yy < V) & (xx >= 0) & (xx < Nu)
+            val = s[:, :, np.clip(yy, 0, V - 1), :, np.clip(xx, 0, Nu - 1)]  # [Vout, Nt, B, C, Nv]
+            val = np.moveaxis(val, (0, 1), (3, 4))                              # [B, C, Nv, Vout, Nt]
+            out += np.moveaxis(val * (wx * wy * ok), 2, 3)
+    return out
+
+
+def fan_to_parallel_rebin(sino, angles, iso_source, det_spacing, det_shift=0.0, detector_type="arc",
+                          output_angles=None, output_det_count=None, output_det_spacing=None,
+                          output_det_shift=0.0):
+    """FP64 restatement of the reference's fan_to_parallel_rebin
+    (rebin.py:10-95): (parallel sinogram, output angles, t)."""
+    s = np.asarray(sino)
+    s5 = s[:, :, :, None, :] if s.ndim == 4 else s
+    Nu = s5.shape[-1]
+    oa = np.asarray(angles if output_angles is None else output_angles, np.float32)
+    Nt = Nu if output_det_count is None else int(output_det_count)
+    grid, t = rebin_grid(angles, Nu, iso_source, det_spacing, det_shift, detector_type, oa, Nt,
+                         output_det_spacing, output_det_shift)
+    out = grid_sample_rows(s5, grid)
+    return (out[:, :, :, 0, :] if s.ndim == 4 else out), oa, t

@@ -20,7 +20,10 @@ from the reference's code path on CPU:
   geometries; filters.npz: the filter tables;
 * sysmat{2,3}d_<geom>.npz: the reference's sparse projection matrices
   (system_matrix2d_cpu / system_matrix3d_cpu) for small shifted geometries
-  (``python tests/golden/make_golden.py sysmat`` writes only these).
+  (``python tests/golden/make_golden.py sysmat`` writes only these);
+* rebin_<case>.npz: the reference's fan/helical -> parallel rebinning
+  (xrecon/utils/rebin.py, pure torch) on seeded inputs
+  (``python tests/golden/make_golden.py rebin``).
 """
 from __future__ import annotations
 
@@ -177,9 +180,49 @@ def make_sysmat():
     print("system-matrix fixtures written to", HERE)
 
 
+def make_rebin():
+    """rebin_<case>.npz: the reference's fan_to_parallel_rebin /
+    helical_fan_to_parallel_rebin (xrecon/utils/rebin.py, pure torch, run on
+    the CPU) on seeded inputs."""
+    sys.path.insert(0, str(REF_ROOT))
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("xrecon_rebin_ref", REF_ROOT / "xrecon" / "utils" / "rebin.py")
+    R = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(R)
+    rng = np.random.default_rng(21)
+    cases = {
+        "arc4d": ("arc", (1, 1, 90, 64), 0.004, {}),
+        "flat5d": ("flat", (2, 1, 72, 5, 48), 1.5, dict(output_det_count=40, output_det_shift=0.7)),
+        "arc5d_grid": ("arc", (1, 2, 60, 3, 50), 0.004,
+                       dict(output_angles=torch.linspace(0.3, 5.0, 33), output_det_spacing=3.0)),
+    }
+    for name, (det, shape, du, kw) in cases.items():
+        V = shape[2]
+        ang = torch.arange(V, dtype=torch.float32) * (2 * np.pi / V) + 0.1
+        sino = torch.from_numpy(rng.random(shape).astype(np.float32))
+        out, oa, t = R.fan_to_parallel_rebin(sino, ang, 500.0, du, 0.3 * du, det, **kw)
+        extra = {k: (v.numpy() if torch.is_tensor(v) else np.array(v)) for k, v in kw.items()}
+        np.savez_compressed(HERE / f"rebin_{name}.npz", sino=sino.numpy(), angles=ang.numpy(), iso_source=500.0,
+                            det_spacing=du, det_shift=0.3 * du, detector_type=det, out=out.numpy(),
+                            out_angles=oa.numpy(), t=t.numpy(), **{f"kw_{k}": v for k, v in extra.items()})
+    V = 80
+    ang = torch.arange(V, dtype=torch.float32) * (2 * np.pi / V)
+    zsrc = torch.linspace(-20.0, 20.0, V)
+    sino = torch.from_numpy(rng.random((1, 1, V, 4, 40)).astype(np.float32))
+    oa_in = torch.linspace(-0.2, 6.5, 50)
+    out, oa, t, z = R.helical_fan_to_parallel_rebin(sino, ang, zsrc, 550.0, 0.005, 0.0, "arc", output_angles=oa_in)
+    np.savez_compressed(HERE / "rebin_helical.npz", sino=sino.numpy(), angles=ang.numpy(), source_z=zsrc.numpy(),
+                        out_angles_in=oa_in.numpy(), out=out.numpy(), out_angles=oa.numpy(), t=t.numpy(),
+                        out_source_z=z.numpy())
+    print("rebinning fixtures written to", HERE)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["sysmat"]:
         make_sysmat()
+    elif sys.argv[1:] == ["rebin"]:
+        make_rebin()
     else:
         main()
         make_sysmat()
+        make_rebin()

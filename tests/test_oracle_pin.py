@@ -93,3 +93,22 @@ def test_reference_system_matrix_is_the_oracle_projection(dim, scan):
     x = rng.random(img_shape)
     exact = (O.dd2d if dim == 2 else O.dd3d)("A", x, o, g["angles"]).reshape(-1)
     assert rel_l2(M @ x.reshape(-1), exact) < TOL[scan]
+
+
+def _rebin_kwargs(g):
+    kw = {}
+    for k in g:
+        if k.startswith("kw_"):
+            v = g[k]
+            kw[k[3:]] = v if v.ndim else v.item()
+    return kw
+
+
+@pytest.mark.parametrize("case", ["arc4d", "flat5d", "arc5d_grid"])
+def test_oracle_rebin_matches_reference(case):
+    g = load_golden(f"rebin_{case}")
+    out, oa, t = O.fan_to_parallel_rebin(g["sino"], g["angles"], float(g["iso_source"]), float(g["det_spacing"]),
+                                         float(g["det_shift"]), str(g["detector_type"]), **_rebin_kwargs(g))
+    assert out.shape == g["out"].shape
+    np.testing.assert_array_equal(t, g["t"])
+    assert rel_l2(out, g["out"]) < 1e-5

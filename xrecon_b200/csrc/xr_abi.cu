@@ -20,6 +20,7 @@
 #include "xr_vox_prefix.cuh"
 #include "xr_ragged.cuh"
 #include "xr_sysmat.cuh"
+#include "xr_rebin.cuh"
 #include "../../include/xrecon_b200.h"
 
 
@@ -760,19 +761,21 @@ int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, i
     if (smem > 200 * 1024) return xr::fail(XR_ERR_UNSUPPORTED, "detector width %d too large for the filter kernel", Nu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int grid = std::min((nrows + rpc - 1) / rpc, 148 * 8);
-    if (dtype_in == xr::DT_F32) {
-        auto k = xr::fbp_filter_kernel<float, OUTS>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, 256, smem, st>>>(static_cast<const float*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker, tpr, rpc);
-    } else if (dtype_in == xr::DT_BF16) {
-        auto k = xr::fbp_filter_kernel<__nv_bfloat16, OUTS>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, 256, smem, st>>>(static_cast<const __nv_bfloat16*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker, tpr, rpc);
-    } else {
-        auto k = xr::fbp_filter_kernel<__half, OUTS>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, 256, smem, st>>>(static_cast<const __half*>(in), out, nrows, Nu, nview, rows_per_view, cosw, filt, parker, tpr, rpc);
-    }
+    auto launch = [&](auto rows_src) -> int {
+        auto k = xr::fbp_filter_kernel<decltype(rows_src), OUTS>;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return xr::fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
+        k<<<grid, 256, smem, st>>>(rows_src, out, nrows, Nu, filt, tpr, rpc);
+        return XR_OK;
+    };
+    int rc;
+    if (dtype_in == xr::DT_F32)
+        rc = launch(xr::SinoRows<float>{static_cast<const float*>(in), cosw, parker, Nu, nview, rows_per_view});
+    else if (dtype_in == xr::DT_BF16)
+        rc = launch(xr::SinoRows<__nv_bfloat16>{static_cast<const __nv_bfloat16*>(in), cosw, parker, Nu, nview, rows_per_view});
+    else
+        rc = launch(xr::SinoRows<__half>{static_cast<const __half*>(in), cosw, parker, Nu, nview, rows_per_view});
+    if (rc) return rc;
     return xr::check_cuda("fbp_filter");
 }
 
@@ -829,6 +832,54 @@ int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in,
 }
 
 unsigned long long xr_launch_count(void) { return xr::g_launches.load(std::memory_order_relaxed); }
+
+int xr_rebin_parallel(const void* in, int dtype_in, float* out, int nbatch, int nview, int Nv, int Nu,
+                      const float* grid, int nview_out, int Nt, const float* filt, void* stream) {
+    using namespace xr;
+    if (!in || !out || !grid) return fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
+    if (nbatch < 0 || nview < 1 || Nv < 1 || Nu < 1 || nview_out < 0 || Nt < 1)
+        return fail(XR_ERR_INVALID_ARGUMENT, "bad rebinning sizes");
+    if (!dtype_ok(dtype_in)) return fail(XR_ERR_INVALID_ARGUMENT, "unsupported dtype %d", dtype_in);
+    if (reinterpret_cast<uintptr_t>(grid) % 8 != 0) return fail(XR_ERR_INVALID_ARGUMENT, "grid must be 8-byte aligned");
+    const long long total = (long long)nbatch * nview_out * Nv * Nt;
+    if (total == 0) return XR_OK;
+    if ((long long)nbatch * nview_out * Nv > 0x7fffffffll) return fail(XR_ERR_UNSUPPORTED, "too many rows");
+    const RebinGrid r{grid, nview, Nv, Nu, nview_out, Nt};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!filt) {
+        if (Nv > 65535) return fail(XR_ERR_UNSUPPORTED, "more than 65535 detector rows");
+        const int nz = nbatch * nview_out;
+        for (int z0 = 0; z0 < nz; z0 += 65535) {
+            const dim3 grid((Nt + 255) / 256, Nv, std::min(65535, nz - z0));
+            if (dtype_in == DT_F32) rebin_kernel<float><<<grid, 256, 0, st>>>(static_cast<const float*>(in), out, r, z0);
+            else if (dtype_in == DT_BF16) rebin_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(static_cast<const __nv_bfloat16*>(in), out, r, z0);
+            else rebin_kernel<__half><<<grid, 256, 0, st>>>(static_cast<const __half*>(in), out, r, z0);
+            if (int rc = check_cuda("rebin")) return rc;
+        }
+        return XR_OK;
+    }
+    // rebinning fused into the filter kernel's row loads
+    constexpr int OUTS = 8;
+    const int nrows = (int)((long long)nbatch * nview_out * Nv);
+    const int tpr = std::min(256, ((Nt + OUTS - 1) / OUTS + 31) / 32 * 32);
+    const int rpc = std::max(1, 256 / tpr);
+    const size_t smem = ((size_t)(filt_taps_smem(Nt) + 3) / 4 * 4 + (size_t)rpc * filt_row_pitch(Nt)) * sizeof(float);
+    if (smem > 200 * 1024) return fail(XR_ERR_UNSUPPORTED, "detector width %d too large for the filter kernel", Nt);
+    const int grid_blocks = std::min((nrows + rpc - 1) / rpc, 148 * 8);
+    auto launch = [&](auto rows_src) -> int {
+        auto k = fbp_filter_kernel<decltype(rows_src), OUTS>;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
+        k<<<grid_blocks, 256, smem, st>>>(rows_src, out, nrows, Nt, filt, tpr, rpc);
+        return XR_OK;
+    };
+    int rc;
+    if (dtype_in == DT_F32) rc = launch(RebinRows<float>{static_cast<const float*>(in), r});
+    else if (dtype_in == DT_BF16) rc = launch(RebinRows<__nv_bfloat16>{static_cast<const __nv_bfloat16*>(in), r});
+    else rc = launch(RebinRows<__half>{static_cast<const __half*>(in), r});
+    if (rc) return rc;
+    return check_cuda("rebin_filter");
+}
 
 size_t xr_sysmat2d_workspace_size(const xr_geom2d* geom, int nview) {
     if (!geom) return 0;

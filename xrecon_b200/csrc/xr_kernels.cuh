@@ -637,11 +637,26 @@ __host__ __device__ inline int filt_taps_len(int Nu) { return 2 * ((Nu + 7) / 8 
 __host__ __device__ inline int filt_taps_smem(int Nu) { const int n = filt_taps_len(Nu); return n + n / 32 + 1; }
 __device__ __forceinline__ int tap_pos(int i) { return i + (i >> 5); }
 
-template <typename TI, int OUTS>
+// Row source of the filter: a stored sinogram row times the cosine and
+// Parker weights.
+template <typename TI>
+struct SinoRows {
+    const TI* in;
+    const float* cosw;
+    const float* parker;
+    int Nu, nview, rows_per_view;
+    __device__ __forceinline__ float operator()(int row, int j) const {
+        float val = ld(in + (size_t)row * Nu + j);
+        if (cosw) val *= cosw[j];
+        if (parker) val *= parker[(size_t)((row / rows_per_view) % nview) * Nu + j];
+        return val;
+    }
+};
+
+template <typename Rows, int OUTS>
 __global__ void __launch_bounds__(256)
-fbp_filter_kernel(const TI* __restrict__ in, float* __restrict__ out, const int nrows, const int Nu,
-                  const int nview, const int rows_per_view, const float* __restrict__ cosw,
-                  const float* __restrict__ filt, const float* __restrict__ parker, const int tpr, const int rpc) {
+fbp_filter_kernel(const Rows src, float* __restrict__ out, const int nrows, const int Nu,
+                  const float* __restrict__ filt, const int tpr, const int rpc) {
     static_assert(OUTS == 8, "the register window below is written for 8 outputs per thread");
     extern __shared__ __align__(16) float smem[];
     const int nf = 2 * Nu - 1;
@@ -659,13 +674,7 @@ fbp_filter_kernel(const TI* __restrict__ in, float* __restrict__ out, const int 
         for (int e = threadIdx.x; e < rpc * pitch; e += blockDim.x) {
             const int rr = e / pitch, j = e - rr * pitch;
             const int row = row0 + rr;
-            float val = 0.0f;
-            if (j < Nu && row < nrows) {
-                val = ld(in + (size_t)row * Nu + j);
-                if (cosw) val *= cosw[j];
-                if (parker) val *= parker[(size_t)((row / rows_per_view) % nview) * Nu + j];
-            }
-            xs[e] = val;
+            xs[e] = (j < Nu && row < nrows) ? src(row, j) : 0.0f;
         }
         __syncthreads();
         const int row = row0 + r;
