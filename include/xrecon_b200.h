@@ -55,8 +55,8 @@ typedef struct {
 } xr_geom2d;
 
 /* 3D geometry: the 18 packed options of Projector3d (projector3d.py:98-107),
- * unpacked as torch_binding.cpp:82-124 (helical fields are not part of this
- * path). */
+ * unpacked as torch_binding.cpp:82-124 (the helical fields travel in
+ * xr_helical_opts). */
 typedef struct {
     int W, H, D, Nu, Nv, type;
     float dx, dy, dz, du, dv, sod, sdd;
@@ -90,6 +90,36 @@ int xr_dd2d(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* o
 int xr_dd3d(int op, const xr_geom3d* geom, const void* in, int dtype_in, void* out, int dtype_out,
             const float* angles, int nbatch, int nview, void* workspace, size_t workspace_bytes,
             void* stream);
+
+/*
+ * Helical cone-beam scans with an arc detector (replaces the six *_helical3d
+ * bindings, torch_binding.cpp:525-612, over src/kernels/helical_arc3d.cu).
+ * Options: entries 18..23 of HelicalProjector3d's packed options
+ * (projector3d.py:375-400), with the binding's defaults
+ * (torch_binding.cpp:103-108): view_mode 2, weight_mode 0, view_turns 0,
+ * halfscan_coef 1, tang_k 5, tang_blend 0.
+ */
+typedef struct {
+    int view_mode;      /* 0 auto (from the pitch), 1 half scan, 2 one turn, 3 view_turns turns */
+    int weight_mode;    /* 0 conjugate-ray redundancy ("2d"), 1 tangential ("tang3d") */
+    float view_turns, halfscan_coef, tang_k, tang_blend;
+} xr_helical_opts;
+
+size_t xr_helical3d_workspace_size(int op, const xr_geom3d* geom, int nbatch, int nview);
+
+/*
+ * Apply one helical operator (op as xr_op; geom->type must be XR_FAN_ARC).
+ *   in / out   : device float32, image [nbatch, D, H, W], sinogram
+ *                [nbatch, nview, Nv, Nu]; `out` is fully overwritten.
+ *   angles     : device float32 [nview].
+ *   source_pos : device float32 [4, nview], rows source_z, shift_radius,
+ *                shift_angle, shift_z (the reference's source_pos,
+ *                torch_binding.cpp:128-138).
+ * The reference supports float32 only; so does this entry.
+ */
+int xr_helical3d(int op, const xr_geom3d* geom, const xr_helical_opts* opts, const float* in, float* out,
+                 const float* angles, const float* source_pos, int nbatch, int nview, void* workspace,
+                 size_t workspace_bytes, void* stream);
 
 /*
  * Fused FBP/FDK pre-filter (replaces the `sino * weight` and

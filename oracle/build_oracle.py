@@ -1,6 +1,12 @@
 """Build recipe for the test oracle (test infrastructure only).
 
 * ``oracle/lib/libxr_oracle.so`` -- the FP64 C restatement ``dd_oracle.c``.
+* ``oracle/_ref/libxrecon_ref_helical.so`` -- the reference's own helical
+  CUDA operators (XRecon ``src/kernels/helical_arc3d.cu``, which needs only
+  the reference ``include/`` directory) compiled in place with the
+  reference's nvcc flags (setup.py:16) for sm_100a, together with
+  ``ref_helical_shim.cu``; it only serves tests/golden/make_golden_helical.py,
+  which records the reference's helical outputs on a GPU.
 * ``oracle/_ref/libxrecon_ref_cpu.so`` -- the reference's own CPU operators
   (XRecon ``src/cpu/{forward2d,backward2d,system_matrix2d,system_matrix3d,
   forward3d,backward3d}.cpp``) compiled in place from the reference sources together with
@@ -23,6 +29,7 @@ LIB_DIR = HERE / "lib"
 REF_DIR = HERE / "_ref"
 ORACLE_SO = LIB_DIR / "libxr_oracle.so"
 REF_SO = REF_DIR / "libxrecon_ref_cpu.so"
+REF_HELICAL_SO = REF_DIR / "libxrecon_ref_helical.so"
 REFERENCE_ROOT = Path(os.environ.get("XRECON_REFERENCE_ROOT", "/root/reference"))
 REF_CPU_SOURCES = ["forward2d.cpp", "backward2d.cpp", "system_matrix2d.cpp", "system_matrix3d.cpp",
                    "forward3d.cpp", "backward3d.cpp"]
@@ -66,6 +73,23 @@ def build_ref(force: bool = False) -> Path | None:
     return REF_SO
 
 
+def build_ref_helical(force: bool = False) -> Path | None:
+    """Compile the reference's helical CUDA launchers with the shim; returns
+    None when the reference tree is absent (a prebuilt .so is used as is)."""
+    src = REFERENCE_ROOT / "src" / "kernels" / "helical_arc3d.cu"
+    if not src.is_file():
+        return REF_HELICAL_SO if REF_HELICAL_SO.exists() else None
+    shim = HERE / "ref_helical_shim.cu"
+    REF_DIR.mkdir(exist_ok=True)
+    if force or _stale(REF_HELICAL_SO, [src, shim]):
+        nvcc = str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "bin" / "nvcc")
+        _run([nvcc, "-O3", "--use_fast_math", "-lineinfo", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+              "-Xcompiler", "-fPIC", "-shared", f"-I{REFERENCE_ROOT / 'include'}", "-o", str(REF_HELICAL_SO),
+              str(src), str(shim)])
+    return REF_HELICAL_SO
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
+    print(build_ref_helical(force="--force" in sys.argv))

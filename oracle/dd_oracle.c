@@ -403,3 +403,445 @@ int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
     free(D); free(X); free(xa); free(xb); free(xl);
     return 0;
 }
+
+/* ----------------------------------------------------------- helical ---- */
+/*
+ * Helical cone-beam operators with an arc detector (XRecon
+ * src/kernels/helical_arc3d.cu, bound at src/api/torch_binding.cpp:525-612,
+ * Python xrecon/projector/projector3d.py:289-576).
+ *
+ * A, A^T, B, B^T (helical_arc3d.cu:364-1111, :1507-1761) are the cone-arc DD
+ * operators above with per-view geometry taken from source_pos [4][V] =
+ * (source_z, shift_radius, shift_angle, shift_z), helical_arc3d.cu:382-395:
+ *     sod' = SOD + sr, sdd' = SDD + sr, du' = du SDD / sdd',
+ *     shu' = shu SDD / sdd' - sa (sdd' - sod') / sdd',
+ *     source at angle beta + sa (float sum), column angles sg du' + shu' + beta,
+ *     source z = source_z + shift_z, detector rows at
+ *     (r - Nv/2) dv + source_z + shv,
+ * all z measured from the source z.  Two details follow the reference:
+ *   - A's cell cosine (triangle_cosine, helical_arc3d.cu:432) takes the mean
+ *     row position on the axis plane WITHOUT subtracting the source z
+ *     (det_row_axis carries "+ src_z");
+ *   - B's column width is sod' du' (helical_arc3d.cu:896).
+ * The per-view scalars are formed in float as the reference forms them; the
+ * overlaps are evaluated in double as in xo_dd3d.
+ *
+ * Bw and Bw^T (helical_arc3d.cu:1112-1505) weight every (voxel, view) pair
+ * of the voxel's view window with a redundancy weight and normalise per
+ * voxel; the weights are restated below in float with the reference's
+ * operation order, the DD footprint in double.
+ */
+
+#define XO_PI_F 3.14159265358979323846f
+
+typedef struct {
+    int view_mode, weight_mode;
+    float view_turns, halfscan_coef, tang_k, tang_blend;
+} hopt_t;
+
+typedef struct {
+    geo3_t g;        /* sod, sdd, du, shu of this view */
+    view_t v;        /* source at float(beta + shift_angle), radius sod' */
+    double zsrc;     /* source z */
+    double zrow0;    /* lower boundary of detector row 0, relative to zsrc */
+    double cwB;      /* B / B^T column width sod' du' */
+} hview_t;
+
+static void helical_view(const geo3_t* g0, const float* ang, const float* sp, int nview, int view, hview_t* h)
+{
+    const float zs = sp[view], sr = sp[nview + view], sa = sp[2 * nview + view], szs = sp[3 * nview + view];
+    const float SOD = (float)g0->sod, SDD = (float)g0->sdd, du0 = (float)g0->du, shu0 = (float)g0->shu;
+    const float sod = SOD + sr;
+    const float sdd = SDD + sr;
+    const float du = du0 * SDD / sdd;
+    const float shu = shu0 * SDD / sdd - sa * (sdd - sod) / sdd;
+    const float beta = ang[view] + sa;
+    const float zsrc = zs + szs;
+    h->g = *g0;
+    h->g.sod = sod;
+    h->g.sdd = sdd;
+    h->g.du = du;
+    /* column angle sg du' + shu' + beta_unshifted, written relative to the
+     * source angle the header carries */
+    h->g.shu = (double)shu + ((double)ang[view] - (double)beta);
+    h->v = make_view(beta, sod);
+    h->zsrc = zsrc;
+    h->zrow0 = -0.5 * g0->Nv * g0->dv + (double)zs + g0->shv - (double)zsrc;
+    h->cwB = (double)(sod * du);
+}
+
+/* ---- weights, float, helical_arc3d.cu:8-336 ---- */
+
+static float hw_clamp_unit(float x) { return fminf(1.0f, fmaxf(0.0f, x)); }
+
+static float hw_smooth_step(float x)
+{
+    x = hw_clamp_unit(x);
+    return 0.5f * (1.0f - cosf(XO_PI_F * x));
+}
+
+static float hw_window_quality(float beta, float bs, float be, float gamma, float gmax)
+{
+    const float lo = fminf(bs, be), hi = fmaxf(bs, be);
+    if (beta < lo || beta > hi) return 0.0f;
+    const float gc = fminf(fmaxf(gamma, -gmax), gmax);
+    const float lw = fmaxf(1.0e-6f, 2.0f * (gmax - gc));
+    const float rw = fmaxf(1.0e-6f, 2.0f * (gmax + gc));
+    if (beta < lo + lw) return hw_smooth_step((beta - lo) / lw);
+    if (beta > hi - rw) return hw_smooth_step((hi - beta) / rw);
+    return 1.0f;
+}
+
+static float hw_center_turn(float beta, float bc, float bs, float be, float db)
+{
+    const float lo = fminf(bs, be), hi = fmaxf(bs, be);
+    if (beta < lo || beta > hi) return 0.0f;
+    const float adb = fmaxf(fabsf(db), 1.0e-6f);
+    const float half = 0.5f * (hi - lo);
+    const float dist = fabsf(beta - bc);
+    const float crad = fminf(XO_PI_F, half);
+    if (dist <= crad) return 1.0f;
+    const float ow = fmaxf(half - crad, 4.0f * adb);
+    return hw_smooth_step((half - dist) / ow);
+}
+
+static float hw_source_z_at(float beta, const float* ang, const float* zsrc, int nview)
+{
+    if (nview <= 1) return zsrc[0];
+    const float a0 = ang[0], a1 = ang[nview - 1];
+    const float range = a1 - a0;
+    if (fabsf(range) <= 1.0e-6f) return zsrc[0];
+    const float dzdb = (zsrc[nview - 1] - zsrc[0]) / range;
+    return zsrc[0] + (beta - a0) * dzdb;
+}
+
+static float hw_edge_taper(float beta, float bc, float bs, float be, float db)
+{
+    const float lo = fminf(bs, be), hi = fmaxf(bs, be);
+    if (beta < lo || beta > hi) return 0.0f;
+    const float span = hi - lo, half = 0.5f * span;
+    if (span <= XO_PI_F + 8.0f * fabsf(db)) return 1.0f;
+    const float crad = fminf(XO_PI_F, half);
+    const float dist = fabsf(beta - bc);
+    if (dist <= crad) return 1.0f;
+    const float ew = fmaxf(half - crad, 4.0f * fabsf(db));
+    return hw_smooth_step((half - dist) / ew);
+}
+
+static float hw_center_beta(float pz, const float* ang, const float* zsrc, int vs, int ve, int nview)
+{
+    const float bs = ang[vs], be = ang[ve];
+    if (nview <= 1) return 0.5f * (bs + be);
+    const float a0 = ang[0], a1 = ang[nview - 1], z0 = zsrc[0], z1 = zsrc[nview - 1];
+    const float range = a1 - a0;
+    const float dzdb = (fabsf(range) > 1.0e-6f) ? (z1 - z0) / range : 0.0f;
+    if (fabsf(dzdb) <= 1.0e-8f) return 0.5f * (bs + be);
+    const float beta = a0 + (pz - z0) / dzdb;
+    return fminf(fmaxf(beta, fminf(bs, be)), fmaxf(bs, be));
+}
+
+/* helical_arc3d.cu:141-210 */
+static void hw_view_window(float pz, const float* ang, const float* zsrc, const geo3_t* g, const hopt_t* o,
+                           int nview, int* vs, int* ve)
+{
+    if (nview <= 1) { *vs = 0; *ve = 0; return; }
+    const float a0 = ang[0], a1 = ang[nview - 1], z0 = zsrc[0], z1 = zsrc[nview - 1];
+    const float range = a1 - a0;
+    if (fabsf(range) < 1.0e-6f) { *vs = 0; *ve = nview - 1; return; }
+    const float db = range / fmaxf(1.0f, (float)(nview - 1));
+    const float dzdb = (z1 - z0) / range;
+    if (fabsf(db) < 1.0e-8f || fabsf(dzdb) < 1.0e-8f) { *vs = 0; *ve = nview - 1; return; }
+    const float du = (float)g->du, dv = (float)g->dv, SOD = (float)g->sod, SDD = (float)g->sdd;
+    const float gmax = du * (float)(g->Nu - 1) * 0.5f;
+    const float half_scan = (XO_PI_F + 2.0f * gmax) * fmaxf(o->halfscan_coef, 1.0f);
+    float span = 2.0f * XO_PI_F;
+    if (o->view_mode == 1) span = half_scan;
+    else if (o->view_mode == 2) span = 2.0f * XO_PI_F;
+    else if (o->view_mode == 3) span = fmaxf(0.25f, o->view_turns) * 2.0f * XO_PI_F;
+    else {
+        const float ppt = fabsf(dzdb) * 2.0f * XO_PI_F;
+        const float iso_h = fmaxf(dv * (float)g->Nv * SOD / SDD, dv);
+        const float np = ppt / fmaxf(iso_h, 1.0e-6f);
+        if (np >= 1.25f) span = half_scan;
+        else if (np >= 0.45f) span = 2.0f * XO_PI_F;
+        else if (np >= 0.25f) span = 3.0f * XO_PI_F;
+        else span = 5.0f * XO_PI_F;
+    }
+    /* a window of V or more views is all views, and a centre beyond +-4V
+     * gives the same clamped window as +-4V: both bounds keep the integer
+     * arithmetic in range (the reference's values wherever it has them) */
+    const float nwf = ceilf(span / fabsf(db));
+    const int nwin = (nwf >= (float)nview) ? nview : (nwf < 1.0f ? 1 : (int)nwf);
+    const float bc = a0 + (pz - z0) / dzdb;
+    const float vcf = roundf((bc - a0) / db);
+    const int vc = (int)fminf(fmaxf(vcf, -4.0f * (float)nview), 4.0f * (float)nview);
+    int s = vc - nwin / 2;
+    if (s < 0) s = 0;
+    int e = s + nwin - 1;
+    if (e > nview - 1) e = nview - 1;
+    s = e - nwin + 1;
+    if (s < 0) s = 0;
+    *vs = s; *ve = e;
+}
+
+/* helical_arc3d.cu:212-241 */
+static float hw_conjugate(float beta, float gamma, float bc, float bs, float be, float db, float gmax)
+{
+    const float span = fabsf(be - bs);
+    const float adb = fmaxf(fabsf(db), 1.0e-6f);
+    if (span >= 2.0f * XO_PI_F - 2.0f * adb) {
+        const float turns = fmaxf(1.0f, floorf((span + 2.0f * adb) / (2.0f * XO_PI_F)));
+        return 0.5f * hw_center_turn(beta, bc, bs, be, db) / turns;
+    }
+    const float q = hw_window_quality(beta, bs, be, gamma, gmax);
+    if (q <= 0.0f) return 0.0f;
+    const float dir = (db >= 0.0f) ? 1.0f : -1.0f;
+    float den = 0.0f;
+    for (int k = -4; k <= 4; ++k) {
+        const float turn = dir * 2.0f * XO_PI_F * (float)k;
+        den += hw_window_quality(beta + turn, bs, be, gamma, gmax);
+        den += hw_window_quality(beta + dir * (XO_PI_F + 2.0f * gamma) + turn, bs, be, -gamma, gmax);
+    }
+    return q / fmaxf(den, 1.0e-6f);
+}
+
+/* helical_arc3d.cu:243-303 */
+static float hw_weight(float px, float py, float pz, float beta, float gamma, float src_z, float ray_xy, float bc,
+                       float bs, float be, float db, float gmax, const float* ang, const float* zsrc, int nview,
+                       const geo3_t* g, const hopt_t* o)
+{
+    if (o->weight_mode == 0) return hw_conjugate(beta, gamma, bc, bs, be, db, gmax);
+    const float span = fabsf(be - bs);
+    const float dir = (beta < bc) ? 1.0f : -1.0f;
+    const float bcj = beta + dir * (XO_PI_F + 2.0f * gamma);
+    float dq, cq;
+    if (span < 2.0f * XO_PI_F - 2.0f * fabsf(db)) {
+        dq = hw_window_quality(beta, bs, be, gamma, gmax);
+        cq = hw_window_quality(bcj, bs, be, -gamma, gmax);
+    } else {
+        dq = hw_edge_taper(beta, bc, bs, be, db);
+        cq = hw_edge_taper(bcj, bc, bs, be, db);
+    }
+    if (dq <= 0.0f) return 0.0f;
+    if (cq <= 0.0f) return 1.0f;
+    const float zc = hw_source_z_at(bcj, ang, zsrc, nview);
+    const float SOD = (float)g->sod;
+    const float sxc = -sinf(bcj) * SOD, syc = cosf(bcj) * SOD;
+    const float rxc = px - sxc, ryc = py - syc;
+    const float rxyc = sqrtf(rxc * rxc + ryc * ryc);
+    const float ta = fabsf(pz - src_z) / fmaxf(ray_xy, 1.0e-6f);
+    const float tac = fabsf(pz - zc) / fmaxf(rxyc, 1.0e-6f);
+    const float k = fminf(fmaxf(o->tang_k, 0.0f), 32.0f);
+    const float gg = powf(fmaxf(ta, 1.0e-6f), k);
+    const float ggc = powf(fmaxf(tac, 1.0e-6f), k);
+    const float w2 = dq / fmaxf(dq + cq, 1.0e-6f);
+    const float den = dq * ggc + cq * gg;
+    const float w3 = (dq * ggc) / fmaxf(den, 1.0e-6f);
+    const float blend = hw_clamp_unit(o->tang_blend);
+    return (1.0f - blend) * w2 + blend * w3;
+}
+
+/* Per-view float scalars of the weighted kernels (helical_arc3d.cu:1148-1160). */
+typedef struct {
+    float sod, sdd, du, shu, beta, sinv, cosv, sx, sy, szv;
+} hwview_t;
+
+static hwview_t hw_view(const geo3_t* g, const float* ang, const float* sp, int nview, int v)
+{
+    hwview_t w;
+    const float sr = sp[nview + v], sa = sp[2 * nview + v];
+    const float SOD = (float)g->sod, SDD = (float)g->sdd;
+    w.sod = SOD + sr;
+    w.sdd = SDD + sr;
+    w.du = (float)g->du * SDD / w.sdd;
+    w.shu = (float)g->shu * SDD / w.sdd - sa * (w.sdd - w.sod) / w.sdd;
+    w.beta = ang[v] + sa;
+    w.sinv = sinf(w.beta);
+    w.cosv = cosf(w.beta);
+    w.sx = -w.sinv * w.sod;
+    w.sy = w.cosv * w.sod;
+    w.szv = sp[v] + sp[3 * nview + v];
+    return w;
+}
+
+/* helical_arc3d.cu:305-336 */
+static int hw_measured(float px, float py, float pz, const hwview_t* w, float source_z_view, float shift_z,
+                       const geo3_t* g)
+{
+    const float xb = w->cosv * px - w->sinv * py;
+    const float yb = w->sinv * px + w->cosv * py;
+    const float gamma = atan2f(yb, w->sod - xb);
+    const float col = (gamma - w->shu) / w->du + (float)g->Nu * 0.5f - 0.5f;
+    if (col < -0.5f || col > (float)g->Nu - 0.5f) return 0;
+    const float src_z = source_z_view + shift_z;
+    const float rx = px - w->sx, ry = py - w->sy;
+    const float rxy = sqrtf(rx * rx + ry * ry);
+    if (rxy <= 1.0e-6f) return 0;
+    const float det_z = src_z + w->sdd * (pz - src_z) / rxy;
+    const float row = (det_z - source_z_view - (float)g->shv) / (float)g->dv + (float)g->Nv * 0.5f - 0.5f;
+    return row >= -0.5f && row <= (float)g->Nv - 0.5f;
+}
+
+/* View window of a z slice: [vs, ve], its end angles and centre angle. */
+typedef struct {
+    int vs, ve;
+    float bs, be, bc;
+} hzwin_t;
+
+/* Redundancy weight of one (voxel, view) pair (helical_arc3d.cu:1148-1180);
+ * *measured says whether the voxel centre projects onto the detector. */
+static float hw_pair_weight(const geo3_t* g, const hopt_t* o, const float* ang, const float* sp, int nview,
+                            const hzwin_t* zw, float db, float gmax, int ix, int iy, int iz, int v, int* measured)
+{
+    const float px = ((float)ix - (float)g->W / 2.0f + 0.5f) * (float)g->dx + (float)g->shx;
+    const float py = ((float)g->H * 0.5f - (float)iy - 0.5f) * (float)g->dy + (float)g->shy;
+    const float pz = ((float)iz - (float)g->D / 2.0f + 0.5f) * (float)g->dz + (float)g->shz;
+    const hwview_t w = hw_view(g, ang, sp, nview, v);
+    *measured = 0;
+    const float rx = px - w.sx, ry = py - w.sy;
+    const float rxy = sqrtf(rx * rx + ry * ry);
+    if (rxy <= 1.0e-6f) return 0.0f;
+    const float xb = w.cosv * px - w.sinv * py;
+    const float yb = w.sinv * px + w.cosv * py;
+    const float gamma = atan2f(yb, w.sod - xb);
+    const float wt = hw_weight(px, py, pz, w.beta, gamma, w.szv, rxy, zw->bc, zw->bs, zw->be, db, gmax, ang, sp,
+                               nview, g, o);
+    if (wt != 0.0f) *measured = hw_measured(px, py, pz, &w, sp[v], sp[3 * nview + v], g);
+    return wt;
+}
+
+/* Apply one helical operator.  fo = {view_mode, weight_mode, view_turns,
+ * halfscan_coef, tang_k, tang_blend}; sp = source_pos [4][nview]. */
+int xo_helical3d(int op, const int* ni, const double* fv, const double* fg, const double* fo,
+                 const double* in, double* out, const float* ang, const float* sp, int nbatch, int nview)
+{
+    geo3_t g;
+    g.W = ni[0]; g.H = ni[1]; g.D = ni[2]; g.Nu = ni[3]; g.Nv = ni[4]; g.type = GEO_ARC;
+    g.dx = fv[0]; g.dy = fv[1]; g.dz = fv[2]; g.shx = fv[3]; g.shy = fv[4]; g.shz = fv[5];
+    g.du = fg[0]; g.dv = fg[1]; g.shu = fg[2]; g.shv = fg[3]; g.sod = fg[4]; g.sdd = fg[5];
+    hopt_t o;
+    o.view_mode = (int)fo[0]; o.weight_mode = (int)fo[1];
+    o.view_turns = (float)fo[2]; o.halfscan_coef = (float)fo[3]; o.tang_k = (float)fo[4]; o.tang_blend = (float)fo[5];
+    if (op < 0 || op > 5 || nview < 1) return 1;
+    const long long nvox = (long long)g.W * g.H * g.D;
+    const long long ncell = (long long)g.Nu * g.Nv;
+    const int out_is_sino = (op == OP_A || op == OP_BT || op == OP_BWT);
+    memset(out, 0, sizeof(double) * (size_t)nbatch * (size_t)(out_is_sino ? ncell * nview : nvox));
+    const int weighted = (op == OP_BW || op == OP_BWT);
+
+    /* weighted ops: per-slice windows and per-voxel scales */
+    hzwin_t* zw = NULL;
+    float* scale = NULL;
+    const float db = (nview > 1) ? (ang[nview - 1] - ang[0]) / (float)(nview - 1) : 0.0f;
+    const float gmax = (float)g.du * (float)(g.Nu - 1) * 0.5f;
+    if (weighted) {
+        zw = malloc(sizeof(hzwin_t) * g.D);
+        scale = malloc(sizeof(float) * (size_t)nvox);
+        for (int iz = 0; iz < g.D; ++iz) {
+            const float pz = ((float)iz - (float)g.D / 2.0f + 0.5f) * (float)g.dz + (float)g.shz;
+            hw_view_window(pz, ang, sp, &g, &o, nview, &zw[iz].vs, &zw[iz].ve);
+            zw[iz].bs = ang[zw[iz].vs];
+            zw[iz].be = ang[zw[iz].ve];
+            zw[iz].bc = hw_center_beta(pz, ang, sp, zw[iz].vs, zw[iz].ve, nview);
+        }
+        for (int iz = 0; iz < g.D; ++iz)
+            for (int iy = 0; iy < g.H; ++iy)
+                for (int ix = 0; ix < g.W; ++ix) {
+                    float valid = 0.0f;
+                    for (int v = zw[iz].vs; v <= zw[iz].ve; ++v) {
+                        int meas;
+                        const float wt = hw_pair_weight(&g, &o, ang, sp, nview, &zw[iz], db, gmax, ix, iy, iz, v, &meas);
+                        if (wt != 0.0f && meas) valid += wt;
+                    }
+                    const float ideal = (fabsf(db) > 1.0e-8f) ? (XO_PI_F / fabsf(db)) : valid;
+                    float s = ideal / fmaxf(valid, 1.0e-6f);
+                    s = fminf(32.0f, fmaxf(0.03125f, s));
+                    scale[((long long)iz * g.H + iy) * g.W + ix] = s;
+                }
+    }
+    const double cwW = (double)((float)g.sod * (float)g.du);   /* helical_arc3d.cu:1144 */
+
+    const int nline_max = g.W > g.H ? g.W : g.H;
+    double* D = malloc(sizeof(double) * (g.Nu + 1));
+    double* M = malloc(sizeof(double) * g.Nu);
+    double* zd = malloc(sizeof(double) * (g.Nv + 1));
+    double* X = malloc(sizeof(double) * (nline_max + 1));
+    double* Zv = malloc(sizeof(double) * (g.D + 1));
+    double* Zc = malloc(sizeof(double) * (g.Nv + 1));
+    const int nxo = nline_max + g.Nu + 2, nzo = g.D + g.Nv + 2;
+    int* xa = malloc(sizeof(int) * nxo); int* xb = malloc(sizeof(int) * nxo);
+    double* xl = malloc(sizeof(double) * nxo);
+    int* za = malloc(sizeof(int) * nzo); int* zb = malloc(sizeof(int) * nzo);
+    double* zl = malloc(sizeof(double) * nzo);
+    const double z0 = -0.5 * g.D * g.dz + g.shz;
+
+    for (int view = 0; view < nview; ++view) {
+        hview_t hv;
+        helical_view(&g, ang, sp, nview, view, &hv);
+        const geo3_t* gv = &hv.g;
+        const view_t* v = &hv.v;
+        view_columns3d(gv, v, D, M, zd);
+        for (int r = 0; r <= g.Nv; ++r) zd[r] = hv.zrow0 + r * g.dv;
+        const double dperp = v->use_x ? g.dy : g.dx;
+        const int nlines = v->use_x ? g.H : g.W;
+        for (int line = 0; line < nlines; ++line) {
+            double Mv, perp;
+            const int npix = line_pixels3d(gv, v, line, X, &Mv, &perp);
+            for (int i = 0; i <= g.D; ++i) Zv[i] = Mv * (z0 - hv.zsrc + i * g.dz);
+            const int nx = overlaps(X, npix, D, g.Nu, xa, xb, xl);
+            for (int e = 0; e < nx; ++e) {
+                const int p = xa[e], k = xb[e];
+                const int ix = v->use_x ? p : line;
+                const int iy = v->use_x ? line : g.H - 1 - p;
+                const int col = v->keep ? k : g.Nu - 1 - k;
+                for (int r = 0; r <= g.Nv; ++r) Zc[r] = M[k] * zd[r];
+                const int nz = overlaps(Zv, g.D, Zc, g.Nv, za, zb, zl);
+                const double pixz = (X[p + 1] - X[p]) * Mv * g.dz;
+                double fbpw = 0.0;
+                if (weighted) {
+                    double px, py;
+                    voxel_xy(&g, ix, iy, &px, &py);
+                    const double ex = v->sx - px, ey = v->sy - py;
+                    fbpw = cwW / (pixz * (ex * ex + ey * ey));
+                }
+                for (int q = 0; q < nz; ++q) {
+                    const int iz = za[q], r = zb[q];
+                    const double coef = xl[e] * zl[q];
+                    double s;
+                    if (op == OP_A || op == OP_AT) {
+                        const double dD = D[k + 1] - D[k];
+                        const double dZ = Zc[r + 1] - Zc[r];
+                        const double a = 0.5 * (D[k + 1] + D[k]) - v->spar;
+                        const double b = 0.5 * (Zc[r + 1] + Zc[r]) + hv.zsrc;
+                        const double cosw = fabs(v->sperp) / sqrt(a * a + b * b + v->sperp * v->sperp);
+                        s = dperp / (dD * dZ * cosw);
+                    } else if (!weighted) {
+                        s = hv.cwB / pixz;
+                    } else {
+                        if (view < zw[iz].vs || view > zw[iz].ve) continue;
+                        int meas;
+                        const float wt = hw_pair_weight(&g, &o, ang, sp, nview, &zw[iz], db, gmax, ix, iy, iz, view,
+                                                        &meas);
+                        if (wt == 0.0f) continue;
+                        s = fbpw * (double)wt * (double)scale[((long long)iz * g.H + iy) * g.W + ix];
+                    }
+                    for (int bt = 0; bt < nbatch; ++bt) {
+                        const long long vi = ((long long)(bt * g.D + iz) * g.H + iy) * g.W + ix;
+                        const long long ci = (((long long)bt * nview + view) * g.Nv + r) * g.Nu + col;
+                        switch (op) {
+                        case OP_A:   out[ci] += coef * s * in[vi]; break;
+                        case OP_AT:
+                        case OP_B:
+                        case OP_BW:  out[vi] += coef * s * in[ci]; break;
+                        default:     out[ci] += coef * s * in[vi]; break;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    free(D); free(M); free(zd); free(X); free(Zv); free(Zc);
+    free(xa); free(xb); free(xl); free(za); free(zb); free(zl);
+    free(zw); free(scale);
+    return 0;
+}

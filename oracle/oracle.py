@@ -4,8 +4,8 @@ TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
 CPU-baseline leg of ``bench.py`` import this module; the product package never
 does.
 
-* :func:`dd2d` / :func:`dd3d` run the C restatement ``dd_oracle.c`` in double
-  precision.  They take the reference's packed ``options`` vector (12 entries
+* :func:`dd2d` / :func:`dd3d` / :func:`helical3d` run the C restatement
+  ``dd_oracle.c`` in double precision.  They take the reference's packed ``options`` vector (12 entries
   in 2D, 18 in 3D) and unpack it exactly as the reference binding does
   (XRecon ``src/api/torch_binding.cpp:62-124``), so both sides see identical
   float32 parameter values.
@@ -44,6 +44,11 @@ def _load():
                            ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                            ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int]
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.xo_helical3d.restype = ctypes.c_int
+        lib.xo_helical3d.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp, dp, dp, dp, dp,
+                                     ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                     ctypes.c_int, ctypes.c_int]
         _lib = lib
     return _lib
 
@@ -105,6 +110,43 @@ def dd3d(op: str, x, options, angles):
                          _p(ang, ctypes.c_float), B * C, V)
     if rc != 0:
         raise RuntimeError(f"oracle dd3d failed with status {rc}")
+    return out
+
+
+def unpack_helical(options):
+    """Helical fields of the 3D options vector with the binding's defaults
+    (torch_binding.cpp:103-108): view_mode, weight_mode, view_turns,
+    halfscan_coef, tang_k, tang_blend."""
+    o = np.asarray(options, dtype=np.float32)
+    dflt = [2.0, 0.0, 0.0, 1.0, 5.0, 0.0]
+    vals = [float(o[18 + i]) if o.size > 18 + i else dflt[i] for i in range(6)]
+    vals[0], vals[1] = float(int(vals[0])), float(int(vals[1]))
+    return vals
+
+
+def helical3d(op: str, x, options, angles, source_pos):
+    """Apply a helical arc-detector operator (the reference's
+    src/kernels/helical_arc3d.cu).  x: [B, C, D, H, W] or [B, C, V, Nv, Nu];
+    source_pos: [4, V] (source_z, shift_radius, shift_angle, shift_z)."""
+    g = unpack3d(options)
+    ang = np.ascontiguousarray(angles, dtype=np.float32)
+    V = ang.shape[0]
+    sp = np.ascontiguousarray(source_pos, dtype=np.float32)
+    if sp.shape != (4, V):
+        raise ValueError(f"source_pos must be [4, {V}], got {sp.shape}")
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    B, C = x.shape[:2]
+    out_shape = (B, C, V, g["Nv"], g["Nu"]) if op in SINO_OUT else (B, C, g["D"], g["H"], g["W"])
+    out = np.zeros(out_shape, dtype=np.float64)
+    ni = np.array([g["W"], g["H"], g["D"], g["Nu"], g["Nv"]], dtype=np.int32)
+    fv = np.array([g["dx"], g["dy"], g["dz"], g["shx"], g["shy"], g["shz"]], dtype=np.float64)
+    fg = np.array([g["du"], g["dv"], g["shu"], g["shv"], g["SOD"], g["SDD"]], dtype=np.float64)
+    fo = np.array(unpack_helical(options), dtype=np.float64)
+    rc = _load().xo_helical3d(OPS[op], _p(ni, ctypes.c_int), _p(fv, ctypes.c_double), _p(fg, ctypes.c_double),
+                              _p(fo, ctypes.c_double), _p(x, ctypes.c_double), _p(out, ctypes.c_double),
+                              _p(ang, ctypes.c_float), _p(sp, ctypes.c_float), B * C, V)
+    if rc != 0:
+        raise RuntimeError(f"oracle helical3d failed with status {rc}")
     return out
 
 

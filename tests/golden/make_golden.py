@@ -23,7 +23,11 @@ from the reference's code path on CPU:
   (``python tests/golden/make_golden.py sysmat`` writes only these);
 * rebin_<case>.npz: the reference's fan/helical -> parallel rebinning
   (xrecon/utils/rebin.py, pure torch) on seeded inputs
-  (``python tests/golden/make_golden.py rebin``).
+  (``python tests/golden/make_golden.py rebin``);
+* helical_host.npz: HelicalProjector3d's packed options, weight, filter and
+  source positions (``python tests/golden/make_golden.py helical_host``).
+The reference's helical operators themselves are CUDA only; their outputs
+are recorded on a GPU by tests/golden/make_golden_helical.py.
 """
 from __future__ import annotations
 
@@ -217,12 +221,52 @@ def make_rebin():
     print("rebinning fixtures written to", HERE)
 
 
+HELICAL_HOST_CASES = {
+    # name: (constructor keyword arguments, number of views)
+    "one_turn": (dict(image_size=(32, 32, 16), num_det=(48, 8), pix_size=(2.0, 2.0, 1.0), det_size=(2.4, 2.0),
+                      iso_source=300.0, source_detector=600.0, pixshift=(0.1, -0.2, 0.3), binshift=(0.3, -0.1),
+                      pitch=8.0, z0=-8.0), 192),
+    "auto_tang": (dict(image_size=(24, 20, 12), num_det=(40, 6), pix_size=(2.5, 2.5, 1.5), det_size=(3.0, 2.5),
+                       iso_source=320.0, source_detector=640.0, pitch=12.0, z0=-9.0, helical_view_mode="auto",
+                       helical_weight_mode="tang3d", helical_tang_k=3.0, helical_tang_blend=0.6,
+                       filter_type="hann"), 150),
+    "half_scan": (dict(image_size=(32, 32, 16), num_det=(48, 8), pix_size=(2.0, 2.0, 1.0), det_size=(2.4, 2.0),
+                       iso_source=300.0, source_detector=600.0, pitch=14.0, z0=-10.0, helical_view_mode="half",
+                       helical_halfscan_coef=1.1, filter_type="shepplogan"), 180),
+}
+
+
+def make_helical_host():
+    """helical_host.npz: the reference HelicalProjector3d's packed options,
+    cell weight, filter, source_position and mean angle step
+    (xrecon/projector/projector3d.py:289-576, pure Python) for a few
+    configurations; no operator is run."""
+    sys.modules["xrecon_C"] = refcpu.RefXreconC()
+    sys.path.insert(0, str(REF_ROOT))
+    from xrecon.projector.projector3d import HelicalProjector3d
+    out = {}
+    for name, (kw, V) in HELICAL_HOST_CASES.items():
+        P = HelicalProjector3d(**kw)
+        ang = torch.arange(V, dtype=torch.float32) * (2 * np.pi / 96) + 0.05
+        out[f"{name}_options"] = P.options.numpy()
+        out[f"{name}_weight"] = P.weight.numpy()
+        out[f"{name}_filter"] = P.filter.numpy()
+        out[f"{name}_angles"] = ang.numpy()
+        out[f"{name}_source_pos"] = P.source_position(ang).numpy()
+        out[f"{name}_mean_step"] = np.float32(P._mean_angle_step(ang).item())
+    np.savez_compressed(HERE / "helical_host.npz", **out)
+    print("helical host fixtures written to", HERE)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["sysmat"]:
         make_sysmat()
     elif sys.argv[1:] == ["rebin"]:
         make_rebin()
+    elif sys.argv[1:] == ["helical_host"]:
+        make_helical_host()
     else:
         main()
         make_sysmat()
         make_rebin()
+        make_helical_host()

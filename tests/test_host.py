@@ -131,3 +131,66 @@ def test_backend_surface_matches_reference_names():
         assert callable(getattr(backend, n))
     with pytest.raises(RuntimeError, match="at least 18"):
         backend._geom(3, torch.zeros(10))
+
+
+HELICAL_CASES = {
+    "one_turn": dict(image_size=(32, 32, 16), num_det=(48, 8), pix_size=(2.0, 2.0, 1.0), det_size=(2.4, 2.0),
+                     iso_source=300.0, source_detector=600.0, pixshift=(0.1, -0.2, 0.3), binshift=(0.3, -0.1),
+                     pitch=8.0, z0=-8.0),
+    "auto_tang": dict(image_size=(24, 20, 12), num_det=(40, 6), pix_size=(2.5, 2.5, 1.5), det_size=(3.0, 2.5),
+                      iso_source=320.0, source_detector=640.0, pitch=12.0, z0=-9.0, helical_view_mode="auto",
+                      helical_weight_mode="tang3d", helical_tang_k=3.0, helical_tang_blend=0.6, filter_type="hann"),
+    "half_scan": dict(image_size=(32, 32, 16), num_det=(48, 8), pix_size=(2.0, 2.0, 1.0), det_size=(2.4, 2.0),
+                      iso_source=300.0, source_detector=600.0, pitch=14.0, z0=-10.0, helical_view_mode="half",
+                      helical_halfscan_coef=1.1, filter_type="shepplogan"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(HELICAL_CASES))
+def test_helical_projector_host_tables_match_reference(case):
+    """Packed options, cell weight, filter, source positions and mean angle
+    step of HelicalProjector3d against the reference's own class
+    (tests/golden/helical_host.npz)."""
+    from xrecon_b200 import HelicalProjector3d
+    g = load_golden("helical_host")
+    P = HelicalProjector3d(**HELICAL_CASES[case])
+    np.testing.assert_array_equal(P.options.numpy(), g[f"{case}_options"])
+    np.testing.assert_allclose(P.weight.numpy(), g[f"{case}_weight"], rtol=1e-6, atol=0)
+    ref_f = g[f"{case}_filter"]
+    np.testing.assert_allclose(P.filter.numpy(), ref_f, rtol=2e-6, atol=1e-7 * np.abs(ref_f).max())
+    ang = torch.from_numpy(g[f"{case}_angles"])
+    np.testing.assert_allclose(P.source_position(ang).numpy(), g[f"{case}_source_pos"], rtol=1e-6, atol=1e-6)
+    assert abs(float(P._mean_angle_step(ang)) - float(g[f"{case}_mean_step"])) <= 1e-7
+
+
+def test_helical_validation_without_gpu():
+    """xr_helical3d argument checks (no kernel runs): arc detector only,
+    known view / weight modes, workspace size."""
+    from xrecon_b200 import HelicalProjector3d, backend
+    P = HelicalProjector3d(**HELICAL_CASES["one_turn"])
+    lib = _native.lib()
+    g = P._host_geom.struct
+    h = P._host_geom.hopts
+    assert (h.view_mode, h.weight_mode) == (2, 0)
+    for op in range(6):
+        assert lib.xr_helical3d_workspace_size(op, ctypes.byref(g), 1, 192) > 0
+    p = ctypes.c_void_p(256)
+    flat = _native.geom3d_from_values(P.options.tolist()[:17] + [1.0])
+    rc = lib.xr_helical3d(0, ctypes.byref(flat), ctypes.byref(h), p, p, p, p, 1, 4, None, 0, None)
+    assert rc == 1 and b"arc" in lib.xr_last_error()
+    bad = _native.HelicalOpts(view_mode=7, weight_mode=0, view_turns=0.0, halfscan_coef=1.0, tang_k=5.0,
+                              tang_blend=0.0)
+    rc = lib.xr_helical3d(0, ctypes.byref(g), ctypes.byref(bad), p, p, p, p, 1, 4, None, 0, None)
+    assert rc == 1 and b"view mode" in lib.xr_last_error()
+    rc = lib.xr_helical3d(4, ctypes.byref(g), ctypes.byref(h), p, p, p, p, 1, 4, None, 0, None)
+    assert rc == 2 and b"workspace" in lib.xr_last_error()
+    for n in ("forward_projection_helical3d", "projection_transpose_helical3d", "backward_projection_helical3d",
+              "weighted_backward_projection_helical3d", "backward_projection_transpose_helical3d",
+              "weighted_backward_projection_transpose_helical3d"):
+        assert callable(getattr(backend, n))
+    with pytest.raises(NotImplementedError):
+        HelicalProjector3d(**dict(HELICAL_CASES["one_turn"], scan_type="flat"))
+    with pytest.raises(ValueError, match="helical_view_mode"):
+        HelicalProjector3d(**dict(HELICAL_CASES["one_turn"], helical_view_mode="spiral"))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        P.projection(torch.zeros(1, 1, 16, 32, 32), torch.zeros(3))

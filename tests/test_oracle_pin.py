@@ -112,3 +112,58 @@ def test_oracle_rebin_matches_reference(case):
     assert out.shape == g["out"].shape
     np.testing.assert_array_equal(t, g["t"])
     assert rel_l2(out, g["out"]) < 1e-5
+
+
+# ---------------------------------------------------------------- helical
+
+def _helical_case():
+    """Small arc geometry, 60 views over one turn, and its options vector."""
+    W, H, D, Nu, Nv = 24, 24, 12, 40, 8
+    opts = np.array([W, H, D, Nu, Nv, 1.0, 1.0, 1.0, 0.004, 1.2, 300.0, 600.0, 0.3, -0.2, 0.4, 0.001, 0.1, 2],
+                    np.float32)
+    V = 60
+    ang = (np.arange(V) * (2 * np.pi / V) + 0.05).astype(np.float32)
+    rng = np.random.default_rng(3)
+    x = rng.random((1, 1, D, H, W))
+    y = rng.random((1, 1, V, Nv, Nu))
+    return opts, ang, x, y, rng
+
+
+def test_helical_oracle_reduces_to_the_circular_arc():
+    """With every source offset zero the helical operators are the cone-arc
+    ones (which are pinned to the reference above): A and A^T identically, B
+    and B^T up to the column width sod du vs 2 sod tan(du/2) (du^2/12).  With
+    a constant source z, B and B^T equal the circular ones on a volume shifted
+    by -z; A carries the reference's absolute-z cell cosine and moves."""
+    opts, ang, x, y, _ = _helical_case()
+    V = ang.size
+    sp = np.zeros((4, V), np.float32)
+    for op, inp, tol in (("A", x, 1e-12), ("AT", y, 1e-12), ("B", y, 2e-6), ("BT", x, 2e-6)):
+        err = rel_l2(O.helical3d(op, inp, opts, ang, sp), O.dd3d(op, inp, opts, ang))
+        assert err < tol, (op, err)
+    c = np.float32(2.5)
+    sp[0] = c
+    shifted = opts.copy()
+    shifted[14] = opts[14] - c
+    for op, inp in (("B", y), ("BT", x)):
+        assert rel_l2(O.helical3d(op, inp, opts, ang, sp), O.dd3d(op, inp, shifted, ang)) < 2e-6
+    assert rel_l2(O.helical3d("A", x, opts, ang, sp), O.dd3d("A", x, shifted, ang)) > 1e-5
+
+
+@pytest.mark.parametrize("modes", [(2, 0), (0, 1), (1, 0), (3, 0)])
+def test_helical_oracle_adjoint_pairs(modes):
+    """<A x, y> = <x, A^T y>, <B^T x, y> = <x, B y>, <Bw^T x, y> = <x, Bw y>
+    with flying-focal-spot style offsets, for several view / weight modes."""
+    opts, ang, x, y, rng = _helical_case()
+    V = ang.size
+    o = np.concatenate([opts, np.array([modes[0], modes[1], 1.5, 1.0, 4.0, 0.5], np.float32)])
+    sp = np.zeros((4, V), np.float32)
+    sp[0] = np.linspace(-4.0, 4.0, V)
+    sp[1] = rng.normal(0.0, 1.0, V)
+    sp[2] = rng.normal(0.0, 5e-4, V)
+    sp[3] = rng.normal(0.0, 0.3, V)
+    for fwd, adj in (("A", "AT"), ("BT", "B"), ("BWT", "BW")):
+        lhs = float(np.sum(O.helical3d(fwd, x, o, ang, sp) * y))
+        rhs = float(np.sum(x * O.helical3d(adj, y, o, ang, sp)))
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs), (fwd, adj, lhs, rhs)
+        assert lhs != 0.0

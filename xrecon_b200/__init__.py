@@ -10,12 +10,13 @@ module ``xrecon_C``.
 from .geometry import (ConeBeam3d, Detector2d, Detector3d, FanBeam2d, HelicalConeBeam3d, ParallelBeam2d,
                        ParallelBeam3d, Volume2d, Volume3d)
 from .phantom import phantom
-from .projector import Projector2d, Projector3d, projector2d, projector3d
+from .projector import HelicalProjector3d, Projector2d, Projector3d, projector2d, projector3d
 
 __version__ = "0.1.0"
 
 __all__ = [
-    "Detector2d", "Detector3d", "FanBeam2d", "ConeBeam3d", "HelicalConeBeam3d", "ParallelBeam2d",
+    "Detector2d", "Detector3d", "FanBeam2d", "ConeBeam3d", "HelicalConeBeam3d", "HelicalProjector3d",
+    "ParallelBeam2d",
     "ParallelBeam3d", "Projector2d", "Projector3d", "Volume2d", "Volume3d", "projector2d", "projector3d",
     "phantom",
 ]

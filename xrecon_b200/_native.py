@@ -33,6 +33,12 @@ class Geom3d(ctypes.Structure):
                 ("shift_u", c_float), ("shift_v", c_float)]
 
 
+class HelicalOpts(ctypes.Structure):
+    """xr_helical_opts: entries 18..23 of HelicalProjector3d's options."""
+    _fields_ = [("view_mode", c_int), ("weight_mode", c_int), ("view_turns", c_float),
+                ("halfscan_coef", c_float), ("tang_k", c_float), ("tang_blend", c_float)]
+
+
 _lib = None
 
 
@@ -78,6 +84,11 @@ def lib():
         fn = getattr(L, f"xr_sysmat{d}d")
         fn.restype = c_int
         fn.argtypes = [ctypes.POINTER(G), c_void_p, c_int] + [c_void_p] * 5 + [c_void_p, c_size_t, c_void_p]
+    L.xr_helical3d_workspace_size.restype = c_size_t
+    L.xr_helical3d_workspace_size.argtypes = [c_int, ctypes.POINTER(Geom3d), c_int, c_int]
+    L.xr_helical3d.restype = c_int
+    L.xr_helical3d.argtypes = [c_int, ctypes.POINTER(Geom3d), ctypes.POINTER(HelicalOpts), c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_int, c_int, c_void_p, c_size_t, c_void_p]
     L.xr_launch_count.restype = ctypes.c_ulonglong
     L.xr_launch_count.argtypes = []
     L.xr_version.restype = ctypes.c_char_p
@@ -186,6 +197,49 @@ def apply(dim: int, op: str, x: torch.Tensor, geom, angles: torch.Tensor,
                 ang.data_ptr(), nbatch, V, ws.data_ptr(), ws.numel(), stream)
     if rc != 0:
         _raise(rc, f"xr_dd{dim}d({op})")
+    return out
+
+
+def helical_opts_from_values(vals) -> HelicalOpts:
+    """Entries 18..23 of the packed helical options with the binding's
+    defaults when absent (torch_binding.cpp:103-108)."""
+    v = [float(x) for x in vals]
+    get = (lambda i, d: v[i] if len(v) > i else d)
+    return HelicalOpts(view_mode=int(get(18, 2.0)), weight_mode=int(get(19, 0.0)), view_turns=get(20, 0.0),
+                       halfscan_coef=get(21, 1.0), tang_k=get(22, 5.0), tang_blend=get(23, 0.0))
+
+
+def helical(op: str, x: torch.Tensor, geom: Geom3d, hopts: HelicalOpts, angles: torch.Tensor,
+            source_pos: torch.Tensor) -> torch.Tensor:
+    """Run one helical operator (float32) on a CUDA tensor; returns a new tensor."""
+    _check_cuda("input", x)
+    dev = x.device
+    if x.dtype != torch.float32:
+        raise RuntimeError("Helical 3D tensors must be float32")
+    if x.dim() != 5 or not x.is_contiguous():
+        raise RuntimeError("input must be a contiguous 5-D tensor")
+    ang = _angles(angles, dev)
+    V = ang.numel()
+    sp = source_pos.to(device=dev, dtype=torch.float32).contiguous()
+    if tuple(sp.shape) != (4, V):
+        raise RuntimeError("source_pos must have shape [4, num_view]")
+    if op in SINO_OUT:
+        shape = (x.shape[0], x.shape[1], V, geom.Nv, geom.Nu)
+    else:
+        shape = (x.shape[0], x.shape[1], geom.D, geom.H, geom.W)
+    nbatch = int(x.shape[0] * x.shape[1])
+    if V == 0 or nbatch == 0 or x.numel() == 0:
+        return torch.zeros(shape, dtype=torch.float32, device=dev)
+    out = torch.empty(shape, dtype=torch.float32, device=dev)
+    L = lib()
+    with torch.cuda.device(dev):
+        nbytes = L.xr_helical3d_workspace_size(OPS[op], ctypes.byref(geom), nbatch, V)
+        ws = _workspace(nbytes, dev)
+        rc = L.xr_helical3d(OPS[op], ctypes.byref(geom), ctypes.byref(hopts), x.data_ptr(), out.data_ptr(),
+                            ang.data_ptr(), sp.data_ptr(), nbatch, V, ws.data_ptr(), ws.numel(),
+                            torch.cuda.current_stream(dev).cuda_stream)
+    if rc != 0:
+        _raise(rc, f"xr_helical3d({op})")
     return out
 
 

@@ -129,3 +129,67 @@ def backward_projection_transpose3d(image, options, ang):
 
 def weighted_backward_projection_transpose3d(image, options, ang):
     return _run(3, "BWT", image, options, ang)
+
+
+# ------------------------------------------------------------------ helical
+# torch_binding.cpp:525-612: (input, options[24], angles[V], source_pos[4, V]),
+# float32 CUDA tensors, arc detector only.
+
+class HelicalHostGeometry:
+    """Packed helical options (24 entries) already on the host."""
+
+    __slots__ = ("values", "struct", "hopts")
+
+    def __init__(self, values):
+        import numpy as np
+        self.values = [float(np.float32(v)) for v in values]
+        self.struct = _native.geom3d_from_values(self.values[:18])
+        self.hopts = _native.helical_opts_from_values(self.values)
+
+
+def _helical_geom(options):
+    if isinstance(options, HelicalHostGeometry):
+        return options
+    if isinstance(options, torch.Tensor):
+        if options.dtype != torch.float32:
+            raise RuntimeError("Helical 3D tensors must be float32")
+        vals = options.detach().reshape(-1).cpu().tolist()
+    else:
+        vals = list(options)
+    if len(vals) < 18:
+        raise RuntimeError("3D option tensor must have at least 18 elements.")
+    return HelicalHostGeometry(vals)
+
+
+def _run_helical(op, x, options, angles, source_pos):
+    _check(x, options, angles)
+    if source_pos.device != x.device:
+        raise RuntimeError("Expected all tensors on the same device")
+    if not source_pos.is_contiguous():
+        raise RuntimeError("Expected all tensors to be contiguous")
+    hg = _helical_geom(options)
+    return _native.helical(op, x, hg.struct, hg.hopts, angles, source_pos)
+
+
+def forward_projection_helical3d(image, options, ang, source_pos):
+    return _run_helical("A", image, options, ang, source_pos)
+
+
+def projection_transpose_helical3d(proj, options, ang, source_pos):
+    return _run_helical("AT", proj, options, ang, source_pos)
+
+
+def backward_projection_helical3d(proj, options, ang, source_pos):
+    return _run_helical("B", proj, options, ang, source_pos)
+
+
+def weighted_backward_projection_helical3d(proj, options, ang, source_pos):
+    return _run_helical("BW", proj, options, ang, source_pos)
+
+
+def backward_projection_transpose_helical3d(image, options, ang, source_pos):
+    return _run_helical("BT", image, options, ang, source_pos)
+
+
+def weighted_backward_projection_transpose_helical3d(image, options, ang, source_pos):
+    return _run_helical("BWT", image, options, ang, source_pos)

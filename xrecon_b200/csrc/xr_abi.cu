@@ -21,6 +21,7 @@
 #include "xr_ragged.cuh"
 #include "xr_sysmat.cuh"
 #include "xr_rebin.cuh"
+#include "xr_helical.cuh"
 #include "../../include/xrecon_b200.h"
 
 
@@ -305,6 +306,7 @@ ViewTables tables_at(char* ws, const Layout& l) {
     t.colE = reinterpret_cast<float*>(ws + l.colE);
     t.colF = reinterpret_cast<float*>(ws + l.colF);
     t.colM = reinterpret_cast<float*>(ws + l.colM);
+    t.hel = nullptr;
     return t;
 }
 
@@ -363,11 +365,12 @@ template <> constexpr int dtype_code<float>() { return DT_F32; }
 template <> constexpr int dtype_code<__nv_bfloat16>() { return DT_BF16; }
 template <> constexpr int dtype_code<__half>() { return DT_F16; }
 
-template <typename TI, typename TO, int R, int MODE>
+template <typename TI, typename TO, int R, int MODE, bool HEL>
 int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr, const CUtensorMap& mc,
                          const TI* rows, const TI* cols, int pitch_r, int pitch_c, TO* out, int nbatch, int nview,
                          const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
-    auto kern = p.fine ? cell_tma3d_kernel<TI, TO, R, 2, MODE, true> : cell_tma3d_kernel<TI, TO, R, 2, MODE, false>;
+    auto kern = p.fine ? cell_tma3d_kernel<TI, TO, R, 2, MODE, true, HEL>
+                       : cell_tma3d_kernel<TI, TO, R, 2, MODE, false, HEL>;
     const int maxlines = std::max(g.W, g.H);
     const size_t smem = 2 * (size_t)cell_stage_elems<TI>(p.BP, p.BZ) * sizeof(TI) + 16 + (size_t)maxlines * sizeof(int4);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -386,12 +389,25 @@ int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr
 
 // Cell gather with TMA line windows; returns -1 when this configuration is
 // not covered (the caller then uses the plain kernel).
-template <typename TI, typename TO>
+// Window plan of a helical scan: the views' z placement varies, so the z
+// extent is sized on a volume deep enough that no window is clamped, then
+// capped at the real depth (a window never spans more than D + 2 slices).
+CellPlan plan_cell_helical(const Geom& g) {
+    Geom gp = g;
+    gp.D = 1 << 20;
+    gp.shz = 0.0;
+    CellPlan p = plan_cell(gp);
+    p.BZ = std::min(p.BZ, g.D + 2);
+    p.ok = p.ok && p.BZ >= 1;
+    return p;
+}
+
+template <typename TI, typename TO, bool HEL = false>
 int run_cell_tma(int eff, const Geom& g, const TI* in, TO* out, int nbatch, int nview, char* ws, const Layout& l,
                  const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
     if (!std::is_same<TO, TI>::value && !std::is_same<TO, float>::value) return -1;
     if (reinterpret_cast<uintptr_t>(in) % 16 != 0) return -1;
-    const CellPlan p = plan_cell(g);
+    const CellPlan p = HEL ? plan_cell_helical(g) : plan_cell(g);
     if (!p.ok || !encode_fn()) return -1;
     const size_t es = sizeof(TI);
     const int Hp = round_up(g.H, 8);
@@ -415,13 +431,13 @@ int run_cell_tma(int eff, const Geom& g, const TI* in, TO* out, int nbatch, int 
         !encode_line_map(&mc, dtype_code<TI>(), cols, g.H, g.W, g.D, nbatch, Hp, p.BP, p.BZ))
         return -1;
     if (p.R == 16) {
-        if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 16, OP_A>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-        if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 16, OP_BT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-        return launch_cell_tma_mode<TI, TO, 16, OP_BWT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+        if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 16, OP_A, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+        if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 16, OP_BT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+        return launch_cell_tma_mode<TI, TO, 16, OP_BWT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
     }
-    if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 8, OP_A>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-    if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 8, OP_BT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-    return launch_cell_tma_mode<TI, TO, 8, OP_BWT>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+    if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 8, OP_A, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+    if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 8, OP_BT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+    return launch_cell_tma_mode<TI, TO, 8, OP_BWT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
 }
 
 template <typename TI, typename TO>
@@ -651,6 +667,150 @@ int sysmat(int dim3d, const Geom& g, const float* ang, int nview, const long lon
     return check_cuda("sysmat");
 }
 
+// ------------------------------------------------------ helical scans
+
+struct HelLayout {
+    Layout l;  // view tables (+ the flipped image for A / B^T, row prefix tables for B, A^T, Bw)
+    size_t hel, wv, zw, scan, scale, imgs, total;
+};
+
+HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
+    HelLayout h;
+    // Bw^T reads the normalised image directly: view tables only
+    h.l = layout(1, op == OP_BWT ? -1 : op, g, nbatch, nview, DT_F32);
+    size_t o = h.l.total;
+    const size_t V = (size_t)(nview > 0 ? nview : 1);
+    h.hel = o;  o = align256(o + V * sizeof(HelView));
+    h.wv = o;   o = align256(o + V * sizeof(HelWView));
+    h.zw = h.scan = h.scale = h.imgs = o;
+    if (op == OP_BW || op == OP_BWT) {
+        const size_t nvox = (size_t)g.D * g.H * g.W;
+        h.zw = o;    o = align256(o + (size_t)g.D * sizeof(HelZ));
+        h.scan = o;  o = align256(o + sizeof(HelScanF));
+        h.scale = o; o = align256(o + nvox * sizeof(float));
+        if (op == OP_BWT) { h.imgs = o; o = align256(o + (size_t)nbatch * nvox * sizeof(float)); }
+    }
+    h.total = o;
+    return h;
+}
+
+constexpr int HEL_WBP_R = 8;
+constexpr int HEL_WBP_NWY = 8;
+constexpr int HEL_WBPT_R = 8;
+
+int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out, const float* ang,
+            const float* sp, int nbatch, int nview, void* workspace, size_t ws_bytes, void* stream) {
+    if (int rc = validate(g, 1, op, nbatch, nview)) return rc;
+    if (g.type != GEO_ARC)
+        return fail(XR_ERR_INVALID_ARGUMENT, "helical operators need the arc detector (type 2), got %d", g.type);
+    if (nview < 1) return fail(XR_ERR_INVALID_ARGUMENT, "helical operators need at least one view");
+    if (!in || !out || !ang || !sp) return fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
+    if (o.view_mode < 0 || o.view_mode > 3) return fail(XR_ERR_INVALID_ARGUMENT, "view mode %d not in 0..3", o.view_mode);
+    if (o.weight_mode < 0 || o.weight_mode > 1)
+        return fail(XR_ERR_INVALID_ARGUMENT, "weight mode %d not in 0..1", o.weight_mode);
+    const HelLayout hl = hel_layout(op, g, nbatch, nview);
+    if (!workspace || ws_bytes < hl.total)
+        return fail(XR_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", hl.total, ws_bytes);
+    if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+        return fail(XR_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* ws = static_cast<char*>(workspace);
+    ViewTables vt = tables_at(ws, hl.l);
+    vt.hel = reinterpret_cast<HelView*>(ws + hl.hel);
+    HelWView* wv = reinterpret_cast<HelWView*>(ws + hl.wv);
+    {
+        dim3 grid((g.Nu + 1 + 127) / 128, nview);
+        setup_views_helical_kernel<<<grid, 128, 0, st>>>(g, ang, sp, nview, vt, wv);
+        if (int rc = check_cuda("setup_views_helical")) return rc;
+    }
+    double zd0, dvv, z0dz;
+    row_params(g, zd0, dvv, z0dz);  // dvv; the z placement is per view
+    const GeomF gf = make_geomf(g, 1);
+    if (op == OP_A || op == OP_BT) {
+        if (!g_force_plain) {
+            const int rc = run_cell_tma<float, float, true>(op, g, in, out, nbatch, nview, ws, hl.l, vt, st, z0dz,
+                                                              zd0, dvv, 0.0f);
+            if (rc >= 0) return rc;
+        }
+        float* volT = reinterpret_cast<float*>(ws + hl.l.volT);
+        dim3 tg((g.W + 31) / 32, (g.H + 31) / 32, g.D * nbatch);
+        transpose_flip_kernel<float><<<tg, dim3(32, 8), 0, st>>>(in, volT, g.H, g.W, g.H);
+        if (int rc = check_cuda("transpose")) return rc;
+        const int nwarp = std::min(8, (g.Nv + CELL_R - 1) / CELL_R);
+        const int rows_per_cta = nwarp * CELL_R;
+        const int total = nview * nbatch;
+        for (int v0 = 0; v0 < total; v0 += 65535) {
+            const int nz = std::min(65535, total - v0);
+            dim3 grid((g.Nu + 31) / 32, (g.Nv + rows_per_cta - 1) / rows_per_cta, nz);
+            if (op == OP_A)
+                cell_gather3d_kernel<float, float, CELL_R, OP_A, true><<<grid, dim3(32, nwarp), 0, st>>>(
+                    g, vt, in, volT, out, nview, v0, z0dz, zd0, dvv, 0.0f);
+            else
+                cell_gather3d_kernel<float, float, CELL_R, OP_BT, true><<<grid, dim3(32, nwarp), 0, st>>>(
+                    g, vt, in, volT, out, nview, v0, z0dz, zd0, dvv, 0.0f);
+            if (int rc = check_cuda("cell_gather3d")) return rc;
+        }
+        return XR_OK;
+    }
+    if ((double)(g.Nv + 2) * g.Nu * sizeof(float2) >= 2147483648.0)
+        return fail(XR_ERR_UNSUPPORTED, "detector of %d x %d cells too large for one view's row table", g.Nu, g.Nv);
+    HelZ* zw = reinterpret_cast<HelZ*>(ws + hl.zw);
+    HelScanF* scan = reinterpret_cast<HelScanF*>(ws + hl.scan);
+    float* scale = reinterpret_cast<float*>(ws + hl.scale);
+    if (op == OP_BW || op == OP_BWT) {
+        hel_zwin_kernel<<<(g.D + 127) / 128, 128, 0, st>>>(g, o, ang, sp, nview, zw, scan);
+        if (int rc = check_cuda("hel_zwin")) return rc;
+        dim3 sg((g.W + 31) / 32, (g.H + 7) / 8, g.D);
+        hel_scale_kernel<<<sg, dim3(32, 8), 0, st>>>(g, o, scan, wv, zw, ang, sp, nview, scale);
+        if (int rc = check_cuda("hel_scale")) return rc;
+    }
+    if (op == OP_BWT) {
+        float* imgs = reinterpret_cast<float*>(ws + hl.imgs);
+        const size_t nvox = (size_t)g.D * g.H * g.W, n = nvox * nbatch;
+        hel_prescale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, scale, imgs, nvox, n);
+        if (int rc = check_cuda("hel_prescale")) return rc;
+        const int nwarp = std::min(8, (g.Nv + HEL_WBPT_R - 1) / HEL_WBPT_R);
+        const int rows_per_cta = nwarp * HEL_WBPT_R;
+        const int total = nview * nbatch;
+        for (int v0 = 0; v0 < total; v0 += 65535) {
+            const int nz = std::min(65535, total - v0);
+            dim3 grid((g.Nu + 31) / 32, (g.Nv + rows_per_cta - 1) / rows_per_cta, nz);
+            hel_wbpt_kernel<HEL_WBPT_R><<<grid, dim3(32, nwarp), 0, st>>>(g, vt, o, scan, wv, zw, ang, sp, imgs,
+                                                                          out, nview, v0, dvv);
+            if (int rc = check_cuda("hel_wbpt")) return rc;
+        }
+        return XR_OK;
+    }
+    float2* tab = reinterpret_cast<float2*>(ws + hl.l.sinoS);
+    const int nbv = nbatch * nview;
+    dim3 pg((g.Nu + 127) / 128, std::min(nbv, 65535));
+    if (op == OP_AT)
+        row_prefix3d_kernel<float, true, true><<<pg, 128, 0, st>>>(g, vt, in, tab, nview, nbv, zd0, dvv);
+    else
+        row_prefix3d_kernel<float, false><<<pg, 128, 0, st>>>(g, vt, in, tab, nview, nbv, zd0, dvv);
+    if (int rc = check_cuda("row_prefix3d")) return rc;
+    if (op == OP_BW) {
+        const int nzg = (g.D + HEL_WBP_R - 1) / HEL_WBP_R;
+        if ((long long)nzg * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
+        dim3 grid((g.W + 31) / 32, (g.H + HEL_WBP_NWY - 1) / HEL_WBP_NWY, nzg * nbatch);
+        hel_wbp_kernel<HEL_WBP_R, HEL_WBP_NWY><<<grid, dim3(32, HEL_WBP_NWY), 0, st>>>(
+            g, gf, vt, o, scan, wv, zw, ang, sp, tab, scale, out, nview, nzg, dvv);
+        return check_cuda("hel_wbp");
+    }
+    const int nzp = (g.D + PFX_R - 1) / PFX_R;
+    if ((long long)nzp * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
+    dim3 pgrid((g.W + 31) / 32, (g.H + PFX_NWY - 1) / PFX_NWY, nzp * nbatch);
+    dim3 pblock(32, PFX_NWY);
+    const float atconst = (float)(g.dx * g.dy * g.dz / (g.du * g.dv));
+    if (op == OP_AT)
+        vox_prefix3d_kernel<float, PFX_R, PFX_NWY, OP_AT, true><<<pgrid, pblock, 0, st>>>(
+            g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, 0.0f, atconst, 1.0f);
+    else
+        vox_prefix3d_kernel<float, PFX_R, PFX_NWY, OP_B, true><<<pgrid, pblock, 0, st>>>(
+            g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, 0.0f, atconst, 1.0f);
+    return check_cuda("vox_prefix3d");
+}
+
 // ------------------------------------------------------ ragged 2D batches
 
 struct RaggedLayout {
@@ -744,6 +904,26 @@ int xr_dd3d(int op, const xr_geom3d* geom, const void* in, int dtype_in, void* o
     if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
     return xr::apply(1, op, xr::geom_from(geom), in, dtype_in, out, dtype_out, angles, nbatch, nview,
                      workspace, workspace_bytes, stream, 1.0f);
+}
+
+size_t xr_helical3d_workspace_size(int op, const xr_geom3d* geom, int nbatch, int nview) {
+    if (!geom) return 0;
+    return xr::hel_layout(op, xr::geom_from(geom), nbatch, nview).total;
+}
+
+int xr_helical3d(int op, const xr_geom3d* geom, const xr_helical_opts* opts, const float* in, float* out,
+                 const float* angles, const float* source_pos, int nbatch, int nview, void* workspace,
+                 size_t workspace_bytes, void* stream) {
+    if (!geom || !opts) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry or options");
+    xr::HelOpts o;
+    o.view_mode = opts->view_mode;
+    o.weight_mode = opts->weight_mode;
+    o.view_turns = opts->view_turns;
+    o.halfscan_coef = opts->halfscan_coef;
+    o.tang_k = opts->tang_k;
+    o.tang_blend = opts->tang_blend;
+    return xr::helical(op, xr::geom_from(geom), o, in, out, angles, source_pos, nbatch, nview, workspace,
+                       workspace_bytes, stream);
 }
 
 int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, int nview, int rows_per_view,
@@ -989,6 +1169,7 @@ int xr_ragged2d_plan_bind(xr_ragged2d_plan* P, const float* images, float* sino,
         r.vt.colE = reinterpret_cast<float*>(ws + L.colE[i]);
         r.vt.colF = reinterpret_cast<float*>(ws + L.colF[i]);
         r.vt.colM = reinterpret_cast<float*>(ws + L.colM[i]);
+        r.vt.hel = nullptr;
         r.nview = in.nview;
         r.cw = column_width(r.g, 0);
         r.scale = in.scale;

@@ -94,13 +94,16 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
 #ifndef XR_CELL_MINB
 #define XR_CELL_MINB 2  // CTAs per SM the register budget is sized for
 #endif
-template <typename TI, typename TO, int R, int NB, int MODE, bool FINE>
+//
+// HEL: helical scan, the view's z placement and column width come from
+// vt.hel (the volume and detector rows measured from the view's source z).
+template <typename TI, typename TO, int R, int NB, int MODE, bool FINE, bool HEL = false>
 __global__ void __launch_bounds__(256, XR_CELL_MINB)
 cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUtensorMap map_rows,
                   const __grid_constant__ CUtensorMap map_cols, const TI* __restrict__ fb_rows,
                   const TI* __restrict__ fb_cols, const int pitch_rows, const int pitch_cols,
-                  TO* __restrict__ sino, const int nview, const int view0, const double z0dz, const double zd0,
-                  const double dvv, const float cw, const int BP, const int BZ) {
+                  TO* __restrict__ sino, const int nview, const int view0, const double z0dz_p,
+                  const double zd0_p, const double dvv, const float cw_p, const int BP, const int BZ) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // each stage starts on a 128-byte boundary (TMA destination alignment) and
     // holds BZ + 1 rows: the spare row absorbs the look-ahead read of the
@@ -124,6 +127,9 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     const bool active = (k < Nu) && (r0 < g.Nv);
 
     const ViewHdr h = vt.hdr[v];
+    const double z0dz = HEL ? vt.hel[v].z0dz : z0dz_p;
+    const double zd0 = HEL ? vt.hel[v].zd0 : zd0_p;
+    const float cw = HEL ? vt.hel[v].cw : cw_p;
     const int use_x = h.use_x, nlines = h.nlines, npix = h.npix;
     const size_t ob = (size_t)v * (Nu + 1);
     const double bA0 = vt.bA[ob + kc], bB0 = vt.bB[ob + kc];
@@ -347,7 +353,8 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
         if (r < g.Nv) {
             float sv = acc[i];
             if (MODE == OP_A) {
-                const float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+                float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+                if (HEL) zc += vt.hel[v].zsrc;  // helical: the row's absolute z
                 sv *= E * sqrtf(F + zc * zc);
             }
             st(out + (size_t)r * Nu, sv);

@@ -58,6 +58,18 @@ struct ViewHdr {
 //              order) on line L in pixel units, k = 0..Nu
 //   colQ[k]  = M_k / dz (3D), colR[k] = 1 / colQ[k] ; colE, colF, colM: cell scale of A,
 //              s_A(k, r) = colE[k] * sqrt(colF[k] + (colM[k] * zc_r)^2)
+// Per-view z placement and column scalars of a helical scan (all z measured
+// from the view's source z), used by the kernels' HEL variants:
+//   z0dz  = (volume bottom - source z) / dz
+//   zd0   = lower boundary of detector row 0 - source z   (rows zd0 + r dv)
+//   cw    = column width of B / B^T, sod' du'
+//   zsrc  = source z (the projection's cell cosine takes the row's absolute z)
+//   inv_du = 1 / du' (column guesses)
+struct HelView {
+    double z0dz, zd0;
+    float cw, zsrc, inv_du, pad;
+};
+
 struct ViewTables {
     ViewHdr* hdr;
     double* bA;
@@ -67,6 +79,7 @@ struct ViewTables {
     float* colE;
     float* colF;
     float* colM;
+    HelView* hel;  // helical scans only, else null
 };
 
 // ---------------------------------------------------------------- dtype io

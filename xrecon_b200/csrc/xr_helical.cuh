@@ -1,0 +1,635 @@
+// Helical cone-beam scans with an arc detector (the reference's
+// src/kernels/helical_arc3d.cu, bound at src/api/torch_binding.cpp:525-612).
+//
+// Every view has its own source placement, source_pos[4][V] =
+// (source_z, shift_radius, shift_angle, shift_z), helical_arc3d.cu:382-395:
+//     sod' = SOD + sr, sdd' = SDD + sr, du' = du SDD / sdd',
+//     shu' = shu SDD / sdd' - sa (sdd' - sod') / sdd',
+//     source at angle beta + sa, column angles sg du' + shu' + beta,
+//     source z = source_z + shift_z, detector rows (r - Nv/2) dv + source_z + shv.
+// A, A^T, B, B^T are the cone-arc DD operators of the circular path with
+// these per-view values: setup_views_helical_kernel writes the usual view
+// tables from a per-view Geom, plus a HelView with the view's z placement,
+// and the kernels' HEL variants read it.  The reference's A takes the cell
+// cosine with the row's absolute z (helical_arc3d.cu:432), which the HEL
+// variants reproduce.
+//
+// Bw and Bw^T (helical_arc3d.cu:1112-1505) weight each (voxel, view) pair of
+// the voxel's view window (a span of views centred on the view whose source
+// z is the voxel's z) with a redundancy weight and scale each voxel by
+// (pi / |dbeta|) / (sum of the weights of the views whose detector its centre
+// hits), clamped to [1/32, 32].  The window, the weights and the "measured"
+// test are evaluated in FP32 with the reference's operation order (explicit
+// round-to-nearest intrinsics where the result feeds a discrete decision), the
+// DD footprint through the FP64 view tables as elsewhere:
+//   hel_zwin_kernel   per z slice: window [vs, ve], its end angles, centre angle
+//   hel_scale_kernel  per voxel: the normalisation
+//   hel_wbp_kernel    Bw: voxel gather over the run's window through the row
+//                     prefix tables (xr_vox_prefix.cuh), per-voxel weights
+//   hel_wbpt_kernel   Bw^T: cell gather, the weight evaluated per voxel
+#pragma once
+
+#include "xr_vox_prefix.cuh"
+
+namespace xr {
+
+struct HelOpts {
+    int view_mode;    // 0 auto (from the pitch), 1 half scan, 2 one turn, 3 fixed turns
+    int weight_mode;  // 0 conjugate-ray redundancy ("2d"), 1 tangential ("tang3d")
+    float view_turns, halfscan_coef, tang_k, tang_blend;
+};
+
+// Per-view FP32 scalars of the weighted kernels (helical_arc3d.cu:1148-1160).
+struct HelWView {
+    float sod, sdd, du, shu, beta, sinv, cosv, sx, sy, szv, zs, shz;
+};
+
+// Per z slice: view window [vs, ve], its end angles, the centre angle, the
+// slice's z.
+struct HelZ {
+    int vs, ve;
+    float bs, be, bc, pz;
+};
+
+constexpr float XR_PI_F = 3.14159265358979323846f;
+
+// Scan scalars of the weighted kernels: mean angle step (angles[V-1] -
+// angles[0]) / (V - 1), half fan angle du (Nu - 1) / 2, column width SOD du.
+// Written on the device by hel_zwin_kernel (the angles live there).
+struct HelScanF {
+    float db, gmax, cwW, pad;
+};
+
+// ----------------------------------------------------------------- setup
+
+// One thread per (view, boundary k = 0..Nu), as setup_views_kernel, with the
+// view's own Geom; thread k == 0 also writes the view's HelView / HelWView.
+__global__ void setup_views_helical_kernel(const Geom g, const float* __restrict__ ang,
+                                           const float* __restrict__ sp, const int nview, const ViewTables vt,
+                                           HelWView* __restrict__ wv) {
+    const int v = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nview || k > g.Nu) return;
+    const float zs = sp[v], sr = sp[nview + v], sa = sp[2 * nview + v], szs = sp[3 * nview + v];
+    const float SOD = (float)g.sod, SDD = (float)g.sdd;
+    const float sod = __fadd_rn(SOD, sr), sdd = __fadd_rn(SDD, sr);
+    const float du = __fdiv_rn(__fmul_rn((float)g.du, SDD), sdd);
+    const float shu = __fsub_rn(__fdiv_rn(__fmul_rn((float)g.shu, SDD), sdd),
+                                __fdiv_rn(__fmul_rn(sa, __fsub_rn(sdd, sod)), sdd));
+    const float beta = __fadd_rn(ang[v], sa);
+    const float zsrc = __fadd_rn(zs, szs);
+    Geom gv = g;
+    gv.sod = sod;
+    gv.sdd = sdd;
+    gv.du = du;
+    // column angle sg du' + shu' + beta_unshifted, relative to the source angle
+    gv.shu = (double)shu + ((double)ang[v] - (double)beta);
+    setup_view_entry(gv, 1, beta, v, k, vt);
+    if (k != 0) return;
+    HelView hv;
+    hv.zd0 = -0.5 * g.Nv * g.dv + (double)zs + g.shv - (double)zsrc;
+    hv.z0dz = (-0.5 * g.D * g.dz + g.shz - (double)zsrc) / g.dz;
+    hv.cw = __fmul_rn(sod, du);
+    hv.zsrc = zsrc;
+    hv.inv_du = (float)(1.0 / (double)du);
+    hv.pad = 0.0f;
+    vt.hel[v] = hv;
+    HelWView w;
+    w.sod = sod;
+    w.sdd = sdd;
+    w.du = du;
+    w.shu = shu;
+    w.beta = beta;
+    w.sinv = sinf(beta);
+    w.cosv = cosf(beta);
+    w.sx = __fmul_rn(-w.sinv, sod);
+    w.sy = __fmul_rn(w.cosv, sod);
+    w.szv = zsrc;
+    w.zs = zs;
+    w.shz = szs;
+    wv[v] = w;
+}
+
+// ---------------------------------------------------------------- weights
+
+__device__ __forceinline__ float hw_clamp_unit(float x) { return fminf(1.0f, fmaxf(0.0f, x)); }
+
+__device__ __forceinline__ float hw_smooth_step(float x) {
+    x = hw_clamp_unit(x);
+    return 0.5f * (1.0f - cosf(XR_PI_F * x));
+}
+
+__device__ __forceinline__ float hw_window_quality(float beta, float bs, float be, float gamma, float gmax) {
+    const float lo = fminf(bs, be), hi = fmaxf(bs, be);
+    if (beta < lo || beta > hi) return 0.0f;
+    const float gc = fminf(fmaxf(gamma, -gmax), gmax);
+    const float lw = fmaxf(1.0e-6f, 2.0f * (gmax - gc));
+    const float rw = fmaxf(1.0e-6f, 2.0f * (gmax + gc));
+    if (beta < __fadd_rn(lo, lw)) return hw_smooth_step(__fdiv_rn(beta - lo, lw));
+    if (beta > __fsub_rn(hi, rw)) return hw_smooth_step(__fdiv_rn(hi - beta, rw));
+    return 1.0f;
+}
+
+__device__ __forceinline__ float hw_center_turn(float beta, float bc, float bs, float be, float db) {
+    const float lo = fminf(bs, be), hi = fmaxf(bs, be);
+    if (beta < lo || beta > hi) return 0.0f;
+    const float adb = fmaxf(fabsf(db), 1.0e-6f);
+    const float half = 0.5f * (hi - lo);
+    const float dist = fabsf(beta - bc);
+    const float crad = fminf(XR_PI_F, half);
+    if (dist <= crad) return 1.0f;
+    const float ow = fmaxf(half - crad, 4.0f * adb);
+    return hw_smooth_step(__fdiv_rn(half - dist, ow));
+}
+
+__device__ __forceinline__ float hw_source_z_at(float beta, const float* __restrict__ ang,
+                                                const float* __restrict__ zsrc, int nview) {
+    if (nview <= 1) return zsrc[0];
+    const float a0 = ang[0], a1 = ang[nview - 1];
+    const float range = a1 - a0;
+    if (fabsf(range) <= 1.0e-6f) return zsrc[0];
+    const float dzdb = __fdiv_rn(zsrc[nview - 1] - zsrc[0], range);
+    return __fadd_rn(zsrc[0], __fmul_rn(beta - a0, dzdb));
+}
+
+__device__ __forceinline__ float hw_edge_taper(float beta, float bc, float bs, float be, float db) {
+    const float lo = fminf(bs, be), hi = fmaxf(bs, be);
+    if (beta < lo || beta > hi) return 0.0f;
+    const float span = hi - lo, half = 0.5f * span;
+    if (span <= __fadd_rn(XR_PI_F, __fmul_rn(8.0f, fabsf(db)))) return 1.0f;
+    const float crad = fminf(XR_PI_F, half);
+    const float dist = fabsf(beta - bc);
+    if (dist <= crad) return 1.0f;
+    const float ew = fmaxf(half - crad, 4.0f * fabsf(db));
+    return hw_smooth_step(__fdiv_rn(half - dist, ew));
+}
+
+// helical_arc3d.cu:212-241
+__device__ __forceinline__ float hw_conjugate(float beta, float gamma, float bc, float bs, float be, float db,
+                                              float gmax) {
+    const float span = fabsf(be - bs);
+    const float adb = fmaxf(fabsf(db), 1.0e-6f);
+    if (span >= __fsub_rn(2.0f * XR_PI_F, 2.0f * adb)) {
+        const float turns = fmaxf(1.0f, floorf(__fdiv_rn(__fadd_rn(span, 2.0f * adb), 2.0f * XR_PI_F)));
+        return __fdiv_rn(0.5f * hw_center_turn(beta, bc, bs, be, db), turns);
+    }
+    const float q = hw_window_quality(beta, bs, be, gamma, gmax);
+    if (q <= 0.0f) return 0.0f;
+    const float dir = (db >= 0.0f) ? 1.0f : -1.0f;
+    float den = 0.0f;
+    for (int k = -4; k <= 4; ++k) {
+        const float turn = dir * 2.0f * XR_PI_F * (float)k;
+        den += hw_window_quality(__fadd_rn(beta, turn), bs, be, gamma, gmax);
+        const float bcj = __fadd_rn(__fadd_rn(beta, __fmul_rn(dir, __fadd_rn(XR_PI_F, 2.0f * gamma))), turn);
+        den += hw_window_quality(bcj, bs, be, -gamma, gmax);
+    }
+    return __fdiv_rn(q, fmaxf(den, 1.0e-6f));
+}
+
+// Redundancy weight of one (voxel, view) pair, helical_arc3d.cu:243-303.
+__device__ __forceinline__ float hw_weight(const HelOpts& o, const Geom& g, float px, float py, float pz, float beta,
+                                          float gamma, float src_z, float ray_xy, float bc, float bs, float be,
+                                          float db, float gmax, const float* __restrict__ ang,
+                                          const float* __restrict__ zsrc, int nview) {
+    if (o.weight_mode == 0) return hw_conjugate(beta, gamma, bc, bs, be, db, gmax);
+    const float span = fabsf(be - bs);
+    const float dir = (beta < bc) ? 1.0f : -1.0f;
+    const float bcj = __fadd_rn(beta, __fmul_rn(dir, __fadd_rn(XR_PI_F, 2.0f * gamma)));
+    float dq, cq;
+    if (span < __fsub_rn(2.0f * XR_PI_F, 2.0f * fabsf(db))) {
+        dq = hw_window_quality(beta, bs, be, gamma, gmax);
+        cq = hw_window_quality(bcj, bs, be, -gamma, gmax);
+    } else {
+        dq = hw_edge_taper(beta, bc, bs, be, db);
+        cq = hw_edge_taper(bcj, bc, bs, be, db);
+    }
+    if (dq <= 0.0f) return 0.0f;
+    if (cq <= 0.0f) return 1.0f;
+    const float zc = hw_source_z_at(bcj, ang, zsrc, nview);
+    const float SOD = (float)g.sod;
+    const float sxc = -sinf(bcj) * SOD, syc = cosf(bcj) * SOD;
+    const float rxc = px - sxc, ryc = py - syc;
+    const float rxyc = sqrtf(rxc * rxc + ryc * ryc);
+    const float ta = __fdiv_rn(fabsf(pz - src_z), fmaxf(ray_xy, 1.0e-6f));
+    const float tac = __fdiv_rn(fabsf(pz - zc), fmaxf(rxyc, 1.0e-6f));
+    const float kk = fminf(fmaxf(o.tang_k, 0.0f), 32.0f);
+    const float gg = powf(fmaxf(ta, 1.0e-6f), kk);
+    const float ggc = powf(fmaxf(tac, 1.0e-6f), kk);
+    const float w2 = __fdiv_rn(dq, fmaxf(dq + cq, 1.0e-6f));
+    const float den = dq * ggc + cq * gg;
+    const float w3 = __fdiv_rn(dq * ggc, fmaxf(den, 1.0e-6f));
+    const float blend = hw_clamp_unit(o.tang_blend);
+    return (1.0f - blend) * w2 + blend * w3;
+}
+
+// Voxel centre in world coordinates, helical_arc3d.cu:1130-1132.
+__device__ __forceinline__ float hw_px(const Geom& g, int ix) {
+    return __fadd_rn(__fmul_rn(__fadd_rn(__fsub_rn((float)ix, __fdiv_rn((float)g.W, 2.0f)), 0.5f), (float)g.dx),
+                     (float)g.shx);
+}
+__device__ __forceinline__ float hw_py(const Geom& g, int iy) {
+    return __fadd_rn(__fmul_rn(__fsub_rn(__fsub_rn(__fmul_rn((float)g.H, 0.5f), (float)iy), 0.5f), (float)g.dy),
+                     (float)g.shy);
+}
+__device__ __forceinline__ float hw_pz(const Geom& g, int iz) {
+    return __fadd_rn(__fmul_rn(__fadd_rn(__fsub_rn((float)iz, __fdiv_rn((float)g.D, 2.0f)), 0.5f), (float)g.dz),
+                     (float)g.shz);
+}
+
+// Fan angle of the voxel centre in this view and the ray's length in xy
+// (helical_arc3d.cu:1161-1166).
+__device__ __forceinline__ void hw_ray(const HelWView& w, float px, float py, float& gamma, float& rxy,
+                                       float& rx, float& ry) {
+    rx = __fsub_rn(px, w.sx);
+    ry = __fsub_rn(py, w.sy);
+    rxy = sqrtf(__fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
+    const float xb = __fsub_rn(__fmul_rn(w.cosv, px), __fmul_rn(w.sinv, py));
+    const float yb = __fadd_rn(__fmul_rn(w.sinv, px), __fmul_rn(w.cosv, py));
+    gamma = atan2f(yb, __fsub_rn(w.sod, xb));
+}
+
+// Does the ray through the voxel centre hit the detector?
+// helical_arc3d.cu:305-336 (gamma and the xy ray length as hw_ray gives them).
+__device__ __forceinline__ bool hw_measured(const Geom& g, const HelWView& w, float gamma, float rxy, float pz) {
+    const float col = __fsub_rn(__fadd_rn(__fdiv_rn(__fsub_rn(gamma, w.shu), w.du), __fmul_rn((float)g.Nu, 0.5f)),
+                                0.5f);
+    if (col < -0.5f || col > __fsub_rn((float)g.Nu, 0.5f)) return false;
+    if (rxy <= 1.0e-6f) return false;
+    const float det_z = __fadd_rn(w.szv, __fdiv_rn(__fmul_rn(w.sdd, __fsub_rn(pz, w.szv)), rxy));
+    const float row = __fsub_rn(__fadd_rn(__fdiv_rn(__fsub_rn(__fsub_rn(det_z, w.zs), (float)g.shv), (float)g.dv),
+                                          __fmul_rn((float)g.Nv, 0.5f)),
+                                0.5f);
+    return row >= -0.5f && row <= __fsub_rn((float)g.Nv, 0.5f);
+}
+
+// ------------------------------------------------------------ view windows
+
+// helical_arc3d.cu:141-210 and :121-139, one thread per z slice; thread 0
+// also writes the scan scalars.
+__global__ void hel_zwin_kernel(const Geom g, const HelOpts o, const float* __restrict__ ang,
+                                const float* __restrict__ zsrc, const int nview, HelZ* __restrict__ zw,
+                                HelScanF* __restrict__ scan) {
+    const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iz == 0) {
+        HelScanF sc;
+        sc.db = (nview > 1) ? __fdiv_rn(__fsub_rn(ang[nview - 1], ang[0]), (float)(nview - 1)) : 0.0f;
+        sc.gmax = __fmul_rn(__fmul_rn((float)g.du, (float)(g.Nu - 1)), 0.5f);
+        sc.cwW = __fmul_rn((float)g.sod, (float)g.du);
+        sc.pad = 0.0f;
+        *scan = sc;
+    }
+    if (iz >= g.D) return;
+    const float pz = hw_pz(g, iz);
+    int vs = 0, ve = 0;
+    if (nview > 1) {
+        const float a0 = ang[0], a1 = ang[nview - 1], z0 = zsrc[0], z1 = zsrc[nview - 1];
+        const float range = __fsub_rn(a1, a0);
+        if (fabsf(range) < 1.0e-6f) {
+            ve = nview - 1;
+        } else {
+            const float db = __fdiv_rn(range, fmaxf(1.0f, (float)(nview - 1)));
+            const float dzdb = __fdiv_rn(__fsub_rn(z1, z0), range);
+            if (fabsf(db) < 1.0e-8f || fabsf(dzdb) < 1.0e-8f) {
+                ve = nview - 1;
+            } else {
+                const float du = (float)g.du, dv = (float)g.dv, SOD = (float)g.sod, SDD = (float)g.sdd;
+                const float gmax = __fmul_rn(__fmul_rn(du, (float)(g.Nu - 1)), 0.5f);
+                const float half_scan = __fmul_rn(__fadd_rn(XR_PI_F, __fmul_rn(2.0f, gmax)),
+                                                  fmaxf(o.halfscan_coef, 1.0f));
+                float span = 2.0f * XR_PI_F;
+                if (o.view_mode == 1) span = half_scan;
+                else if (o.view_mode == 2) span = 2.0f * XR_PI_F;
+                else if (o.view_mode == 3) span = __fmul_rn(__fmul_rn(fmaxf(0.25f, o.view_turns), 2.0f), XR_PI_F);
+                else {
+                    const float ppt = __fmul_rn(__fmul_rn(fabsf(dzdb), 2.0f), XR_PI_F);
+                    const float iso_h = fmaxf(__fdiv_rn(__fmul_rn(__fmul_rn(dv, (float)g.Nv), SOD), SDD), dv);
+                    const float np = __fdiv_rn(ppt, fmaxf(iso_h, 1.0e-6f));
+                    if (np >= 1.25f) span = half_scan;
+                    else if (np >= 0.45f) span = 2.0f * XR_PI_F;
+                    else if (np >= 0.25f) span = 3.0f * XR_PI_F;
+                    else span = 5.0f * XR_PI_F;
+                }
+                // A window of V or more views is all views, and a centre
+                // beyond +-4V gives the same clamped window as +-4V: both
+                // bounds keep the integer arithmetic below in range.
+                const float nwf = ceilf(__fdiv_rn(span, fabsf(db)));
+                const int nwin = (nwf >= (float)nview) ? nview : (nwf < 1.0f ? 1 : (int)nwf);
+                const float bc = __fadd_rn(a0, __fdiv_rn(__fsub_rn(pz, z0), dzdb));
+                const float vcf = roundf(__fdiv_rn(__fsub_rn(bc, a0), db));
+                const int vc = (int)fminf(fmaxf(vcf, -4.0f * (float)nview), 4.0f * (float)nview);
+                vs = max(0, vc - nwin / 2);
+                ve = min(nview - 1, vs + nwin - 1);
+                vs = max(0, ve - nwin + 1);
+            }
+        }
+    }
+    HelZ z;
+    z.vs = vs;
+    z.ve = ve;
+    z.bs = ang[vs];
+    z.be = ang[ve];
+    z.pz = pz;
+    // centre angle, helical_arc3d.cu:121-139
+    float bc;
+    if (nview <= 1) {
+        bc = 0.5f * (z.bs + z.be);
+    } else {
+        const float a0 = ang[0], a1 = ang[nview - 1], z0 = zsrc[0], z1 = zsrc[nview - 1];
+        const float range = __fsub_rn(a1, a0);
+        const float dzdb = (fabsf(range) > 1.0e-6f) ? __fdiv_rn(__fsub_rn(z1, z0), range) : 0.0f;
+        if (fabsf(dzdb) <= 1.0e-8f) {
+            bc = 0.5f * (z.bs + z.be);
+        } else {
+            const float b = __fadd_rn(a0, __fdiv_rn(__fsub_rn(pz, z0), dzdb));
+            bc = fminf(fmaxf(b, fminf(z.bs, z.be)), fmaxf(z.bs, z.be));
+        }
+    }
+    z.bc = bc;
+    zw[iz] = z;
+}
+
+// Per-voxel normalisation (helical_arc3d.cu:1141-1180), one thread per voxel.
+__global__ void __launch_bounds__(256)
+hel_scale_kernel(const Geom g, const HelOpts o, const HelScanF* __restrict__ scan, const HelWView* __restrict__ wv,
+                 const HelZ* __restrict__ zw, const float* __restrict__ ang, const float* __restrict__ zsrc,
+                 const int nview, float* __restrict__ scale) {
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int iz = blockIdx.z;
+    if (ix >= g.W || iy >= g.H) return;
+    const HelScanF s = *scan;
+    const HelZ z = zw[iz];
+    const float px = hw_px(g, ix), py = hw_py(g, iy), pz = z.pz;
+    float valid = 0.0f;
+    for (int v = z.vs; v <= z.ve; ++v) {
+        const HelWView w = wv[v];
+        float gamma, rxy, rx, ry;
+        hw_ray(w, px, py, gamma, rxy, rx, ry);
+        if (rxy <= 1.0e-6f) continue;
+        const float wt = hw_weight(o, g, px, py, pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db, s.gmax,
+                                   ang, zsrc, nview);
+        if (wt == 0.0f) continue;
+        if (hw_measured(g, w, gamma, rxy, pz)) valid += wt;
+    }
+    const float ideal = (fabsf(s.db) > 1.0e-8f) ? __fdiv_rn(XR_PI_F, fabsf(s.db)) : valid;
+    float sc = __fdiv_rn(ideal, fmaxf(valid, 1.0e-6f));
+    sc = fminf(32.0f, fmaxf(0.03125f, sc));
+    scale[((size_t)iz * g.H + iy) * g.W + ix] = sc;
+}
+
+// ---------------------------------------------------------------------- Bw
+
+// Voxel gather of the weighted backprojection.  CTA = 32 x NWY pixels of the
+// image plane times a run of R z slices (the run's windows are CTA-uniform);
+// the view loop covers the union of the run's windows.  The z integral of a
+// (voxel, column) pair comes from the row prefix table of the view
+// (xr_vox_prefix.cuh) as in vox_prefix3d_kernel; every voxel of the run has
+// its own weight, and its normalisation is applied at the end.
+template <int R, int NWY>
+__global__ void __launch_bounds__(32 * NWY)
+hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts o, const HelScanF* __restrict__ scan,
+               const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ ang,
+               const float* __restrict__ zsrc, const float2* __restrict__ tab, const float* __restrict__ scale,
+               float* __restrict__ vol, const int nview, const int nzg, const double dvv) {
+    __shared__ HelZ szw[R];
+    __shared__ int sv[2];
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * NWY + threadIdx.y;
+    const int zg = blockIdx.z % nzg, b = blockIdx.z / nzg;
+    const int j0 = zg * R;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid < R) {
+        HelZ z;
+        if (j0 + tid < g.D) z = zw[j0 + tid];
+        else { z.vs = 1; z.ve = 0; z.bs = z.be = z.bc = z.pz = 0.0f; }
+        szw[tid] = z;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int lo = nview, hi = -1;
+        for (int i = 0; i < R; ++i)
+            if (szw[i].vs <= szw[i].ve) { lo = min(lo, szw[i].vs); hi = max(hi, szw[i].ve); }
+        sv[0] = lo;
+        sv[1] = hi;
+    }
+    __syncthreads();
+    if (ix >= g.W || iy >= g.H || j0 >= g.D) return;
+    const int Nu = g.Nu, Nv = g.Nv;
+    const size_t vstride = (size_t)(Nv + 2) * Nu;
+    const float2* __restrict__ tb = tab + (size_t)b * nview * vstride;
+    const float px = hw_px(g, ix), py = hw_py(g, iy);
+    const HelScanF s = *scan;
+    float acc[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = 0.0f;
+
+    for (int v = sv[0]; v <= sv[1]; ++v) {
+        const HelWView w = wv[v];
+        float gamma, rxy, rx, ry;
+        hw_ray(w, px, py, gamma, rxy, rx, ry);
+        if (rxy <= 1.0e-6f) continue;
+        float wt[R];
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const HelZ& z = szw[i];
+            float wi = 0.0f;
+            if (v >= z.vs && v <= z.ve)
+                wi = hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db, s.gmax, ang,
+                               zsrc, nview);
+            wt[i] = wi;
+            any |= (wi != 0.0f);
+        }
+        if (!any) continue;
+        const ViewHdr& h = vt.hdr[v];
+        const HelView hv = vt.hel[v];
+        const int keep = h.keep;
+        int L, p;
+        float xa, ya, xb, yb;
+        if (h.use_x) {
+            L = iy; p = ix;
+            ya = yb = gf.yc0 - (float)L * gf.dy;
+            xa = gf.x0 + (float)p * gf.dx;
+            xb = xa + gf.dx;
+        } else {
+            L = ix; p = g.H - 1 - iy;
+            xa = xb = gf.xc0 + (float)L * gf.dx;
+            ya = gf.y0 + (float)p * gf.dy;
+            yb = ya + gf.dy;
+        }
+        const double zs = (double)j0 + hv.z0dz;
+        const double zoffh = -hv.zd0 / dvv - 0.5;
+        const double q = fma(h.q1, (double)L, h.q0);
+        const double mvdv = 1.0 / (q * dvv);
+        // column width SOD du over the squared source distance
+        const float lf = __fdiv_rn(s.cwW, __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
+        const float margin = 0.5f + XR_GUESS_ATAN_ERR * hv.inv_du;
+        const float sf = (float)h.s, cf = (float)h.c;
+        const float kf0 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xa, ya, hv.inv_du);
+        const float kf1 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xb, yb, hv.inv_du);
+        const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
+        const int ka = max(0, (int)floorf(lo - margin));
+        const int kb = min(Nu - 1, (int)floorf(hi + margin));
+        if (ka > kb) continue;
+        const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
+        const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
+        const double* __restrict__ Rq = vt.colR + (size_t)v * Nu;
+        const float2* __restrict__ tv = tb + (size_t)v * vstride;
+        const double dp = (double)p, dL = (double)L;
+        int k = ka;
+        float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
+        float pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+        while (!(pk1 > 0.0f) && k < kb) {
+            ++k;
+            pkl = pk1;
+            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+        }
+        for (;;) {
+            const float wf = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
+            if (wf > 0.0f) {
+                const double ib = mvdv * Rq[k];  // detector rows per voxel
+                const double u0 = fma(zs, ib, zoffh);
+                if ((float)ib < 4096.0f && u0 < (double)Nv - 0.5 && u0 + R * ib > -0.5) {
+                    const double n0 = floor(u0 + 0.5);
+                    const int r0 = (int)n0;
+                    const float f0 = (float)(u0 - n0), fib = (float)ib;
+                    const int col = keep ? k : Nu - 1 - k;
+                    const float wk = __fdiv_rn(wf * lf, fib);
+                    const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
+                    float gprev = 0.0f;
+#pragma unroll
+                    for (int i = 0; i <= R; ++i) {
+                        // boundary i in rows relative to r0, clamped to the
+                        // table (rows -1 .. Nv of the detector: t in [0, Nv + 1])
+                        const float uc = fminf(fmaxf(fmaf((float)i, fib, f0), ulo), uhi);
+                        const float nf = rintf(uc);
+                        const int t = r0 + 1 + (int)nf;
+                        const float2 e = __ldg(tv + (size_t)t * Nu + col);
+                        const float gi = fmaf(uc - nf, e.y, e.x);
+                        if (i > 0) acc[i - 1] = fmaf(wk * wt[i - 1], gi - gprev, acc[i - 1]);
+                        gprev = gi;
+                    }
+                }
+            }
+            if (++k > kb) break;
+            pkl = pk1;
+            if (pkl >= 1.0f) break;
+            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int j = j0 + i;
+        if (j < g.D) {
+            const size_t oi = ((size_t)j * g.H + iy) * g.W + ix;
+            vol[(size_t)b * g.D * g.H * g.W + oi] = acc[i] * scale[oi];
+        }
+    }
+}
+
+// -------------------------------------------------------------------- Bw^T
+
+// img_s = img * scale (per voxel, every batch element).
+__global__ void hel_prescale_kernel(const float* __restrict__ img, const float* __restrict__ scale,
+                                    float* __restrict__ out, const size_t nvox, const size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = img[i] * scale[i % nvox];
+}
+
+// Cell gather of the weighted backprojection's transpose: thread = (view,
+// detector column in traversal order, run of R rows), as cell_gather3d_kernel;
+// every voxel of a column's footprint is weighted by its own redundancy
+// weight (its slice's window, the pixel's fan angle) and read from the
+// normalised image img_s.
+template <int R>
+__global__ void __launch_bounds__(256)
+hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelScanF* __restrict__ scan,
+                const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ ang,
+                const float* __restrict__ zsrc, const float* __restrict__ img_s, float* __restrict__ sino,
+                const int nview, const int view0, const double dvv) {
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int r0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
+    const int vb = blockIdx.z + view0;
+    const int v = vb % nview, b = vb / nview;
+    const int Nu = g.Nu;
+    if (k >= Nu || r0 >= g.Nv) return;
+    const ViewHdr h = vt.hdr[v];
+    const HelView hv = vt.hel[v];
+    const HelWView w = wv[v];
+    const HelScanF s = *scan;
+    const size_t ob = (size_t)v * (Nu + 1) + k;
+    const double bA0 = vt.bA[ob], bB0 = vt.bB[ob], bA1 = vt.bA[ob + 1], bB1 = vt.bB[ob + 1];
+    const double Qk = vt.colQ[(size_t)v * Nu + k];
+    const int nlines = h.nlines, npix = h.npix;
+    const size_t plane = (size_t)g.H * g.W;
+    const float* __restrict__ vol = img_s + (size_t)b * g.D * plane;
+    const double zr0 = hv.zd0 + r0 * dvv;
+    float acc[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = 0.0f;
+
+    for (int L = 0; L < nlines; ++L) {
+        const double pk = fma(bB0, (double)L, bA0);
+        const double pk1 = fma(bB1, (double)L, bA1);
+        const int pa = max((int)floor(pk), 0);
+        const int pb = min((int)ceil(pk1) - 1, npix - 1);
+        if (pa > pb) continue;
+        const double q = fma(h.q1, (double)L, h.q0);
+        const double gq = Qk * q;
+        const double t0 = fma(gq, zr0, -hv.z0dz);
+        const double bt = gq * dvv;
+        if (!(bt > 1.0e-4 && bt < 1.0e4)) continue;  // bounds every merge loop
+        if (t0 + R * bt <= 0.0 || t0 >= (double)g.D) continue;
+        const double jf = floor(t0);
+        const int j0 = (int)jf;
+        const float f = (float)(t0 - jf);
+        const float bf = (float)bt;
+        for (int p = pa; p <= pb; ++p) {
+            const float wxy = (float)(fmin((double)p + 1.0, pk1) - fmax((double)p, pk));
+            if (!(wxy > 0.0f)) continue;
+            int ix, iy;
+            if (h.use_x) { ix = p; iy = L; } else { ix = L; iy = g.H - 1 - p; }
+            const float px = hw_px(g, ix), py = hw_py(g, iy);
+            float gamma, rxy, rx, ry;
+            hw_ray(w, px, py, gamma, rxy, rx, ry);
+            if (rxy <= 1.0e-6f) continue;
+            const float lf = wxy * __fdiv_rn(s.cwW, __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
+            const float* __restrict__ col = vol + (size_t)iy * g.W + ix;
+            // value of voxel j of this column: weight x normalised image
+            auto value = [&](int j) -> float {
+                if ((unsigned)j >= (unsigned)g.D) return 0.0f;
+                const HelZ z = zw[j];
+                if (v < z.vs || v > z.ve) return 0.0f;
+                const float wt = hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db,
+                                           s.gmax, ang, zsrc, nview);
+                return wt == 0.0f ? 0.0f : wt * __ldg(col + (size_t)j * plane);
+            };
+            int j = j0;
+            float vj = value(j), pos = f, jn = 1.0f;
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const float top = fmaf(bf, (float)(i + 1), f);
+                float a = 0.0f;
+                while (jn < top) {
+                    a = fmaf(jn - pos, vj, a);
+                    pos = jn;
+                    ++j;
+                    jn += 1.0f;
+                    vj = value(j);
+                }
+                if (top > pos) { a = fmaf(top - pos, vj, a); pos = top; }
+                acc[i] = fmaf(lf, a, acc[i]);
+            }
+        }
+    }
+    const int colo = h.keep ? k : Nu - 1 - k;
+    float* out = sino + (((size_t)b * nview + v) * g.Nv) * Nu + colo;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int r = r0 + i;
+        if (r < g.Nv) out[(size_t)r * Nu] = acc[i];
+    }
+}
+
+}  // namespace xr

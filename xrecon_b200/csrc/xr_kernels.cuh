@@ -152,12 +152,12 @@ __global__ void pad_rows_kernel(const T* __restrict__ in, T* __restrict__ out, i
 // detector rows.  Each thread sweeps the image lines; per line it forms the
 // pixel band of its column (FP64 boundaries, FP32 weights) and merges the
 // z voxels of the band against its R rows in local coordinates.
-template <typename TI, typename TO, int R, int MODE>
+template <typename TI, typename TO, int R, int MODE, bool HEL = false>
 __global__ void __launch_bounds__(256, 3)
 cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ vol_rows,
                      const TI* __restrict__ vol_cols, TO* __restrict__ sino, const int nview,
-                     const int view0, const double z0dz, const double zd0, const double dvv,
-                     const float cw) {
+                     const int view0, const double z0dz_p, const double zd0_p, const double dvv,
+                     const float cw_p) {
     const int k = blockIdx.x * 32 + threadIdx.x;
     const int r0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
     const int vb = blockIdx.z + view0;
@@ -165,6 +165,10 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
     const int Nu = g.Nu;
     if (k >= Nu || r0 >= g.Nv) return;
     const ViewHdr h = vt.hdr[v];
+    // helical scans: the view's own z placement and column width
+    const double z0dz = HEL ? vt.hel[v].z0dz : z0dz_p;
+    const double zd0 = HEL ? vt.hel[v].zd0 : zd0_p;
+    const float cw = HEL ? vt.hel[v].cw : cw_p;
     const size_t ob = (size_t)v * (Nu + 1) + k;
     const double bA0 = vt.bA[ob], bB0 = vt.bB[ob], bA1 = vt.bA[ob + 1], bB1 = vt.bB[ob + 1];
     const double Qk = vt.colQ[(size_t)v * Nu + k];
@@ -269,7 +273,8 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
         if (r < g.Nv) {
             float s = acc[i];
             if (MODE == OP_A) {
-                const float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+                float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+                if (HEL) zc += vt.hel[v].zsrc;  // helical: the row's absolute z
                 s *= E * sqrtf(F + zc * zc);
             }
             st(out + (size_t)r * Nu, s);

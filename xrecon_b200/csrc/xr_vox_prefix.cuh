@@ -32,10 +32,10 @@ namespace xr {
 // One thread per (batch element x view, physical column).  MODE OP_AT with a
 // cone geometry folds the projection's cell scale s_A(k, r) into y, as
 // prescale_at3d_kernel does.
-template <typename TI, bool PRESCALE>
+template <typename TI, bool PRESCALE, bool HEL = false>
 __global__ void __launch_bounds__(128)
 row_prefix3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ in, float2* __restrict__ tab,
-                    const int nview, const int nbv, const double zd0, const double dvv) {
+                    const int nview, const int nbv, const double zd0_p, const double dvv) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int Nu = g.Nu, Nv = g.Nv;
     if (c >= Nu) return;
@@ -44,15 +44,19 @@ row_prefix3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ in
         const TI* __restrict__ src = in + (size_t)bv * Nv * Nu + c;
         float2* __restrict__ dst = tab + (size_t)bv * (Nv + 2) * Nu + c;
         float E = 1.0f, F = 0.0f, M = 0.0f;
+        double zd0 = zd0_p;
+        float zsrc = 0.0f;
         if (PRESCALE) {
             const int k = vt.hdr[v].keep ? c : Nu - 1 - c;
             const size_t oc = (size_t)v * Nu + k;
             E = vt.colE[oc]; F = vt.colF[oc]; M = vt.colM[oc];
+            if (HEL) { zd0 = vt.hel[v].zd0; zsrc = vt.hel[v].zsrc; }
         }
         auto value = [&](int r) -> float {
             const float y = ld(src + (size_t)r * Nu);
             if (!PRESCALE) return y;
-            const float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+            float zc = (float)(zd0 + (r + 0.5) * dvv) * M;
+            if (HEL) zc += zsrc;  // helical: the row's absolute z
             return y * E * sqrtf(F + zc * zc);
         };
         double half = 0.0;
@@ -73,17 +77,17 @@ row_prefix3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ in
 // overlaps themselves come from the FP64 boundary tables.  (dcx, dcy) is the
 // arc detector's central direction for this view.
 __device__ __forceinline__ float col_guess_fast(const GeomF& gf, const ViewHdr& h, float s, float c, float dcx,
-                                                float dcy, float x, float y) {
+                                                float dcy, float x, float y, float inv_du) {
     float sg;
     if (gf.type == GEO_FLAT) {
         const float R = gf.sod;
         const float u = __fdividef(R * (x * c + y * s), R + x * s - y * c);
-        sg = (u * gf.inv_uscale - gf.shu) * gf.inv_du;
+        sg = (u * gf.inv_uscale - gf.shu) * inv_du;
     } else if (gf.type == GEO_ARC) {
         const float ex = x - (float)h.sx, ey = y - (float)h.sy;
-        sg = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * gf.inv_du;
+        sg = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
     } else {
-        sg = (x * c + y * s - gf.shu) * gf.inv_du;
+        sg = (x * c + y * s - gf.shu) * inv_du;
     }
     return h.keep ? sg + 0.5f * gf.Nu : 0.5f * gf.Nu - sg;
 }
@@ -100,7 +104,9 @@ __device__ __forceinline__ float col_guess_fast(const GeomF& gf, const ViewHdr& 
 #ifndef XR_PFX_MINB
 #define XR_PFX_MINB 4
 #endif
-template <typename TO, int R, int NWY, int MODE>
+//   HEL        : helical scan; the view's z placement, column width and
+//                angular column pitch come from vt.hel
+template <typename TO, int R, int NWY, int MODE, bool HEL = false>
 __global__ void __launch_bounds__(32 * NWY, XR_PFX_MINB)
 vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const float2* __restrict__ tab,
                     TO* __restrict__ vol, const int nview, const int nzg, const double z0dz, const double zd0,
@@ -114,11 +120,12 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
     const unsigned Nu8 = (unsigned)Nu * 8u;
     const size_t vstride = (size_t)(Nv + 2) * Nu;
     const float2* __restrict__ tb = tab + (size_t)b * nview * vstride;
-    const double zs = (double)j0 + z0dz;  // run bottom, in voxel units from z = 0
-    const double zoffh = -zd0 / dvv - 0.5;  // u0 = zs * (rows per voxel) + zoffh
+    double zs = (double)j0 + z0dz;  // run bottom, in voxel units from z = 0
+    double zoffh = -zd0 / dvv - 0.5;  // u0 = zs * (rows per voxel) + zoffh
     const float dpdz = (float)g.dz;
     // column bracket margin: half a column, plus the arc guess's angle error
-    const float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * gf.inv_du : 0.0f);
+    float inv_du = gf.inv_du;
+    float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * inv_du : 0.0f);
     float acc[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) acc[i] = 0.0f;
@@ -126,6 +133,15 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
     for (int v = 0; v < nview; ++v) {
         const ViewHdr& h = vt.hdr[v];
         const int keep = h.keep;
+        float cwv = cw;
+        if (HEL) {
+            const HelView hv = vt.hel[v];
+            zs = (double)j0 + hv.z0dz;
+            zoffh = -hv.zd0 / dvv - 0.5;
+            cwv = hv.cw;
+            inv_du = hv.inv_du;
+            margin = 0.5f + XR_GUESS_ATAN_ERR * inv_du;
+        }
         int L, p;
         float xa, ya, xb, yb, px, py;
         if (h.use_x) {
@@ -148,14 +164,14 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             if (g.type == GEO_PARALLEL) lf = atconst;
             else { const float qf = (float)q; lf = (float)h.dpix * dpdz / (qf * qf); }
         } else {
-            lf = cw;
+            lf = cwv;
             if (MODE == OP_BW) lf *= fbp_weight(g, h, px, py);
         }
         lf *= oscale;
         const float sf = (float)h.s, cf = (float)h.c;
         const float dcx = h.dcx, dcy = h.dcy;
-        const float kf0 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xa, ya);
-        const float kf1 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xb, yb);
+        const float kf0 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xa, ya, inv_du);
+        const float kf1 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xb, yb, inv_du);
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const int ka = max(0, (int)floorf(lo - margin));

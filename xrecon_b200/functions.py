@@ -57,6 +57,39 @@ WeightedBackProjectionTranspose3d = _make("WeightedBackProjectionTranspose3d",
                                           _B.weighted_backward_projection3d)
 
 
+def _make_helical(name: str, fwd, bwd):
+    """Helical Functions (functions.py:305-388 of the reference): the same
+    pairing, with ``source_pos`` [4, V] as a fourth, non-differentiable input."""
+    def forward(ctx, input, option, angles, source_pos):
+        out = fwd(_c(input), option, angles, source_pos)
+        ctx.option = option
+        ctx.save_for_backward(angles, source_pos)
+        return out
+
+    def backward(ctx, grad_output):
+        angles, source_pos = ctx.saved_tensors
+        return bwd(_c(grad_output), ctx.option, angles, source_pos), None, None, None
+
+    return type(name, (Function,), {"forward": staticmethod(forward), "backward": staticmethod(backward)})
+
+
+ProjectionHelical3d = _make_helical("ProjectionHelical3d", _B.forward_projection_helical3d,
+                                    _B.projection_transpose_helical3d)
+ProjectionTransposeHelical3d = _make_helical("ProjectionTransposeHelical3d", _B.projection_transpose_helical3d,
+                                             _B.forward_projection_helical3d)
+BackProjectionHelical3d = _make_helical("BackProjectionHelical3d", _B.backward_projection_helical3d,
+                                        _B.backward_projection_transpose_helical3d)
+BackProjectionTransposeHelical3d = _make_helical("BackProjectionTransposeHelical3d",
+                                                 _B.backward_projection_transpose_helical3d,
+                                                 _B.backward_projection_helical3d)
+WeightedBackProjectionHelical3d = _make_helical("WeightedBackProjectionHelical3d",
+                                                _B.weighted_backward_projection_helical3d,
+                                                _B.weighted_backward_projection_transpose_helical3d)
+WeightedBackProjectionTransposeHelical3d = _make_helical("WeightedBackProjectionTransposeHelical3d",
+                                                         _B.weighted_backward_projection_transpose_helical3d,
+                                                         _B.weighted_backward_projection_helical3d)
+
+
 class ProjectionLeastSquares(Function):
     """``0.5 * ||A x - y||^2`` summed over the batch, with A the projection
     (2D or 3D by the rank of ``x``), evaluated over chunks of views.

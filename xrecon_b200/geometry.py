@@ -226,8 +226,9 @@ class ParallelBeam3d:
 
 @dataclass(frozen=True, init=False)
 class HelicalConeBeam3d(ConeBeam3d):
-    """Helical trajectory description (accepted for API compatibility; the
-    helical projector is outside this library's scope)."""
+    """Helical trajectory: cone-beam geometry plus the source's rise per turn
+    (``pitch``) and its z at the first view (``z0``), as the reference's
+    geometry.py:233-248; used by :class:`~xrecon_b200.HelicalProjector3d`."""
     pitch: float
     z0: float
 

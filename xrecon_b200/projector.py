@@ -23,15 +23,18 @@ from torch import Tensor
 from . import _native
 from .backend import HostGeometry
 from .filters import filter_generate
+from .backend import HelicalHostGeometry
 from .functions import (
-    BackProjection2d, BackProjection3d, BackProjectionTranspose2d, BackProjectionTranspose3d,
-    Projection2d, Projection3d, ProjectionTranspose2d, ProjectionTranspose3d,
-    WeightedBackProjection2d, WeightedBackProjection3d, WeightedBackProjectionTranspose2d,
-    WeightedBackProjectionTranspose3d,
+    BackProjection2d, BackProjection3d, BackProjectionHelical3d, BackProjectionTranspose2d,
+    BackProjectionTranspose3d, BackProjectionTransposeHelical3d, Projection2d, Projection3d,
+    ProjectionHelical3d, ProjectionTranspose2d, ProjectionTranspose3d, ProjectionTransposeHelical3d,
+    WeightedBackProjection2d, WeightedBackProjection3d, WeightedBackProjectionHelical3d,
+    WeightedBackProjectionTranspose2d, WeightedBackProjectionTranspose3d,
+    WeightedBackProjectionTransposeHelical3d,
 )
 from .geometry import (
-    ConeBeam3d, FanBeam2d, ParallelBeam2d, ParallelBeam3d, Volume2d, Volume3d, make_geometry2d,
-    make_geometry3d, pack_options2d, pack_options3d,
+    ConeBeam3d, Detector3d, FanBeam2d, HelicalConeBeam3d, ParallelBeam2d, ParallelBeam3d, Volume2d, Volume3d,
+    make_geometry2d, make_geometry3d, pack_options2d, pack_options3d,
 )
 
 _SCAN_ALIASES = {"para": "parallel", "parallel": "parallel", "flat": "flat", "arc": "arc"}
@@ -490,6 +493,247 @@ class Projector3d(_ProjectorBase):
         Nu, Nv = self.num_det
         if sino.shape[2] != angles.numel() or sino.shape[3] != Nv or sino.shape[4] != Nu:
             raise ValueError(f"Expected sino shape [B, C, {angles.numel()}, {Nv}, {Nu}], got {tuple(sino.shape)}")
+
+
+class HelicalProjector3d(nn.Module):
+    """Distance-driven helical cone-beam projector, arc detector
+    (xrecon/projector/projector3d.py:289-576 of the reference).
+
+    Shapes: image [B, C, D, H, W], angles [V], sino [B, C, V, Nv, Nu],
+    source_pos [4, V] = (source_z, shift_radius, shift_angle, shift_z); when
+    ``source_pos`` is omitted the source rises by ``pitch`` per turn from
+    ``z0`` (:meth:`source_position`).  Operators run in float32, as in the
+    reference.
+    """
+
+    _VIEW_MODES = {"auto": 0, "half": 1, "halfscan": 1, "half_scan": 1, "short": 1, "short_scan": 1,
+                   "one": 2, "one_turn": 2, "1turn": 2, "full": 2, "full_scan": 2,
+                   "fixed": 3, "turns": 3, "multi": 3, "multi_turn": 3}
+    _WEIGHT_MODES = {"legacy": 0, "2d": 0, "redundancy": 0, "tang": 1, "tang3d": 1, "3d": 1, "cone": 1}
+
+    def __init__(self, image_size, num_det=None, pix_size=None, det_size=None, iso_source: float = 0.0,
+                 source_detector: float = 0.0, pixshift=0.0, binshift=0.0, scan_type: str = "arc",
+                 pitch: float = 0.0, z0: float = 0.0, helical_view_mode: str = "one_turn",
+                 helical_view_turns: float = 0.0, helical_halfscan_coef: float = 1.0,
+                 helical_weight_mode: str = "2d", helical_tang_k: float = 5.0, helical_tang_blend: float = 0.0,
+                 filter_type: str = "ramp", trainable: bool = False, dtype=None) -> None:
+        super().__init__()
+        if isinstance(image_size, Volume3d):
+            volume = image_size
+            if isinstance(num_det, HelicalConeBeam3d) and pix_size is None:
+                pix_size = num_det
+            if not isinstance(pix_size, HelicalConeBeam3d):
+                raise TypeError("When image_size is Volume3d, pix_size should be a HelicalConeBeam3d object")
+            geometry = pix_size
+        else:
+            if num_det is None or pix_size is None or det_size is None:
+                raise TypeError("num_det, pix_size and det_size are required with the legacy constructor")
+            volume = Volume3d(image_size, pix_size, pixshift)
+            geometry = HelicalConeBeam3d(Detector3d(num_det, det_size, binshift), iso_source, source_detector,
+                                         scan_type, pitch=pitch, z0=z0)
+        scan = geometry.scan_type.lower().strip()
+        if scan != "arc":
+            raise NotImplementedError(
+                "Direct helical projection/backprojection currently supports arc detector geometry only")
+        W, H, D = volume.size
+        dx, dy, dz = volume.spacing
+        shx, shy, shz = volume.shift
+        Nu, Nv = geometry.detector.count
+        du, dv = geometry.effective_det_spacing
+        shu, shv = geometry.effective_det_shift
+        self.volume = volume
+        self.geometry = geometry
+        self.image_size = (W, H, D)
+        self.pix_size = (dx, dy, dz)
+        self.num_det = (Nu, Nv)
+        self.det_size = (du, dv)
+        self.binshift = (shu, shv)
+        self.pixshift = (shx * dx, shy * dy, shz * dz)
+        self.scan_type = scan
+        self.filter_type = filter_type.lower().strip()
+        self.iso_source = float(geometry.iso_source)
+        self.source_detector = float(geometry.source_detector)
+        self.pitch = float(geometry.pitch)
+        self.z0 = float(geometry.z0)
+        self.helical_view_mode = self._view_mode_id(helical_view_mode)
+        self.helical_weight_mode = self._weight_mode_id(helical_weight_mode)
+        self.helical_view_turns = float(helical_view_turns)
+        self.helical_halfscan_coef = float(helical_halfscan_coef)
+        self.helical_tang_k = float(helical_tang_k)
+        self.helical_tang_blend = float(helical_tang_blend)
+        self._default_dtype = dtype or torch.float32
+        packed = [W, H, D, Nu, Nv, dx, dy, dz, du, dv, self.iso_source, self.source_detector,
+                  self.pixshift[0], self.pixshift[1], self.pixshift[2], shu, shv, geometry.scan_id,
+                  self.helical_view_mode, self.helical_weight_mode, self.helical_view_turns,
+                  self.helical_halfscan_coef, self.helical_tang_k, self.helical_tang_blend]
+        self._host_geom = HelicalHostGeometry(packed)
+        self.register_buffer("options", torch.tensor(packed, dtype=self._default_dtype), persistent=False)
+        w = self._make_weight(dtype=self._default_dtype)
+        if trainable:
+            self.weight = nn.Parameter(w.clone())
+        else:
+            self.register_buffer("weight", w, persistent=False)
+        f = self._filter_generate(filter_type=self.filter_type, dtype=self._default_dtype)
+        if trainable:
+            self.filter = nn.Parameter(f.clone())
+        else:
+            self.register_buffer("filter", f, persistent=False)
+
+    def forward(self, image: Tensor, angles: Tensor, source_pos: Optional[Tensor] = None) -> Tensor:
+        return self.projection(image, angles, source_pos)
+
+    def source_position(self, angles: Tensor, ref: Optional[Tensor] = None) -> Tensor:
+        """[4, V]: source z = z0 + pitch (beta - beta_0) / (2 pi), no shifts
+        (projector3d.py:410-419)."""
+        ref = angles if ref is None else ref
+        angles = self._prepare_angles(angles, ref)
+        if angles.numel() == 0:
+            return angles.new_zeros((4, 0))
+        source_z = self.z0 + self.pitch * (angles - angles[0]) / (2.0 * math.pi)
+        shifts = angles.new_zeros((3, angles.numel()))
+        return torch.cat((source_z.view(1, -1), shifts), dim=0).contiguous()
+
+    def projection(self, image: Tensor, angles: Tensor, source_pos: Optional[Tensor] = None) -> Tensor:
+        self._check_image(image)
+        angles = self._prepare_angles(angles, image)
+        sp = self._prepare_source_pos(source_pos, angles, image)
+        return ProjectionHelical3d.apply(image, self._host_geom, angles, sp)
+
+    def projection_t(self, sino: Tensor, angles: Tensor, source_pos: Optional[Tensor] = None) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        angles = self._prepare_angles(angles, sino)
+        sp = self._prepare_source_pos(source_pos, angles, sino)
+        return ProjectionTransposeHelical3d.apply(sino, self._host_geom, angles, sp)
+
+    def backprojection(self, sino: Tensor, angles: Tensor, source_pos: Optional[Tensor] = None) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        angles = self._prepare_angles(angles, sino)
+        sp = self._prepare_source_pos(source_pos, angles, sino)
+        return BackProjectionHelical3d.apply(sino, self._host_geom, angles, sp)
+
+    def backprojection_weighted(self, sino: Tensor, angles: Tensor, source_pos: Optional[Tensor] = None) -> Tensor:
+        self._check_sino_angles(sino, angles)
+        angles = self._prepare_angles(angles, sino)
+        sp = self._prepare_source_pos(source_pos, angles, sino)
+        return WeightedBackProjectionHelical3d.apply(sino, self._host_geom, angles, sp)
+
+    def backprojection_t(self, image: Tensor, angles: Tensor, source_pos: Optional[Tensor] = None) -> Tensor:
+        self._check_image(image)
+        angles = self._prepare_angles(angles, image)
+        sp = self._prepare_source_pos(source_pos, angles, image)
+        return BackProjectionTransposeHelical3d.apply(image, self._host_geom, angles, sp)
+
+    def backprojection_weighted_t(self, image: Tensor, angles: Tensor,
+                                  source_pos: Optional[Tensor] = None) -> Tensor:
+        self._check_image(image)
+        angles = self._prepare_angles(angles, image)
+        sp = self._prepare_source_pos(source_pos, angles, image)
+        return WeightedBackProjectionTransposeHelical3d.apply(image, self._host_geom, angles, sp)
+
+    projection_transpose = projection_t
+    backprojection_transpose = backprojection_t
+    weighted_backprojection_transpose = backprojection_weighted_t
+    backprojection_w = backprojection_weighted
+
+    def filtered_backprojection(self, sino: Tensor, angles: Tensor, source_pos: Optional[Tensor] = None,
+                                filter: Optional[Tensor] = None, filter_type: Optional[str] = None) -> Tensor:
+        """Helical FDK (projector3d.py:465-481): cell weight [Nv, Nu], u-filter,
+        weighted backprojection, x mean angle step (no redundancy halving)."""
+        self._check_sino_angles(sino, angles)
+        angles = self._prepare_angles(angles, sino)
+        sp = self._prepare_source_pos(source_pos, angles, sino)
+        if filter is not None:
+            filt = filter
+        elif filter_type is None or filter_type.lower() == self.filter_type:
+            filt = self.filter
+        else:
+            filt = self._filter_generate(filter_type.lower(), dtype=sino.dtype).to(sino.device)
+        Nu, Nv = self.num_det
+        V = angles.numel()
+        wt = self.weight
+        needs_grad = torch.is_grad_enabled() and (
+            sino.requires_grad or (isinstance(filt, Tensor) and filt.requires_grad) or wt.requires_grad)
+        scale = mean_angle_step(angles)
+        if needs_grad:
+            sw = sino * wt.to(device=sino.device, dtype=sino.dtype)
+            ones = torch.ones(Nu, device=sino.device, dtype=torch.float32)
+            filtered = _FilterRows.apply(sw.to(torch.float32), ones, filt, None, V, Nv)
+            recon = self.backprojection_weighted(filtered.contiguous(), angles, sp)
+            return recon * scale.to(device=recon.device, dtype=recon.dtype)
+        with torch.no_grad():
+            s = sino if sino.is_contiguous() else sino.contiguous()
+            # the [Nv, Nu] cell weight enters as the per-row weight of the
+            # fused filter (one "view" per detector row)
+            filtered = _native.fbp_filter(s, nview=Nv, rows_per_view=1, cosw=None,
+                                          filt=filt.detach().reshape(-1),
+                                          parker=wt.detach().reshape(Nv, Nu))
+            recon = self.backprojection_weighted(filtered, angles, sp)
+            return recon * scale.to(device=recon.device, dtype=recon.dtype)
+
+    helical_fdk = filtered_backprojection
+
+    @classmethod
+    def _view_mode_id(cls, mode: str) -> int:
+        key = str(mode).lower().strip()
+        if key not in cls._VIEW_MODES:
+            raise ValueError(f"Unsupported helical_view_mode: {mode}")
+        return cls._VIEW_MODES[key]
+
+    @classmethod
+    def _weight_mode_id(cls, mode: str) -> int:
+        key = str(mode).lower().strip()
+        if key not in cls._WEIGHT_MODES:
+            raise ValueError(f"Unsupported helical_weight_mode: {mode}")
+        return cls._WEIGHT_MODES[key]
+
+    def _filter_generate(self, filter_type: str, dtype=None) -> Tensor:
+        return filter_generate(self.num_det[0], self.det_size[0], filter_type, dtype)[None, None, None, None, :]
+
+    def _make_weight(self, dtype=None) -> Tensor:
+        """SOD / |ray| of every cell (projector3d.py:535-545)."""
+        dtype = dtype or torch.float32
+        Nu, Nv = self.num_det
+        du, dv = self.det_size
+        shu, shv = self.binshift
+        u = torch.arange(-Nu / 2 + 0.5, Nu / 2, 1.0, dtype=dtype) * du + shu
+        v = torch.arange(-Nv / 2 + 0.5, Nv / 2, 1.0, dtype=dtype) * dv + shv
+        col = torch.tan(u) * self.iso_source
+        row = v * self.iso_source / self.source_detector
+        w = self.iso_source / torch.sqrt(row[:, None].pow(2) + col[None, :].pow(2)
+                                         + self.iso_source * self.iso_source)
+        return w.view(1, 1, 1, Nv, Nu)
+
+    def _check_image(self, image: Tensor) -> None:
+        if image.ndim != 5:
+            raise ValueError(f"Expected image shape [B, C, D, H, W], got {tuple(image.shape)}")
+        W, H, D = self.image_size
+        if tuple(image.shape[2:]) != (D, H, W):
+            raise ValueError(f"Expected image shape [B, C, {D}, {H}, {W}], got {tuple(image.shape)}")
+
+    def _check_sino_angles(self, sino: Tensor, angles: Tensor) -> None:
+        if sino.ndim != 5:
+            raise ValueError(f"Expected sino shape [B, C, V, Nv, Nu], got {tuple(sino.shape)}")
+        if angles.ndim != 1:
+            raise ValueError(f"Expected angles shape [V], got {tuple(angles.shape)}")
+        Nu, Nv = self.num_det
+        if sino.shape[2] != angles.numel() or sino.shape[3] != Nv or sino.shape[4] != Nu:
+            raise ValueError(f"Expected sino shape [B, C, {angles.numel()}, {Nv}, {Nu}], got {tuple(sino.shape)}")
+
+    def _prepare_source_pos(self, source_pos: Optional[Tensor], angles: Tensor, ref: Tensor) -> Tensor:
+        if source_pos is None:
+            return self.source_position(angles, ref)
+        source_pos = source_pos.to(device=ref.device, dtype=ref.dtype).contiguous()
+        if source_pos.shape != (4, angles.numel()):
+            raise ValueError(f"Expected source_pos shape [4, {angles.numel()}], got {tuple(source_pos.shape)}")
+        return source_pos
+
+    @staticmethod
+    def _prepare_angles(angles: Tensor, ref: Tensor) -> Tensor:
+        return angles.to(device=ref.device, dtype=ref.dtype).contiguous()
+
+    @staticmethod
+    def _mean_angle_step(angles: Tensor) -> Tensor:
+        return mean_angle_step(angles)
 
 
 projector2d = Projector2d
