@@ -302,6 +302,63 @@ def rebin_measure(P, vol, ang, reps: int = 3):
             "samples": WL["V"] * WL["Nv"] * WL["Nu"]}
 
 
+HEL = dict(W=512, H=512, D=128, dx=0.7, dz=0.8, Nu=736, Nv=64, du=1.2858, dv=1.0947, sod=595.0, sdd=1085.6,
+           views_per_turn=1152, turns=5, pitch=30.7)
+
+
+def helical_projector(dev):
+    """Helical scan of a 512 x 512 x 128 volume (0.7 x 0.7 x 0.8 mm) on a
+    736 x 64 arc detector (1.2858 x 1.0947 mm cells at SDD 1085.6 mm, SOD
+    595 mm), 1152 views per turn over 5 turns, 30.7 mm rise per turn
+    (pitch 0.8 of the 38.4 mm collimation), one-turn view windows."""
+    from xrecon_b200 import HelicalProjector3d
+    h = HEL
+    z_span = h["turns"] * h["pitch"]
+    P = HelicalProjector3d((h["W"], h["H"], h["D"]), (h["Nu"], h["Nv"]), (h["dx"], h["dx"], h["dz"]),
+                           (h["du"], h["dv"]), h["sod"], h["sdd"], pitch=h["pitch"], z0=-0.5 * z_span).to(dev)
+    V = h["views_per_turn"] * h["turns"]
+    import numpy as np
+    import torch
+    ang = torch.from_numpy((np.arange(V) * (2 * np.pi / h["views_per_turn"])).astype(np.float32)).to(dev)
+    return P, ang
+
+
+def helical_measure(dev, reps: int = 2):
+    """Per-operator device times of the helical projector (HEL workload);
+    throughput in voxel-views per second counts each voxel against the views
+    of one turn (the views whose source z is near the voxel's)."""
+    import torch
+    P, ang = helical_projector(dev)
+    h = HEL
+    g = torch.Generator(device=dev).manual_seed(3)
+    vol = torch.rand((1, 1, h["D"], h["H"], h["W"]), device=dev, generator=g)
+    sino = P.projection(vol, ang)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    with torch.no_grad():
+        out["A_ms"] = timed(lambda: P.projection(vol, ang))
+        out["B_ms"] = timed(lambda: P.backprojection(sino, ang))
+        out["Bw_ms"] = timed(lambda: P.backprojection_weighted(sino, ang))
+        out["fdk_ms"] = timed(lambda: P.filtered_backprojection(sino, ang))
+    nvox = h["W"] * h["H"] * h["D"]
+    out["gvoxel_views_per_turn_per_s_fdk"] = nvox * h["views_per_turn"] / (out["fdk_ms"] / 1e3) / 1e9
+    out["views"] = int(ang.numel())
+    del sino, vol
+    torch.cuda.empty_cache()
+    return out
+
+
 def ragged_measure(dev, reps: int = 5):
     """The 64-instance ragged fan-arc batch: projection + FBP of every
     instance as one autotuned persistent launch replayed from a CUDA graph,
@@ -492,6 +549,8 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         line["system_matrix_2d_fan_flat"] = sysmat_measure(dev)
     if not args.no_rebin and world == 1:
         line["rebin_fan_to_parallel"] = rebin_measure(P, vol, ang)
+    if not args.no_helical and world == 1:
+        line["helical_arc_512x512x128_736x64_5x1152views"] = helical_measure(dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         sample = cpu_reference_sample(4, vol.cpu().numpy())
         line["cpu_baseline"] = {k: v for k, v in sample.items() if k != "seconds"} if sample else None
@@ -513,6 +572,7 @@ def main():
     ap.add_argument("--no-ops", action="store_true", help="skip the per-operator timings")
     ap.add_argument("--no-sysmat", action="store_true", help="skip the system-matrix export timing")
     ap.add_argument("--no-rebin", action="store_true", help="skip the rebinning timing")
+    ap.add_argument("--no-helical", action="store_true", help="skip the helical projector timings")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
     args = ap.parse_args()

@@ -437,6 +437,10 @@ int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
 typedef struct {
     int view_mode, weight_mode;
     float view_turns, halfscan_coef, tang_k, tang_blend;
+    /* pin aid: take the window length's quotient span/|dbeta| one float ulp
+     * up before ceil(), as the reference's --use_fast_math division turned
+     * out to do at an exact integer quotient (tests/golden/helical_ref_*) */
+    int window_quotient_up;
 } hopt_t;
 
 typedef struct {
@@ -570,7 +574,8 @@ static void hw_view_window(float pz, const float* ang, const float* zsrc, const 
     /* a window of V or more views is all views, and a centre beyond +-4V
      * gives the same clamped window as +-4V: both bounds keep the integer
      * arithmetic in range (the reference's values wherever it has them) */
-    const float nwf = ceilf(span / fabsf(db));
+    const float quot = span / fabsf(db);
+    const float nwf = ceilf(o->window_quotient_up ? nextafterf(quot, INFINITY) : quot);
     const int nwin = (nwf >= (float)nview) ? nview : (nwf < 1.0f ? 1 : (int)nwf);
     const float bc = a0 + (pz - z0) / dzdb;
     const float vcf = roundf((bc - a0) / db);
@@ -711,7 +716,8 @@ static float hw_pair_weight(const geo3_t* g, const hopt_t* o, const float* ang, 
 }
 
 /* Apply one helical operator.  fo = {view_mode, weight_mode, view_turns,
- * halfscan_coef, tang_k, tang_blend}; sp = source_pos [4][nview]. */
+ * halfscan_coef, tang_k, tang_blend, window_quotient_up}; sp = source_pos
+ * [4][nview]. */
 int xo_helical3d(int op, const int* ni, const double* fv, const double* fg, const double* fo,
                  const double* in, double* out, const float* ang, const float* sp, int nbatch, int nview)
 {
@@ -722,6 +728,7 @@ int xo_helical3d(int op, const int* ni, const double* fv, const double* fg, cons
     hopt_t o;
     o.view_mode = (int)fo[0]; o.weight_mode = (int)fo[1];
     o.view_turns = (float)fo[2]; o.halfscan_coef = (float)fo[3]; o.tang_k = (float)fo[4]; o.tang_blend = (float)fo[5];
+    o.window_quotient_up = (int)fo[6];
     if (op < 0 || op > 5 || nview < 1) return 1;
     const long long nvox = (long long)g.W * g.H * g.D;
     const long long ncell = (long long)g.Nu * g.Nv;

@@ -124,10 +124,17 @@ def unpack_helical(options):
     return vals
 
 
-def helical3d(op: str, x, options, angles, source_pos):
+def helical3d(op: str, x, options, angles, source_pos, window_quotient_up: bool = False):
     """Apply a helical arc-detector operator (the reference's
     src/kernels/helical_arc3d.cu).  x: [B, C, D, H, W] or [B, C, V, Nv, Nu];
-    source_pos: [4, V] (source_z, shift_radius, shift_angle, shift_z)."""
+    source_pos: [4, V] (source_z, shift_radius, shift_angle, shift_z).
+
+    ``window_quotient_up`` takes the view-window length ceil(span / |dbeta|)
+    of a quotient moved one float ulp up: the reference, built with
+    --use_fast_math, evaluates that division approximately, and at an exact
+    integer quotient (whole views per turn) its window came out one view
+    longer than the exact formula gives.  Only the pin against the
+    reference's recorded outputs uses it."""
     g = unpack3d(options)
     ang = np.ascontiguousarray(angles, dtype=np.float32)
     V = ang.shape[0]
@@ -141,7 +148,7 @@ def helical3d(op: str, x, options, angles, source_pos):
     ni = np.array([g["W"], g["H"], g["D"], g["Nu"], g["Nv"]], dtype=np.int32)
     fv = np.array([g["dx"], g["dy"], g["dz"], g["shx"], g["shy"], g["shz"]], dtype=np.float64)
     fg = np.array([g["du"], g["dv"], g["shu"], g["shv"], g["SOD"], g["SDD"]], dtype=np.float64)
-    fo = np.array(unpack_helical(options), dtype=np.float64)
+    fo = np.array(unpack_helical(options) + [1.0 if window_quotient_up else 0.0], dtype=np.float64)
     rc = _load().xo_helical3d(OPS[op], _p(ni, ctypes.c_int), _p(fv, ctypes.c_double), _p(fg, ctypes.c_double),
                               _p(fo, ctypes.c_double), _p(x, ctypes.c_double), _p(out, ctypes.c_double),
                               _p(ang, ctypes.c_float), _p(sp, ctypes.c_float), B * C, V)

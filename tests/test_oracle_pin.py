@@ -167,3 +167,32 @@ def test_helical_oracle_adjoint_pairs(modes):
         rhs = float(np.sum(x * O.helical3d(adj, y, o, ang, sp)))
         assert abs(lhs - rhs) <= 1e-12 * abs(lhs), (fwd, adj, lhs, rhs)
         assert lhs != 0.0
+
+
+HELICAL_REF_TOL = {"A": 2e-4, "AT": 2e-4, "B": 2e-4, "BT": 2e-4, "BW": 5e-4, "BWT": 5e-4}
+
+
+@pytest.mark.parametrize("case", ["one_turn_ffs", "auto_tang", "half_scan"])
+def test_helical_oracle_matches_reference_cuda_outputs(case):
+    """The FP64 helical oracle against the reference's own helical CUDA
+    kernels (helical_arc3d.cu, built from its sources and run on a B200 by
+    tests/golden/make_golden_helical.py).  The reference computes in FP32
+    with --use_fast_math: measured distances are 1e-5 .. 9e-5 for A, A^T, B,
+    B^T and up to 2.2e-4 for the weighted pair, whose few outlying voxels sit
+    on discrete tests (detector edge, window quality) that fast-math rounding
+    flips.  In the one-turn case with 96 views per turn the window length
+    ceil(2 pi / dbeta) has an exact integer quotient; the reference's
+    approximate division came out one view longer, which the oracle's
+    window_quotient_up reproduces (without it Bw differs by 5e-3)."""
+    g = load_golden(f"helical_ref_{case}")
+    assert bool(g["guard_ok"]), "the reference wrote outside its output while recording"
+    tie = case == "one_turn_ffs"
+    for op in ("A", "AT", "B", "BT", "BW", "BWT"):
+        x = g["image"] if op in IMG_IN else g["sino"]
+        got = O.helical3d(op, x, g["options"], g["angles"], g["source_pos"],
+                          window_quotient_up=tie and op in ("BW", "BWT"))
+        err = rel_l2(got, g[op])
+        assert err < HELICAL_REF_TOL[op], f"{case} {op}: rel L2 {err:.3e}"
+    if tie:
+        exact = O.helical3d("BW", g["sino"], g["options"], g["angles"], g["source_pos"])
+        assert rel_l2(exact, g["BW"]) > 1e-3  # the tie is real: the exact window differs by a view
