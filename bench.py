@@ -181,6 +181,61 @@ def cpu_reference_sample(nviews: int = 4, vol=None):
             "seconds": t2 - t0}
 
 
+def helical_reference_measure(reps: int = 1):
+    """The reference's own helical CUDA kernels (helical_arc3d.cu built
+    unchanged into oracle/_ref by oracle/build_oracle.py) on the HEL workload:
+    device times of A, B and Bw, the same operators helical_measure times on
+    this library.  Outputs carry a zero guard band of one plane on both sides
+    (the reference's scatter kernels index them from FP32 guesses)."""
+    import ctypes
+    import numpy as np
+    import torch
+    from oracle import build_oracle
+    so = build_oracle.REF_HELICAL_SO
+    if not so.exists() or not torch.cuda.is_available():
+        return {"unavailable": "reference helical library oracle/_ref not built or no GPU"}
+    lib = ctypes.CDLL(str(so))
+    lib.xr_ref_helical.restype = ctypes.c_int
+    lib.xr_ref_helical.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_float)] + [ctypes.c_void_p] * 4 + \
+                                  [ctypes.c_int, ctypes.c_int]
+    dev = torch.device("cuda:0")
+    P, ang = helical_projector(dev)
+    opts = (ctypes.c_float * 24)(*P.options.cpu().tolist())
+    sp = P.source_position(ang).contiguous()
+    h = HEL
+    V = ang.numel()
+    nvox, ncell = h["W"] * h["H"] * h["D"], V * h["Nv"] * h["Nu"]
+    gi, gs = h["W"] * h["H"], h["Nv"] * h["Nu"]
+    g = torch.Generator(device=dev).manual_seed(3)
+    img = torch.zeros(nvox + 2 * gi, device=dev)
+    sino = torch.zeros(ncell + 2 * gs, device=dev)
+    img[gi:gi + nvox] = torch.rand(nvox, device=dev, generator=g)
+    ip, sp_ = img.data_ptr() + 4 * gi, sino.data_ptr() + 4 * gs
+    out = {}
+    for op, key, zero_img in ((0, "A_ms", False), (2, "B_ms", True), (4, "Bw_ms", True)):
+        ts = []
+        for i in range(reps + 1):
+            if zero_img:
+                img.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            rc = lib.xr_ref_helical(op, opts, ip, sp_, ang.data_ptr(), sp.data_ptr(), 1, V)
+            e1.record()
+            torch.cuda.synchronize()
+            if rc != 0:
+                return {"unavailable": f"reference helical op {op} returned CUDA error {rc}"}
+            if i > 0:
+                ts.append(e0.elapsed_time(e1))
+        out[key] = sum(ts) / len(ts)
+    out["guard_ok"] = bool(img[:gi].abs().max() == 0 and img[gi + nvox:].abs().max() == 0 and
+                           sino[:gs].abs().max() == 0 and sino[gs + ncell:].abs().max() == 0)
+    out["views"] = int(V)
+    del img, sino
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference_arm(args, rank: int):
     if rank != 0:
         return 0
@@ -205,6 +260,8 @@ def run_reference_arm(args, rank: int):
                          "sample": samples[0]["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_helical:
+        line["helical_arc_512x512x128_736x64_5x1152views"] = helical_reference_measure()
     print(json.dumps(line))
     return 0
 
@@ -573,6 +630,8 @@ def main():
     ap.add_argument("--no-sysmat", action="store_true", help="skip the system-matrix export timing")
     ap.add_argument("--no-rebin", action="store_true", help="skip the rebinning timing")
     ap.add_argument("--no-helical", action="store_true", help="skip the helical projector timings")
+    ap.add_argument("--helical-only", action="store_true",
+                    help="profiling: only the helical projector timings (one JSON line)")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
     args = ap.parse_args()
@@ -581,6 +640,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank)
+    if args.helical_only:
+        import torch
+        print(json.dumps({"helical_arc_512x512x128_736x64_5x1152views": helical_measure(torch.device("cuda:0"))}))
+        return 0
     if world > 1:
         import datetime
         import torch

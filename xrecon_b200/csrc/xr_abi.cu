@@ -671,7 +671,7 @@ int sysmat(int dim3d, const Geom& g, const float* ang, int nview, const long lon
 
 struct HelLayout {
     Layout l;  // view tables (+ the flipped image for A / B^T, row prefix tables for B, A^T, Bw)
-    size_t hel, wv, zw, scan, scale, imgs, total;
+    size_t hel, wv, zw, scan, wtab, scale, imgs, total;
 };
 
 HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
@@ -682,13 +682,16 @@ HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
     const size_t V = (size_t)(nview > 0 ? nview : 1);
     h.hel = o;  o = align256(o + V * sizeof(HelView));
     h.wv = o;   o = align256(o + V * sizeof(HelWView));
-    h.zw = h.scan = h.scale = h.imgs = o;
+    h.zw = h.scan = h.wtab = h.scale = h.imgs = o;
     if (op == OP_BW || op == OP_BWT) {
         const size_t nvox = (size_t)g.D * g.H * g.W;
         h.zw = o;    o = align256(o + (size_t)g.D * sizeof(HelZ));
         h.scan = o;  o = align256(o + sizeof(HelScanF));
-        h.scale = o; o = align256(o + nvox * sizeof(float));
-        if (op == OP_BWT) { h.imgs = o; o = align256(o + (size_t)nbatch * nvox * sizeof(float)); }
+        h.wtab = o;  o = align256(o + (size_t)g.D * V * sizeof(float));
+        if (op == OP_BWT) {
+            h.scale = o; o = align256(o + nvox * sizeof(float));
+            h.imgs = o;  o = align256(o + (size_t)nbatch * nvox * sizeof(float));
+        }
     }
     h.total = o;
     return h;
@@ -756,15 +759,21 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
         return fail(XR_ERR_UNSUPPORTED, "detector of %d x %d cells too large for one view's row table", g.Nu, g.Nv);
     HelZ* zw = reinterpret_cast<HelZ*>(ws + hl.zw);
     HelScanF* scan = reinterpret_cast<HelScanF*>(ws + hl.scan);
+    float* wtab = reinterpret_cast<float*>(ws + hl.wtab);
     float* scale = reinterpret_cast<float*>(ws + hl.scale);
+    const int nzg = (g.D + HEL_WBP_R - 1) / HEL_WBP_R;
     if (op == OP_BW || op == OP_BWT) {
+        if ((long long)nzg * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
         hel_zwin_kernel<<<(g.D + 127) / 128, 128, 0, st>>>(g, o, ang, sp, nview, zw, scan);
         if (int rc = check_cuda("hel_zwin")) return rc;
-        dim3 sg((g.W + 31) / 32, (g.H + 7) / 8, g.D);
-        hel_scale_kernel<<<sg, dim3(32, 8), 0, st>>>(g, o, scan, wv, zw, ang, sp, nview, scale);
-        if (int rc = check_cuda("hel_scale")) return rc;
+        hel_wtab_kernel<<<dim3((nview + 127) / 128, g.D), 128, 0, st>>>(scan, wv, zw, nview, wtab);
+        if (int rc = check_cuda("hel_wtab")) return rc;
     }
     if (op == OP_BWT) {
+        dim3 grid((g.W + 31) / 32, (g.H + HEL_WBP_NWY - 1) / HEL_WBP_NWY, nzg);
+        hel_wbp_kernel<HEL_WBP_R, HEL_WBP_NWY, false><<<grid, dim3(32, HEL_WBP_NWY), 0, st>>>(
+            g, gf, vt, o, scan, wv, zw, wtab, ang, sp, nullptr, scale, nview, nzg, dvv);
+        if (int rc = check_cuda("hel_wbp (normalisation)")) return rc;
         float* imgs = reinterpret_cast<float*>(ws + hl.imgs);
         const size_t nvox = (size_t)g.D * g.H * g.W, n = nvox * nbatch;
         hel_prescale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, scale, imgs, nvox, n);
@@ -775,8 +784,8 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
         for (int v0 = 0; v0 < total; v0 += 65535) {
             const int nz = std::min(65535, total - v0);
             dim3 grid((g.Nu + 31) / 32, (g.Nv + rows_per_cta - 1) / rows_per_cta, nz);
-            hel_wbpt_kernel<HEL_WBPT_R><<<grid, dim3(32, nwarp), 0, st>>>(g, vt, o, scan, wv, zw, ang, sp, imgs,
-                                                                          out, nview, v0, dvv);
+            hel_wbpt_kernel<HEL_WBPT_R><<<grid, dim3(32, nwarp), 0, st>>>(g, vt, o, scan, wv, zw, wtab, ang, sp,
+                                                                          imgs, out, nview, v0, dvv);
             if (int rc = check_cuda("hel_wbpt")) return rc;
         }
         return XR_OK;
@@ -790,11 +799,9 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
         row_prefix3d_kernel<float, false><<<pg, 128, 0, st>>>(g, vt, in, tab, nview, nbv, zd0, dvv);
     if (int rc = check_cuda("row_prefix3d")) return rc;
     if (op == OP_BW) {
-        const int nzg = (g.D + HEL_WBP_R - 1) / HEL_WBP_R;
-        if ((long long)nzg * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
         dim3 grid((g.W + 31) / 32, (g.H + HEL_WBP_NWY - 1) / HEL_WBP_NWY, nzg * nbatch);
-        hel_wbp_kernel<HEL_WBP_R, HEL_WBP_NWY><<<grid, dim3(32, HEL_WBP_NWY), 0, st>>>(
-            g, gf, vt, o, scan, wv, zw, ang, sp, tab, scale, out, nview, nzg, dvv);
+        hel_wbp_kernel<HEL_WBP_R, HEL_WBP_NWY, true><<<grid, dim3(32, HEL_WBP_NWY), 0, st>>>(
+            g, gf, vt, o, scan, wv, zw, wtab, ang, sp, tab, out, nview, nzg, dvv);
         return check_cuda("hel_wbp");
     }
     const int nzp = (g.D + PFX_R - 1) / PFX_R;

@@ -65,9 +65,13 @@ struct ViewHdr {
 //   cw    = column width of B / B^T, sod' du'
 //   zsrc  = source z (the projection's cell cosine takes the row's absolute z)
 //   inv_du = 1 / du' (column guesses)
+//   zlo, zhi = world z range, with a margin, of the voxels the view's detector
+//          rows can reach anywhere in the image plane (views outside a voxel
+//          run's z range are skipped)
 struct HelView {
     double z0dz, zd0;
     float cw, zsrc, inv_du, pad;
+    float zlo, zhi;
 };
 
 struct ViewTables {

@@ -22,11 +22,14 @@
 // test are evaluated in FP32 with the reference's operation order (explicit
 // round-to-nearest intrinsics where the result feeds a discrete decision), the
 // DD footprint through the FP64 view tables as elsewhere:
-//   hel_zwin_kernel   per z slice: window [vs, ve], its end angles, centre angle
-//   hel_scale_kernel  per voxel: the normalisation
+//   hel_zwin_kernel   per z slice: window [vs, ve], its end angles, centre
+//                     angle, and whether its weights depend on the view alone
+//   hel_wtab_kernel   the weights of those slices, per (slice, view)
 //   hel_wbp_kernel    Bw: voxel gather over the run's window through the row
-//                     prefix tables (xr_vox_prefix.cuh), per-voxel weights
-//   hel_wbpt_kernel   Bw^T: cell gather, the weight evaluated per voxel
+//                     prefix tables (xr_vox_prefix.cuh), per-voxel weights and
+//                     normalisation in one pass; its DD-free form gives the
+//                     normalisation volume that Bw^T needs
+//   hel_wbpt_kernel   Bw^T: cell gather, per-voxel weights
 #pragma once
 
 #include "xr_vox_prefix.cuh"
@@ -45,10 +48,13 @@ struct HelWView {
 };
 
 // Per z slice: view window [vs, ve], its end angles, the centre angle, the
-// slice's z.
+// slice's z, and whether the slice's weights depend on the view alone (the
+// conjugate-ray weight of a window spanning a full turn), in which case they
+// are tabulated per (slice, view) once per call.
 struct HelZ {
     int vs, ve;
     float bs, be, bc, pz;
+    int full, pad;
 };
 
 constexpr float XR_PI_F = 3.14159265358979323846f;
@@ -93,6 +99,20 @@ __global__ void setup_views_helical_kernel(const Geom g, const float* __restrict
     hv.zsrc = zsrc;
     hv.inv_du = (float)(1.0 / (double)du);
     hv.pad = 0.0f;
+    {
+        // A voxel at in-plane distance r from the source sees detector row
+        // z (relative to the source) at z_vox = z_row r / sdd'.  r spans
+        // sod' -+ the image half-diagonal; 2 % on r and two voxels of margin
+        // keep the range conservative for the DD footprints.
+        const double hx = 0.5 * g.W * g.dx + fabs(g.shx), hy = 0.5 * g.H * g.dy + fabs(g.shy);
+        const double rxy = sqrt(hx * hx + hy * hy);
+        const double rmin = fmax(0.98 * ((double)sod - rxy), 0.0), rmax = 1.02 * ((double)sod + rxy);
+        const double zb0 = hv.zd0, zb1 = hv.zd0 + g.Nv * g.dv;
+        const double lo = fmin(zb0 * rmin, zb0 * rmax) / (double)sdd;
+        const double hi = fmax(zb1 * rmin, zb1 * rmax) / (double)sdd;
+        hv.zlo = (float)((double)zsrc + lo - 2.0 * g.dz);
+        hv.zhi = (float)((double)zsrc + hi + 2.0 * g.dz);
+    }
     vt.hel[v] = hv;
     HelWView w;
     w.sod = sod;
@@ -249,12 +269,15 @@ __device__ __forceinline__ void hw_ray(const HelWView& w, float px, float py, fl
 }
 
 // Does the ray through the voxel centre hit the detector?
-// helical_arc3d.cu:305-336 (gamma and the xy ray length as hw_ray gives them).
-__device__ __forceinline__ bool hw_measured(const Geom& g, const HelWView& w, float gamma, float rxy, float pz) {
+// helical_arc3d.cu:305-336, split into the column test (per pixel and view)
+// and the row test (per voxel), with gamma and the xy ray length as hw_ray
+// gives them.
+__device__ __forceinline__ bool hw_col_in(const Geom& g, const HelWView& w, float gamma) {
     const float col = __fsub_rn(__fadd_rn(__fdiv_rn(__fsub_rn(gamma, w.shu), w.du), __fmul_rn((float)g.Nu, 0.5f)),
                                 0.5f);
-    if (col < -0.5f || col > __fsub_rn((float)g.Nu, 0.5f)) return false;
-    if (rxy <= 1.0e-6f) return false;
+    return !(col < -0.5f || col > __fsub_rn((float)g.Nu, 0.5f));
+}
+__device__ __forceinline__ bool hw_row_in(const Geom& g, const HelWView& w, float rxy, float pz) {
     const float det_z = __fadd_rn(w.szv, __fdiv_rn(__fmul_rn(w.sdd, __fsub_rn(pz, w.szv)), rxy));
     const float row = __fsub_rn(__fadd_rn(__fdiv_rn(__fsub_rn(__fsub_rn(det_z, w.zs), (float)g.shv), (float)g.dv),
                                           __fmul_rn((float)g.Nv, 0.5f)),
@@ -345,52 +368,49 @@ __global__ void hel_zwin_kernel(const Geom g, const HelOpts o, const float* __re
         }
     }
     z.bc = bc;
+    {
+        // hw_conjugate's full-turn branch (no fan angle, no voxel position)
+        const float db = (nview > 1) ? __fdiv_rn(__fsub_rn(ang[nview - 1], ang[0]), (float)(nview - 1)) : 0.0f;
+        const float adb = fmaxf(fabsf(db), 1.0e-6f);
+        z.full = (o.weight_mode == 0) && (fabsf(z.be - z.bs) >= __fsub_rn(2.0f * XR_PI_F, 2.0f * adb));
+    }
+    z.pad = 0;
     zw[iz] = z;
 }
 
-// Per-voxel normalisation (helical_arc3d.cu:1141-1180), one thread per voxel.
-__global__ void __launch_bounds__(256)
-hel_scale_kernel(const Geom g, const HelOpts o, const HelScanF* __restrict__ scan, const HelWView* __restrict__ wv,
-                 const HelZ* __restrict__ zw, const float* __restrict__ ang, const float* __restrict__ zsrc,
-                 const int nview, float* __restrict__ scale) {
-    const int ix = blockIdx.x * 32 + threadIdx.x;
-    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    const int iz = blockIdx.z;
-    if (ix >= g.W || iy >= g.H) return;
-    const HelScanF s = *scan;
+// Weight table of the full-turn slices: wtab[iz * nview + v] for v in the
+// slice's window (entries outside it are never read).
+__global__ void hel_wtab_kernel(const HelScanF* __restrict__ scan, const HelWView* __restrict__ wv,
+                                const HelZ* __restrict__ zw, const int nview, float* __restrict__ wtab) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y;
     const HelZ z = zw[iz];
-    const float px = hw_px(g, ix), py = hw_py(g, iy), pz = z.pz;
-    float valid = 0.0f;
-    for (int v = z.vs; v <= z.ve; ++v) {
-        const HelWView w = wv[v];
-        float gamma, rxy, rx, ry;
-        hw_ray(w, px, py, gamma, rxy, rx, ry);
-        if (rxy <= 1.0e-6f) continue;
-        const float wt = hw_weight(o, g, px, py, pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db, s.gmax,
-                                   ang, zsrc, nview);
-        if (wt == 0.0f) continue;
-        if (hw_measured(g, w, gamma, rxy, pz)) valid += wt;
-    }
-    const float ideal = (fabsf(s.db) > 1.0e-8f) ? __fdiv_rn(XR_PI_F, fabsf(s.db)) : valid;
-    float sc = __fdiv_rn(ideal, fmaxf(valid, 1.0e-6f));
-    sc = fminf(32.0f, fmaxf(0.03125f, sc));
-    scale[((size_t)iz * g.H + iy) * g.W + ix] = sc;
+    if (!z.full || v < z.vs || v > z.ve) return;
+    const HelScanF s = *scan;
+    wtab[(size_t)iz * nview + v] = hw_conjugate(wv[v].beta, 0.0f, z.bc, z.bs, z.be, s.db, s.gmax);
 }
 
 // ---------------------------------------------------------------------- Bw
 
-// Voxel gather of the weighted backprojection.  CTA = 32 x NWY pixels of the
-// image plane times a run of R z slices (the run's windows are CTA-uniform);
-// the view loop covers the union of the run's windows.  The z integral of a
+// Voxel gather of the weighted backprojection, with the per-voxel
+// normalisation in the same pass.  CTA = 32 x NWY pixels of the image plane
+// times a run of R z slices (the run's windows are CTA-uniform); the view
+// loop covers the union of the run's windows.  Per (pixel, view) the fan
+// angle and ray length are computed once; per voxel of the run the weight
+// comes from the slice table (full-turn slices) or is evaluated, and is
+// summed into the voxel's normalisation when the ray through its centre
+// hits the detector (helical_arc3d.cu:1141-1180).  The z integral of a
 // (voxel, column) pair comes from the row prefix table of the view
-// (xr_vox_prefix.cuh) as in vox_prefix3d_kernel; every voxel of the run has
-// its own weight, and its normalisation is applied at the end.
-template <int R, int NWY>
+// (xr_vox_prefix.cuh) as in vox_prefix3d_kernel.
+//   DD true : out = Bw voxels, (pi / |dbeta|) / sum, clamped, times the sum
+//             of the weighted footprints
+//   DD false: out = the normalisation itself (for Bw^T); no footprints
+template <int R, int NWY, bool DD>
 __global__ void __launch_bounds__(32 * NWY)
 hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts o, const HelScanF* __restrict__ scan,
-               const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ ang,
-               const float* __restrict__ zsrc, const float2* __restrict__ tab, const float* __restrict__ scale,
-               float* __restrict__ vol, const int nview, const int nzg, const double dvv) {
+               const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ wtab,
+               const float* __restrict__ ang, const float* __restrict__ zsrc, const float2* __restrict__ tab,
+               float* __restrict__ out, const int nview, const int nzg, const double dvv) {
     __shared__ HelZ szw[R];
     __shared__ int sv[2];
     const int ix = blockIdx.x * 32 + threadIdx.x;
@@ -401,7 +421,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
     if (tid < R) {
         HelZ z;
         if (j0 + tid < g.D) z = zw[j0 + tid];
-        else { z.vs = 1; z.ve = 0; z.bs = z.be = z.bc = z.pz = 0.0f; }
+        else { z.vs = 1; z.ve = 0; z.bs = z.be = z.bc = z.pz = 0.0f; z.full = 0; z.pad = 0; }
         szw[tid] = z;
     }
     __syncthreads();
@@ -416,18 +436,18 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
     if (ix >= g.W || iy >= g.H || j0 >= g.D) return;
     const int Nu = g.Nu, Nv = g.Nv;
     const size_t vstride = (size_t)(Nv + 2) * Nu;
-    const float2* __restrict__ tb = tab + (size_t)b * nview * vstride;
     const float px = hw_px(g, ix), py = hw_py(g, iy);
     const HelScanF s = *scan;
-    float acc[R];
+    float acc[R], valid[R];
 #pragma unroll
-    for (int i = 0; i < R; ++i) acc[i] = 0.0f;
+    for (int i = 0; i < R; ++i) { acc[i] = 0.0f; valid[i] = 0.0f; }
 
     for (int v = sv[0]; v <= sv[1]; ++v) {
         const HelWView w = wv[v];
         float gamma, rxy, rx, ry;
         hw_ray(w, px, py, gamma, rxy, rx, ry);
         if (rxy <= 1.0e-6f) continue;
+        const bool col_in = hw_col_in(g, w, gamma);
         float wt[R];
         bool any = false;
 #pragma unroll
@@ -435,12 +455,16 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
             const HelZ& z = szw[i];
             float wi = 0.0f;
             if (v >= z.vs && v <= z.ve)
-                wi = hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db, s.gmax, ang,
-                               zsrc, nview);
+                wi = z.full ? wtab[(size_t)(j0 + i) * nview + v]
+                            : hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db,
+                                        s.gmax, ang, zsrc, nview);
             wt[i] = wi;
-            any |= (wi != 0.0f);
+            if (wi != 0.0f) {
+                any = true;
+                if (col_in && hw_row_in(g, w, rxy, z.pz)) valid[i] += wi;
+            }
         }
-        if (!any) continue;
+        if (!DD || !any) continue;
         const ViewHdr& h = vt.hdr[v];
         const HelView hv = vt.hel[v];
         const int keep = h.keep;
@@ -475,7 +499,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
         const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
         const double* __restrict__ Rq = vt.colR + (size_t)v * Nu;
-        const float2* __restrict__ tv = tb + (size_t)v * vstride;
+        const float2* __restrict__ tv = tab + ((size_t)b * nview + v) * vstride;
         const double dp = (double)p, dL = (double)L;
         int k = ka;
         float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
@@ -518,12 +542,16 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
             pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
         }
     }
+    const float ideal_db = (fabsf(s.db) > 1.0e-8f) ? __fdiv_rn(XR_PI_F, fabsf(s.db)) : -1.0f;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
         const int j = j0 + i;
         if (j < g.D) {
             const size_t oi = ((size_t)j * g.H + iy) * g.W + ix;
-            vol[(size_t)b * g.D * g.H * g.W + oi] = acc[i] * scale[oi];
+            const float ideal = ideal_db >= 0.0f ? ideal_db : valid[i];
+            const float sc = fminf(32.0f, fmaxf(0.03125f, __fdiv_rn(ideal, fmaxf(valid[i], 1.0e-6f))));
+            if (DD) out[(size_t)b * g.D * g.H * g.W + oi] = acc[i] * sc;
+            else if (b == 0) out[oi] = sc;
         }
     }
 }
@@ -545,7 +573,8 @@ __global__ void hel_prescale_kernel(const float* __restrict__ img, const float* 
 template <int R>
 __global__ void __launch_bounds__(256)
 hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelScanF* __restrict__ scan,
-                const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ ang,
+                const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ wtab,
+                const float* __restrict__ ang,
                 const float* __restrict__ zsrc, const float* __restrict__ img_s, float* __restrict__ sino,
                 const int nview, const int view0, const double dvv) {
     const int k = blockIdx.x * 32 + threadIdx.x;
@@ -601,8 +630,9 @@ hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelSca
                 if ((unsigned)j >= (unsigned)g.D) return 0.0f;
                 const HelZ z = zw[j];
                 if (v < z.vs || v > z.ve) return 0.0f;
-                const float wt = hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db,
-                                           s.gmax, ang, zsrc, nview);
+                const float wt = z.full ? wtab[(size_t)j * nview + v]
+                                        : hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs,
+                                                    z.be, s.db, s.gmax, ang, zsrc, nview);
                 return wt == 0.0f ? 0.0f : wt * __ldg(col + (size_t)j * plane);
             };
             int j = j0;

@@ -126,6 +126,9 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
     // column bracket margin: half a column, plus the arc guess's angle error
     float inv_du = gf.inv_du;
     float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * inv_du : 0.0f);
+    // world z range of the run (helical view skipping)
+    const float zrun_lo = (float)((-0.5 * g.D + j0) * g.dz + g.shz);
+    const float zrun_hi = (float)((-0.5 * g.D + min(j0 + R, g.D)) * g.dz + g.shz);
     float acc[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) acc[i] = 0.0f;
@@ -136,6 +139,8 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         float cwv = cw;
         if (HEL) {
             const HelView hv = vt.hel[v];
+            // CTA-uniform: the whole z run lies outside what this view reaches
+            if (zrun_hi < hv.zlo || zrun_lo > hv.zhi) continue;
             zs = (double)j0 + hv.z0dz;
             zoffh = -hv.zd0 / dvv - 0.5;
             cwv = hv.cw;
