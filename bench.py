@@ -363,13 +363,13 @@ HEL = dict(W=512, H=512, D=128, dx=0.7, dz=0.8, Nu=736, Nv=64, du=1.2858, dv=1.0
            views_per_turn=1152, turns=5, pitch=30.7)
 
 
-def helical_projector(dev):
+def helical_projector(dev, turns=None):
     """Helical scan of a 512 x 512 x 128 volume (0.7 x 0.7 x 0.8 mm) on a
     736 x 64 arc detector (1.2858 x 1.0947 mm cells at SDD 1085.6 mm, SOD
     595 mm), 1152 views per turn over 5 turns, 30.7 mm rise per turn
     (pitch 0.8 of the 38.4 mm collimation), one-turn view windows."""
     from xrecon_b200 import HelicalProjector3d
-    h = HEL
+    h = dict(HEL, turns=turns or HEL["turns"])
     z_span = h["turns"] * h["pitch"]
     P = HelicalProjector3d((h["W"], h["H"], h["D"]), (h["Nu"], h["Nv"]), (h["dx"], h["dx"], h["dz"]),
                            (h["du"], h["dv"]), h["sod"], h["sdd"], pitch=h["pitch"], z0=-0.5 * z_span).to(dev)
@@ -380,12 +380,13 @@ def helical_projector(dev):
     return P, ang
 
 
-def helical_measure(dev, reps: int = 2):
-    """Per-operator device times of the helical projector (HEL workload);
-    throughput in voxel-views per second counts each voxel against the views
-    of one turn (the views whose source z is near the voxel's)."""
+def helical_measure(dev, reps: int = 2, turns=None):
+    """Per-operator device times of the helical projector (HEL workload;
+    ``turns`` fewer turns for profiling captures); throughput in voxel-views
+    per second counts each voxel against the views of one turn (the views
+    whose source z is near the voxel's)."""
     import torch
-    P, ang = helical_projector(dev)
+    P, ang = helical_projector(dev, turns)
     h = HEL
     g = torch.Generator(device=dev).manual_seed(3)
     vol = torch.rand((1, 1, h["D"], h["H"], h["W"]), device=dev, generator=g)
@@ -632,6 +633,8 @@ def main():
     ap.add_argument("--no-helical", action="store_true", help="skip the helical projector timings")
     ap.add_argument("--helical-only", action="store_true",
                     help="profiling: only the helical projector timings (one JSON line)")
+    ap.add_argument("--helical-turns", type=int, default=None,
+                    help="profiling: turns of the helical scan (default 5) with --helical-only")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
     args = ap.parse_args()
@@ -642,7 +645,8 @@ def main():
         return run_reference_arm(args, rank)
     if args.helical_only:
         import torch
-        print(json.dumps({"helical_arc_512x512x128_736x64_5x1152views": helical_measure(torch.device("cuda:0"))}))
+        print(json.dumps({"helical_arc_512x512x128_736x64_5x1152views":
+                          helical_measure(torch.device("cuda:0"), turns=args.helical_turns)}))
         return 0
     if world > 1:
         import datetime

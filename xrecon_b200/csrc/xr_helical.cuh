@@ -45,6 +45,7 @@ struct HelOpts {
 // Per-view FP32 scalars of the weighted kernels (helical_arc3d.cu:1148-1160).
 struct HelWView {
     float sod, sdd, du, shu, beta, sinv, cosv, sx, sy, szv, zs, shz;
+    float inv_du, pad0, pad1, pad2;  // 1 / du (fast pre-tests only)
 };
 
 // Per z slice: view window [vs, ve], its end angles, the centre angle, the
@@ -127,6 +128,8 @@ __global__ void setup_views_helical_kernel(const Geom g, const float* __restrict
     w.szv = zsrc;
     w.zs = zs;
     w.shz = szs;
+    w.inv_du = (float)(1.0 / (double)du);
+    w.pad0 = w.pad1 = w.pad2 = 0.0f;
     wv[v] = w;
 }
 
@@ -285,6 +288,37 @@ __device__ __forceinline__ bool hw_row_in(const Geom& g, const HelWView& w, floa
     return row >= -0.5f && row <= __fsub_rn((float)g.Nv, 0.5f);
 }
 
+// The same two tests decided from cheap approximations (reciprocals, the
+// fitted atan2 of the column guesses), falling back to the exact forms above
+// only when the approximate row or column lies within a safety band of an
+// edge: the approximations differ from the exact FP32 values by far less
+// than the band (the atan2 fit by XR_GUESS_ATAN_ERR rad, the rest by a few
+// ulps of values below 2^13), so every decision equals the exact one.
+constexpr float HW_BAND = 1.0e-3f;
+
+__device__ __forceinline__ bool hw_col_in_fast(const Geom& g, const HelWView& w, float px, float py, float xb,
+                                               float yb) {
+    const float ga = guess_atan2f(yb, w.sod - xb);
+    const float col = (ga - w.shu) * w.inv_du + 0.5f * (float)g.Nu - 0.5f;
+    const float band = HW_BAND + XR_GUESS_ATAN_ERR * w.inv_du;
+    const float top = (float)g.Nu - 0.5f;
+    if (col > -0.5f + band && col < top - band) return true;
+    if (col < -0.5f - band || col > top + band) return false;
+    const float xe = __fsub_rn(__fmul_rn(w.cosv, px), __fmul_rn(w.sinv, py));
+    const float ye = __fadd_rn(__fmul_rn(w.sinv, px), __fmul_rn(w.cosv, py));
+    return hw_col_in(g, w, atan2f(ye, __fsub_rn(w.sod, xe)));
+}
+
+// tz = sdd / rxy (approximate), inv_dv = 1 / dv
+__device__ __forceinline__ bool hw_row_in_fast(const Geom& g, const HelWView& w, float rxy, float tz, float inv_dv,
+                                               float pz) {
+    const float row = (w.szv + (pz - w.szv) * tz - w.zs - (float)g.shv) * inv_dv + 0.5f * (float)g.Nv - 0.5f;
+    const float top = (float)g.Nv - 0.5f;
+    if (row > -0.5f + HW_BAND && row < top - HW_BAND) return true;
+    if (row < -0.5f - HW_BAND || row > top + HW_BAND) return false;
+    return hw_row_in(g, w, rxy, pz);
+}
+
 // ------------------------------------------------------------ view windows
 
 // helical_arc3d.cu:141-210 and :121-139, one thread per z slice; thread 0
@@ -412,7 +446,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
                const float* __restrict__ ang, const float* __restrict__ zsrc, const float2* __restrict__ tab,
                float* __restrict__ out, const int nview, const int nzg, const double dvv) {
     __shared__ HelZ szw[R];
-    __shared__ int sv[2];
+    __shared__ int sv[3];
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y * NWY + threadIdx.y;
     const int zg = blockIdx.z % nzg, b = blockIdx.z / nzg;
@@ -421,18 +455,24 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
     if (tid < R) {
         HelZ z;
         if (j0 + tid < g.D) z = zw[j0 + tid];
-        else { z.vs = 1; z.ve = 0; z.bs = z.be = z.bc = z.pz = 0.0f; z.full = 0; z.pad = 0; }
+        else { z.vs = 1; z.ve = 0; z.bs = z.be = z.bc = z.pz = 0.0f; z.full = 1; z.pad = 0; }
         szw[tid] = z;
     }
     __syncthreads();
     if (tid == 0) {
-        int lo = nview, hi = -1;
-        for (int i = 0; i < R; ++i)
+        int lo = nview, hi = -1, allfull = 1;
+        for (int i = 0; i < R; ++i) {
             if (szw[i].vs <= szw[i].ve) { lo = min(lo, szw[i].vs); hi = max(hi, szw[i].ve); }
+            allfull &= szw[i].full;
+        }
         sv[0] = lo;
         sv[1] = hi;
+        sv[2] = allfull;
     }
     __syncthreads();
+    // every slice's weight comes from the table: no exact fan angle needed
+    // unless a test falls near an edge
+    const bool allfull = sv[2] != 0;
     if (ix >= g.W || iy >= g.H || j0 >= g.D) return;
     const int Nu = g.Nu, Nv = g.Nv;
     const size_t vstride = (size_t)(Nv + 2) * Nu;
@@ -442,12 +482,24 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
 #pragma unroll
     for (int i = 0; i < R; ++i) { acc[i] = 0.0f; valid[i] = 0.0f; }
 
+    const float inv_dv = (float)(1.0 / g.dv);
     for (int v = sv[0]; v <= sv[1]; ++v) {
         const HelWView w = wv[v];
-        float gamma, rxy, rx, ry;
-        hw_ray(w, px, py, gamma, rxy, rx, ry);
+        const float rx = __fsub_rn(px, w.sx), ry = __fsub_rn(py, w.sy);
+        const float rxy = sqrtf(__fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
         if (rxy <= 1.0e-6f) continue;
-        const bool col_in = hw_col_in(g, w, gamma);
+        const float xbv = w.cosv * px - w.sinv * py;
+        const float ybv = w.sinv * px + w.cosv * py;
+        bool col_in;
+        float gamma = 0.0f;
+        if (allfull) {
+            col_in = hw_col_in_fast(g, w, px, py, xbv, ybv);
+        } else {
+            float rxe, rye, rxye;
+            hw_ray(w, px, py, gamma, rxye, rxe, rye);
+            col_in = hw_col_in(g, w, gamma);
+        }
+        const float tz = __fdividef(w.sdd, rxy);
         float wt[R];
         bool any = false;
 #pragma unroll
@@ -461,7 +513,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
             wt[i] = wi;
             if (wi != 0.0f) {
                 any = true;
-                if (col_in && hw_row_in(g, w, rxy, z.pz)) valid[i] += wi;
+                if (col_in && hw_row_in_fast(g, w, rxy, tz, inv_dv, z.pz)) valid[i] += wi;
             }
         }
         if (!DD || !any) continue;
@@ -519,7 +571,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
                     const int r0 = (int)n0;
                     const float f0 = (float)(u0 - n0), fib = (float)ib;
                     const int col = keep ? k : Nu - 1 - k;
-                    const float wk = __fdiv_rn(wf * lf, fib);
+                    const float wk = __fdividef(wf * lf, fib);
                     const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
                     float gprev = 0.0f;
 #pragma unroll
