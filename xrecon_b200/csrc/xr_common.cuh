@@ -68,8 +68,9 @@ struct ViewHdr {
 //   zlo, zhi = world z range, with a margin, of the voxels the view's detector
 //          rows can reach anywhere in the image plane (views outside a voxel
 //          run's z range are skipped)
+//   zoffh = -zd0 / dv - 1/2 (row coordinate offset of the prefix gathers)
 struct HelView {
-    double z0dz, zd0;
+    double z0dz, zd0, zoffh;
     float cw, zsrc, inv_du, pad;
     float zlo, zhi;
 };

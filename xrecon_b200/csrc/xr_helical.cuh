@@ -96,6 +96,7 @@ __global__ void setup_views_helical_kernel(const Geom g, const float* __restrict
     HelView hv;
     hv.zd0 = -0.5 * g.Nv * g.dv + (double)zs + g.shv - (double)zsrc;
     hv.z0dz = (-0.5 * g.D * g.dz + g.shz - (double)zsrc) / g.dz;
+    hv.zoffh = -hv.zd0 / g.dv - 0.5;  // arc rows: dvv = dv
     hv.cw = __fmul_rn(sod, du);
     hv.zsrc = zsrc;
     hv.inv_du = (float)(1.0 / (double)du);
@@ -439,8 +440,11 @@ __global__ void hel_wtab_kernel(const HelScanF* __restrict__ scan, const HelWVie
 //   DD true : out = Bw voxels, (pi / |dbeta|) / sum, clamped, times the sum
 //             of the weighted footprints
 //   DD false: out = the normalisation itself (for Bw^T); no footprints
+#ifndef XR_HWBP_MINB
+#define XR_HWBP_MINB 3  // CTAs per SM the register budget is sized for
+#endif
 template <int R, int NWY, bool DD>
-__global__ void __launch_bounds__(32 * NWY)
+__global__ void __launch_bounds__(32 * NWY, XR_HWBP_MINB)
 hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts o, const HelScanF* __restrict__ scan,
                const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ wtab,
                const float* __restrict__ ang, const float* __restrict__ zsrc, const float2* __restrict__ tab,
@@ -534,9 +538,9 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
             yb = ya + gf.dy;
         }
         const double zs = (double)j0 + hv.z0dz;
-        const double zoffh = -hv.zd0 / dvv - 0.5;
+        const double zoffh = hv.zoffh;
         const double q = fma(h.q1, (double)L, h.q0);
-        const double mvdv = 1.0 / (q * dvv);
+        const double mvdv = __drcp_rn(q * dvv);
         // column width SOD du over the squared source distance
         const float lf = __fdiv_rn(s.cwW, __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
         const float margin = 0.5f + XR_GUESS_ATAN_ERR * hv.inv_du;
@@ -551,7 +555,8 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
         const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
         const double* __restrict__ Rq = vt.colR + (size_t)v * Nu;
-        const float2* __restrict__ tv = tab + ((size_t)b * nview + v) * vstride;
+        const char* __restrict__ tvb = reinterpret_cast<const char*>(tab + ((size_t)b * nview + v) * vstride);
+        const unsigned Nu8 = (unsigned)Nu * 8u;
         const double dp = (double)p, dL = (double)L;
         int k = ka;
         float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
@@ -566,22 +571,30 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
             if (wf > 0.0f) {
                 const double ib = mvdv * Rq[k];  // detector rows per voxel
                 const double u0 = fma(zs, ib, zoffh);
+                // the guard keeps local row indices far below 2^22, where the
+                // FP32 round-to-nearest by 1.5 * 2^23 below is exact
                 if ((float)ib < 4096.0f && u0 < (double)Nv - 0.5 && u0 + R * ib > -0.5) {
-                    const double n0 = floor(u0 + 0.5);
-                    const int r0 = (int)n0;
+                    const double t0 = u0 + 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer
+                    const double n0 = t0 - 6755399441055744.0;
+                    const int r0 = __double2loint(t0);
                     const float f0 = (float)(u0 - n0), fib = (float)ib;
                     const int col = keep ? k : Nu - 1 - k;
-                    const float wk = __fdividef(wf * lf, fib);
+                    // entry of local row n: tvb + ((r0 + 1 + n) Nu + col) 8
+                    //   = cb + bits(n + 1.5 * 2^23) Nu8, bits read as unsigned
+                    const char* cb = reinterpret_cast<const char*>(
+                        reinterpret_cast<uintptr_t>(tvb) +
+                        (uintptr_t)((long long)(r0 + 1) * Nu8 + (long long)col * 8 - 0x4B400000ll * (long long)Nu8));
+                    const float wk = wf * lf * __frcp_rn(fib);
+                    // rows -1 .. Nv of the detector (table rows 0 .. Nv + 1)
                     const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
                     float gprev = 0.0f;
 #pragma unroll
                     for (int i = 0; i <= R; ++i) {
-                        // boundary i in rows relative to r0, clamped to the
-                        // table (rows -1 .. Nv of the detector: t in [0, Nv + 1])
                         const float uc = fminf(fmaxf(fmaf((float)i, fib, f0), ulo), uhi);
-                        const float nf = rintf(uc);
-                        const int t = r0 + 1 + (int)nf;
-                        const float2 e = __ldg(tv + (size_t)t * Nu + col);
+                        const float tr = uc + 12582912.0f;  // round to nearest integer (FMA pipe)
+                        const float nf = tr - 12582912.0f;
+                        const float2 e = __ldg(reinterpret_cast<const float2*>(
+                            cb + (size_t)(unsigned)__float_as_int(tr) * Nu8));
                         const float gi = fmaf(uc - nf, e.y, e.x);
                         if (i > 0) acc[i - 1] = fmaf(wk * wt[i - 1], gi - gprev, acc[i - 1]);
                         gprev = gi;

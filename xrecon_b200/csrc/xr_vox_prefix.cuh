@@ -142,7 +142,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             // CTA-uniform: the whole z run lies outside what this view reaches
             if (zrun_hi < hv.zlo || zrun_lo > hv.zhi) continue;
             zs = (double)j0 + hv.z0dz;
-            zoffh = -hv.zd0 / dvv - 0.5;
+            zoffh = hv.zoffh;
             cwv = hv.cw;
             inv_du = hv.inv_du;
             margin = 0.5f + XR_GUESS_ATAN_ERR * inv_du;
