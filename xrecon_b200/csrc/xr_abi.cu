@@ -671,7 +671,7 @@ int sysmat(int dim3d, const Geom& g, const float* ang, int nview, const long lon
 
 struct HelLayout {
     Layout l;  // view tables (+ the flipped image for A / B^T, row prefix tables for B, A^T, Bw)
-    size_t hel, wv, zw, scan, wtab, scale, imgs, total;
+    size_t hel, wv, zw, scan, wtab, scale, imgs, imgsT, total;
 };
 
 HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
@@ -682,7 +682,7 @@ HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
     const size_t V = (size_t)(nview > 0 ? nview : 1);
     h.hel = o;  o = align256(o + V * sizeof(HelView));
     h.wv = o;   o = align256(o + V * sizeof(HelWView));
-    h.zw = h.scan = h.wtab = h.scale = h.imgs = o;
+    h.zw = h.scan = h.wtab = h.scale = h.imgs = h.imgsT = o;
     if (op == OP_BW || op == OP_BWT) {
         const size_t nvox = (size_t)g.D * g.H * g.W;
         h.zw = o;    o = align256(o + (size_t)g.D * sizeof(HelZ));
@@ -691,6 +691,7 @@ HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
         if (op == OP_BWT) {
             h.scale = o; o = align256(o + nvox * sizeof(float));
             h.imgs = o;  o = align256(o + (size_t)nbatch * nvox * sizeof(float));
+            h.imgsT = o; o = align256(o + (size_t)nbatch * nvox * sizeof(float));
         }
     }
     h.total = o;
@@ -778,6 +779,10 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
         const size_t nvox = (size_t)g.D * g.H * g.W, n = nvox * nbatch;
         hel_prescale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, scale, imgs, nvox, n);
         if (int rc = check_cuda("hel_prescale")) return rc;
+        float* imgsT = reinterpret_cast<float*>(ws + hl.imgsT);
+        dim3 tg((g.W + 31) / 32, (g.H + 31) / 32, g.D * nbatch);
+        transpose_flip_kernel<float><<<tg, dim3(32, 8), 0, st>>>(imgs, imgsT, g.H, g.W, g.H);
+        if (int rc = check_cuda("transpose")) return rc;
         const int nwarp = std::min(8, (g.Nv + HEL_WBPT_R - 1) / HEL_WBPT_R);
         const int rows_per_cta = nwarp * HEL_WBPT_R;
         const int total = nview * nbatch;
@@ -785,7 +790,7 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
             const int nz = std::min(65535, total - v0);
             dim3 grid((g.Nu + 31) / 32, (g.Nv + rows_per_cta - 1) / rows_per_cta, nz);
             hel_wbpt_kernel<HEL_WBPT_R><<<grid, dim3(32, nwarp), 0, st>>>(g, vt, o, scan, wv, zw, wtab, ang, sp,
-                                                                          imgs, out, nview, v0, dvv);
+                                                                          imgs, imgsT, out, nview, v0, dvv);
             if (int rc = check_cuda("hel_wbpt")) return rc;
         }
         return XR_OK;

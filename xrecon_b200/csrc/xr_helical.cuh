@@ -413,16 +413,20 @@ __global__ void hel_zwin_kernel(const Geom g, const HelOpts o, const float* __re
     zw[iz] = z;
 }
 
-// Weight table of the full-turn slices: wtab[iz * nview + v] for v in the
-// slice's window (entries outside it are never read).
+// Weight table of the full-turn slices: wtab[iz * nview + v], zero outside
+// the slice's window (rows of the other slices are zero and never read).
 __global__ void hel_wtab_kernel(const HelScanF* __restrict__ scan, const HelWView* __restrict__ wv,
                                 const HelZ* __restrict__ zw, const int nview, float* __restrict__ wtab) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int iz = blockIdx.y;
+    if (v >= nview) return;
     const HelZ z = zw[iz];
-    if (!z.full || v < z.vs || v > z.ve) return;
-    const HelScanF s = *scan;
-    wtab[(size_t)iz * nview + v] = hw_conjugate(wv[v].beta, 0.0f, z.bc, z.bs, z.be, s.db, s.gmax);
+    float w = 0.0f;
+    if (z.full && v >= z.vs && v <= z.ve) {
+        const HelScanF s = *scan;
+        w = hw_conjugate(wv[v].beta, 0.0f, z.bc, z.bs, z.be, s.db, s.gmax);
+    }
+    wtab[(size_t)iz * nview + v] = w;
 }
 
 // ---------------------------------------------------------------------- Bw
@@ -441,7 +445,7 @@ __global__ void hel_wtab_kernel(const HelScanF* __restrict__ scan, const HelWVie
 //             of the weighted footprints
 //   DD false: out = the normalisation itself (for Bw^T); no footprints
 #ifndef XR_HWBP_MINB
-#define XR_HWBP_MINB 3  // CTAs per SM the register budget is sized for
+#define XR_HWBP_MINB 4  // CTAs per SM the register budget is sized for
 #endif
 template <int R, int NWY, bool DD>
 __global__ void __launch_bounds__(32 * NWY, XR_HWBP_MINB)
@@ -640,8 +644,13 @@ __global__ void __launch_bounds__(256)
 hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelScanF* __restrict__ scan,
                 const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ wtab,
                 const float* __restrict__ ang,
-                const float* __restrict__ zsrc, const float* __restrict__ img_s, float* __restrict__ sino,
-                const int nview, const int view0, const double dvv) {
+                const float* __restrict__ zsrc, const float* __restrict__ img_s, const float* __restrict__ img_sT,
+                float* __restrict__ sino, const int nview, const int view0, const double dvv) {
+    // every slice tabulated: the weight of voxel j is wtab[j][v], with no
+    // fan angle and no window test
+    int full_here = 1;
+    for (int i = threadIdx.y * 32 + threadIdx.x; i < g.D; i += blockDim.x * blockDim.y) full_here &= zw[i].full;
+    const bool allfull = __syncthreads_and(full_here) != 0;
     const int k = blockIdx.x * 32 + threadIdx.x;
     const int r0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
     const int vb = blockIdx.z + view0;
@@ -652,12 +661,17 @@ hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelSca
     const HelView hv = vt.hel[v];
     const HelWView w = wv[v];
     const HelScanF s = *scan;
+    const float* __restrict__ wcol = wtab + v;  // wcol[j * nview] = weight of slice j
     const size_t ob = (size_t)v * (Nu + 1) + k;
     const double bA0 = vt.bA[ob], bB0 = vt.bB[ob], bA1 = vt.bA[ob + 1], bB1 = vt.bB[ob + 1];
     const double Qk = vt.colQ[(size_t)v * Nu + k];
     const int nlines = h.nlines, npix = h.npix;
     const size_t plane = (size_t)g.H * g.W;
-    const float* __restrict__ vol = img_s + (size_t)b * g.D * plane;
+    // lines of x-axis views are image rows; those of y-axis views are image
+    // columns, read from the flipped transpose so that a warp's lanes (the
+    // CTA's detector columns) stay on neighbouring addresses
+    const float* __restrict__ vol = (h.use_x ? img_s : img_sT) + (size_t)b * g.D * plane;
+    const int lpitch = h.use_x ? g.W : g.H;
     const double zr0 = hv.zd0 + r0 * dvv;
     float acc[R];
 #pragma unroll
@@ -685,19 +699,30 @@ hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelSca
             int ix, iy;
             if (h.use_x) { ix = p; iy = L; } else { ix = L; iy = g.H - 1 - p; }
             const float px = hw_px(g, ix), py = hw_py(g, iy);
-            float gamma, rxy, rx, ry;
-            hw_ray(w, px, py, gamma, rxy, rx, ry);
+            const float rx = __fsub_rn(px, w.sx), ry = __fsub_rn(py, w.sy);
+            const float r2 = __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry));
+            const float rxy = sqrtf(r2);
             if (rxy <= 1.0e-6f) continue;
-            const float lf = wxy * __fdiv_rn(s.cwW, __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
-            const float* __restrict__ col = vol + (size_t)iy * g.W + ix;
+            float gamma = 0.0f;
+            if (!allfull) {
+                float rxe, rye, rxye;
+                hw_ray(w, px, py, gamma, rxye, rxe, rye);
+            }
+            const float lf = wxy * __fdividef(s.cwW, r2);
+            const float* __restrict__ col = vol + (size_t)L * lpitch + p;
             // value of voxel j of this column: weight x normalised image
             auto value = [&](int j) -> float {
                 if ((unsigned)j >= (unsigned)g.D) return 0.0f;
-                const HelZ z = zw[j];
-                if (v < z.vs || v > z.ve) return 0.0f;
-                const float wt = z.full ? wtab[(size_t)j * nview + v]
-                                        : hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs,
-                                                    z.be, s.db, s.gmax, ang, zsrc, nview);
+                float wt;
+                if (allfull) {
+                    wt = __ldg(wcol + (size_t)j * nview);
+                } else {
+                    const HelZ z = zw[j];
+                    if (v < z.vs || v > z.ve) return 0.0f;
+                    wt = z.full ? __ldg(wcol + (size_t)j * nview)
+                                : hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db,
+                                            s.gmax, ang, zsrc, nview);
+                }
                 return wt == 0.0f ? 0.0f : wt * __ldg(col + (size_t)j * plane);
             };
             int j = j0;
