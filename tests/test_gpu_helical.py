@@ -101,7 +101,7 @@ def test_helical_adjoint_pairs(cuda, case):
 
 
 def test_helical_plain_kernels_match_oracle(cuda):
-    """A and B^T through the plain (non-TMA) cell gather."""
+    """A, B^T and Bw^T through the plain (non-TMA) cell gathers."""
     from xrecon_b200 import _native
     P = _projector()
     V = 192
@@ -111,7 +111,7 @@ def test_helical_plain_kernels_match_oracle(cuda):
     a, s = torch.from_numpy(ang).to(cuda), torch.from_numpy(sp).to(cuda)
     _native.set_plain_kernels(True)
     try:
-        for op in ("A", "BT"):
+        for op in ("A", "BT", "BWT"):
             got = getattr(P, METHOD[op])(torch.from_numpy(x).to(cuda), a, s).cpu().numpy()
             assert rel_l2(got, O.helical3d(op, x, P.options.numpy(), ang, sp)) < TOL, op
     finally:

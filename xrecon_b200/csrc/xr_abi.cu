@@ -368,7 +368,8 @@ template <> constexpr int dtype_code<__half>() { return DT_F16; }
 template <typename TI, typename TO, int R, int MODE, bool HEL>
 int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr, const CUtensorMap& mc,
                          const TI* rows, const TI* cols, int pitch_r, int pitch_c, TO* out, int nbatch, int nview,
-                         const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
+                         const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw,
+                         const float* zwt) {
     auto kern = p.fine ? cell_tma3d_kernel<TI, TO, R, 2, MODE, true, HEL>
                        : cell_tma3d_kernel<TI, TO, R, 2, MODE, false, HEL>;
     const int maxlines = std::max(g.W, g.H);
@@ -381,7 +382,7 @@ int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr
         const int nz = std::min(65535, total - z0);
         dim3 grid((g.Nu + 31) / 32, (g.Nv + RG - 1) / RG, nz);
         kern<<<grid, dim3(32, CELL_NW), smem, st>>>(g, vt, mr, mc, rows, cols, pitch_r, pitch_c, out, nview, z0, z0dz,
-                                                    zd0, dvv, cw, p.BP, p.BZ);
+                                                    zd0, dvv, cw, p.BP, p.BZ, zwt);
         if (int rc = check_cuda("cell_tma3d")) return rc;
     }
     return XR_OK;
@@ -404,7 +405,8 @@ CellPlan plan_cell_helical(const Geom& g) {
 
 template <typename TI, typename TO, bool HEL = false>
 int run_cell_tma(int eff, const Geom& g, const TI* in, TO* out, int nbatch, int nview, char* ws, const Layout& l,
-                 const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw) {
+                 const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw,
+                 const float* zwt = nullptr) {
     if (!std::is_same<TO, TI>::value && !std::is_same<TO, float>::value) return -1;
     if (reinterpret_cast<uintptr_t>(in) % 16 != 0) return -1;
     const CellPlan p = HEL ? plan_cell_helical(g) : plan_cell(g);
@@ -431,13 +433,13 @@ int run_cell_tma(int eff, const Geom& g, const TI* in, TO* out, int nbatch, int 
         !encode_line_map(&mc, dtype_code<TI>(), cols, g.H, g.W, g.D, nbatch, Hp, p.BP, p.BZ))
         return -1;
     if (p.R == 16) {
-        if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 16, OP_A, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-        if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 16, OP_BT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-        return launch_cell_tma_mode<TI, TO, 16, OP_BWT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+        if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 16, OP_A, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw, zwt);
+        if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 16, OP_BT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw, zwt);
+        return launch_cell_tma_mode<TI, TO, 16, OP_BWT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw, zwt);
     }
-    if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 8, OP_A, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-    if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 8, OP_BT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
-    return launch_cell_tma_mode<TI, TO, 8, OP_BWT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw);
+    if (eff == OP_A) return launch_cell_tma_mode<TI, TO, 8, OP_A, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw, zwt);
+    if (eff == OP_BT) return launch_cell_tma_mode<TI, TO, 8, OP_BT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw, zwt);
+    return launch_cell_tma_mode<TI, TO, 8, OP_BWT, HEL>(g, p, mr, mc, rows, cols, Wp, Hp, out, nbatch, nview, vt, st, z0dz, zd0, dvv, cw, zwt);
 }
 
 template <typename TI, typename TO>
@@ -676,8 +678,7 @@ struct HelLayout {
 
 HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
     HelLayout h;
-    // Bw^T reads the normalised image directly: view tables only
-    h.l = layout(1, op == OP_BWT ? -1 : op, g, nbatch, nview, DT_F32);
+    h.l = layout(1, op, g, nbatch, nview, DT_F32);
     size_t o = h.l.total;
     const size_t V = (size_t)(nview > 0 ? nview : 1);
     h.hel = o;  o = align256(o + V * sizeof(HelView));
@@ -687,7 +688,7 @@ HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
         const size_t nvox = (size_t)g.D * g.H * g.W;
         h.zw = o;    o = align256(o + (size_t)g.D * sizeof(HelZ));
         h.scan = o;  o = align256(o + sizeof(HelScanF));
-        h.wtab = o;  o = align256(o + (size_t)g.D * V * sizeof(float));
+        h.wtab = o;  o = align256(o + (size_t)(g.D + 3) * V * sizeof(float));  // slices -1 .. D + 1
         if (op == OP_BWT) {
             h.scale = o; o = align256(o + nvox * sizeof(float));
             h.imgs = o;  o = align256(o + (size_t)nbatch * nvox * sizeof(float));
@@ -760,14 +761,15 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
         return fail(XR_ERR_UNSUPPORTED, "detector of %d x %d cells too large for one view's row table", g.Nu, g.Nv);
     HelZ* zw = reinterpret_cast<HelZ*>(ws + hl.zw);
     HelScanF* scan = reinterpret_cast<HelScanF*>(ws + hl.scan);
-    float* wtab = reinterpret_cast<float*>(ws + hl.wtab);
+    float* wtab_pad = reinterpret_cast<float*>(ws + hl.wtab);  // slice j at row j + 1
+    float* wtab = wtab_pad + nview;                             // slice j at row j
     float* scale = reinterpret_cast<float*>(ws + hl.scale);
     const int nzg = (g.D + HEL_WBP_R - 1) / HEL_WBP_R;
     if (op == OP_BW || op == OP_BWT) {
         if ((long long)nzg * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
         hel_zwin_kernel<<<(g.D + 127) / 128, 128, 0, st>>>(g, o, ang, sp, nview, zw, scan);
         if (int rc = check_cuda("hel_zwin")) return rc;
-        hel_wtab_kernel<<<dim3((nview + 127) / 128, g.D), 128, 0, st>>>(scan, wv, zw, nview, wtab);
+        hel_wtab_kernel<<<dim3((nview + 127) / 128, g.D + 3), 128, 0, st>>>(scan, wv, zw, g.D, nview, wtab_pad);
         if (int rc = check_cuda("hel_wtab")) return rc;
     }
     if (op == OP_BWT) {
@@ -779,6 +781,15 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
         const size_t nvox = (size_t)g.D * g.H * g.W, n = nvox * nbatch;
         hel_prescale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, scale, imgs, nvox, n);
         if (int rc = check_cuda("hel_prescale")) return rc;
+        // The tabulated slices through the TMA cell gather (their weight is
+        // one number per slice and view); the others, if any, added by the
+        // per-voxel gather.  Without a TMA plan the per-voxel gather does all.
+        int rc_tma = -1;
+        if (!g_force_plain) {
+            rc_tma = run_cell_tma<float, float, true>(OP_BWT, g, imgs, out, nbatch, nview, ws, hl.l, vt, st, z0dz,
+                                                      zd0, dvv, (float)g.sod * (float)g.du, wtab_pad);
+            if (rc_tma > 0) return rc_tma;
+        }
         float* imgsT = reinterpret_cast<float*>(ws + hl.imgsT);
         dim3 tg((g.W + 31) / 32, (g.H + 31) / 32, g.D * nbatch);
         transpose_flip_kernel<float><<<tg, dim3(32, 8), 0, st>>>(imgs, imgsT, g.H, g.W, g.H);
@@ -789,8 +800,12 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
         for (int v0 = 0; v0 < total; v0 += 65535) {
             const int nz = std::min(65535, total - v0);
             dim3 grid((g.Nu + 31) / 32, (g.Nv + rows_per_cta - 1) / rows_per_cta, nz);
-            hel_wbpt_kernel<HEL_WBPT_R><<<grid, dim3(32, nwarp), 0, st>>>(g, vt, o, scan, wv, zw, wtab, ang, sp,
-                                                                          imgs, imgsT, out, nview, v0, dvv);
+            if (rc_tma == 0)
+                hel_wbpt_kernel<HEL_WBPT_R, true><<<grid, dim3(32, nwarp), 0, st>>>(
+                    g, vt, o, scan, wv, zw, wtab, ang, sp, imgs, imgsT, out, nview, v0, dvv);
+            else
+                hel_wbpt_kernel<HEL_WBPT_R, false><<<grid, dim3(32, nwarp), 0, st>>>(
+                    g, vt, o, scan, wv, zw, wtab, ang, sp, imgs, imgsT, out, nview, v0, dvv);
             if (int rc = check_cuda("hel_wbpt")) return rc;
         }
         return XR_OK;

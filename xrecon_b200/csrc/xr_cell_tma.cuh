@@ -97,13 +97,19 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
 //
 // HEL: helical scan, the view's z placement and column width come from
 // vt.hel (the volume and detector rows measured from the view's source z).
+// With MODE OP_BWT the helical weighted backprojection's transpose takes the
+// column width cw_p (SOD du) and weighs slice j of view v by
+// zwt[(j + 1) * nview + v] (rows -1 .. D + 1 of the table; the outer ones
+// are zero).
 template <typename TI, typename TO, int R, int NB, int MODE, bool FINE, bool HEL = false>
 __global__ void __launch_bounds__(256, XR_CELL_MINB)
 cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUtensorMap map_rows,
                   const __grid_constant__ CUtensorMap map_cols, const TI* __restrict__ fb_rows,
                   const TI* __restrict__ fb_cols, const int pitch_rows, const int pitch_cols,
                   TO* __restrict__ sino, const int nview, const int view0, const double z0dz_p,
-                  const double zd0_p, const double dvv, const float cw_p, const int BP, const int BZ) {
+                  const double zd0_p, const double dvv, const float cw_p, const int BP, const int BZ,
+                  const float* __restrict__ zwt) {
+    constexpr bool ZW = HEL && MODE == OP_BWT;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // each stage starts on a 128-byte boundary (TMA destination alignment) and
     // holds BZ + 1 rows: the spare row absorbs the look-ahead read of the
@@ -129,7 +135,10 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     const ViewHdr h = vt.hdr[v];
     const double z0dz = HEL ? vt.hel[v].z0dz : z0dz_p;
     const double zd0 = HEL ? vt.hel[v].zd0 : zd0_p;
-    const float cw = HEL ? vt.hel[v].cw : cw_p;
+    const float cw = (HEL && !ZW) ? vt.hel[v].cw : cw_p;
+    // per-slice weight of this view (helical Bw^T): slice j at wz[(j + 1) * nview]
+    const float* __restrict__ wz = ZW ? zwt + v : nullptr;
+    auto slice_w = [&](int j) -> float { return ZW ? __ldg(wz + (size_t)(j + 1) * nview) : 1.0f; };
     const int use_x = h.use_x, nlines = h.nlines, npix = h.npix;
     const size_t ob = (size_t)v * (Nu + 1);
     const double bA0 = vt.bA[ob + kc], bB0 = vt.bB[ob + kc];
@@ -260,8 +269,9 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         float jn = jlf + 1.0f;
                         const TI* ptr = stage + (size_t)s * stage_elems + (pc - win.p0) +
                                         (size_t)(j0 + (int)jlf - win.z0) * BP;
-                        float bcur = band_smem<TI, NB>(ptr, w, np);
-                        float bnext = band_smem<TI, NB>(ptr + BP, w, np);
+                        int jb = j0 + (int)jlf;  // slice of bcur (bnext: jb + 1)
+                        float bcur = band_smem<TI, NB>(ptr, w, np) * slice_w(jb);
+                        float bnext = band_smem<TI, NB>(ptr + BP, w, np) * slice_w(jb + 1);
 #pragma unroll
                         for (int i = 0; i < R; ++i) {
                             const float t1 = fminf(fmaxf(fmaf(bf, (float)(i + 1), f), tlo), thi);
@@ -272,7 +282,8 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                             bcur = adv ? bnext : bcur;
                             jn = adv ? jn + 1.0f : jn;
                             ptr = adv ? ptr + BP : ptr;
-                            bnext = band_smem<TI, NB>(ptr + BP, w, np);
+                            if (ZW) jb = adv ? jb + 1 : jb;
+                            bnext = band_smem<TI, NB>(ptr + BP, w, np) * slice_w(jb + 1);
                             acc[i] += a;
                             tcur = t1;
                         }
@@ -287,7 +298,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         if (j0 >= win.z0) {
                             jabs = j0;
                             ptr = sbase + (size_t)(j0 - win.z0) * BP;
-                            vj = band_smem<TI, NB>(ptr, w, np);
+                            vj = band_smem<TI, NB>(ptr, w, np) * slice_w(jabs);
                         } else {
                             jabs = win.z0 - 1;
                             ptr = sbase - BP;  // address only, advanced before any read
@@ -303,7 +314,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                                 pos = jn;
                                 ++jabs;
                                 ptr += BP;
-                                if (jabs <= win.zlast) { vj = band_smem<TI, NB>(ptr, w, np); jn += 1.0f; }
+                                if (jabs <= win.zlast) { vj = band_smem<TI, NB>(ptr, w, np) * slice_w(jabs); jn += 1.0f; }
                                 else { vj = 0.0f; jn = 3.0e38f; }
                             }
                             if (top > pos) { a = fmaf(top - pos, vj, a); pos = top; }
@@ -313,7 +324,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         // global fallback with bounds checks
                         const TI* base = fbb + (size_t)L * pitch + pc;
                         int j = j0;
-                        vj = ((unsigned)j < (unsigned)g.D) ? band_at(base + (size_t)j * fb_plane, w, np) : 0.0f;
+                        vj = ((unsigned)j < (unsigned)g.D) ? band_at(base + (size_t)j * fb_plane, w, np) * slice_w(j) : 0.0f;
 #pragma unroll
                         for (int i = 0; i < R; ++i) {
                             const float top = fmaf(bf, (float)(i + 1), f);
@@ -323,7 +334,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                                 pos = jn;
                                 ++j;
                                 jn += 1.0f;
-                                vj = ((unsigned)j < (unsigned)g.D) ? band_at(base + (size_t)j * fb_plane, w, np) : 0.0f;
+                                vj = ((unsigned)j < (unsigned)g.D) ? band_at(base + (size_t)j * fb_plane, w, np) * slice_w(j) : 0.0f;
                             }
                             if (top > pos) { a = fmaf(top - pos, vj, a); pos = top; }
                             acc[i] += a;

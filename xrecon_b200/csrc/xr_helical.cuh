@@ -413,20 +413,24 @@ __global__ void hel_zwin_kernel(const Geom g, const HelOpts o, const float* __re
     zw[iz] = z;
 }
 
-// Weight table of the full-turn slices: wtab[iz * nview + v], zero outside
-// the slice's window (rows of the other slices are zero and never read).
+// Weight table of the full-turn slices, rows for slices -1 .. D + 1:
+// wtab[(iz + 1) * nview + v], zero outside the slice's window, for the other
+// slices and for the three slices outside the volume (which the TMA cell
+// gather's staged window and look-ahead reach).
 __global__ void hel_wtab_kernel(const HelScanF* __restrict__ scan, const HelWView* __restrict__ wv,
-                                const HelZ* __restrict__ zw, const int nview, float* __restrict__ wtab) {
+                                const HelZ* __restrict__ zw, const int D, const int nview, float* __restrict__ wtab) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    const int iz = blockIdx.y;
+    const int iz = (int)blockIdx.y - 1;
     if (v >= nview) return;
-    const HelZ z = zw[iz];
     float w = 0.0f;
-    if (z.full && v >= z.vs && v <= z.ve) {
-        const HelScanF s = *scan;
-        w = hw_conjugate(wv[v].beta, 0.0f, z.bc, z.bs, z.be, s.db, s.gmax);
+    if (iz >= 0 && iz < D) {
+        const HelZ z = zw[iz];
+        if (z.full && v >= z.vs && v <= z.ve) {
+            const HelScanF s = *scan;
+            w = hw_conjugate(wv[v].beta, 0.0f, z.bc, z.bs, z.be, s.db, s.gmax);
+        }
     }
-    wtab[(size_t)iz * nview + v] = w;
+    wtab[(size_t)(iz + 1) * nview + v] = w;
 }
 
 // ---------------------------------------------------------------------- Bw
@@ -639,7 +643,9 @@ __global__ void hel_prescale_kernel(const float* __restrict__ img, const float* 
 // every voxel of a column's footprint is weighted by its own redundancy
 // weight (its slice's window, the pixel's fan angle) and read from the
 // normalised image img_s.
-template <int R>
+//   ACCUM: add to `sino` the slices whose weights are not tabulated (the TMA
+//          cell gather wrote the others); without it, every slice
+template <int R, bool ACCUM>
 __global__ void __launch_bounds__(256)
 hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelScanF* __restrict__ scan,
                 const HelWView* __restrict__ wv, const HelZ* __restrict__ zw, const float* __restrict__ wtab,
@@ -651,6 +657,7 @@ hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelSca
     int full_here = 1;
     for (int i = threadIdx.y * 32 + threadIdx.x; i < g.D; i += blockDim.x * blockDim.y) full_here &= zw[i].full;
     const bool allfull = __syncthreads_and(full_here) != 0;
+    if (ACCUM && allfull) return;  // nothing left to add
     const int k = blockIdx.x * 32 + threadIdx.x;
     const int r0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
     const int vb = blockIdx.z + view0;
@@ -718,7 +725,7 @@ hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelSca
                     wt = __ldg(wcol + (size_t)j * nview);
                 } else {
                     const HelZ z = zw[j];
-                    if (v < z.vs || v > z.ve) return 0.0f;
+                    if (v < z.vs || v > z.ve || (ACCUM && z.full)) return 0.0f;
                     wt = z.full ? __ldg(wcol + (size_t)j * nview)
                                 : hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db,
                                             s.gmax, ang, zsrc, nview);
@@ -748,7 +755,10 @@ hel_wbpt_kernel(const Geom g, const ViewTables vt, const HelOpts o, const HelSca
 #pragma unroll
     for (int i = 0; i < R; ++i) {
         const int r = r0 + i;
-        if (r < g.Nv) out[(size_t)r * Nu] = acc[i];
+        if (r < g.Nv) {
+            if (ACCUM) out[(size_t)r * Nu] += acc[i];
+            else out[(size_t)r * Nu] = acc[i];
+        }
     }
 }
 
