@@ -351,12 +351,12 @@ def rebin_measure(P, vol, ang, reps: int = 3):
     ms = timed(lambda: fan_to_parallel_rebin(sino, ang, *args))
     ms_fused = timed(lambda: fan_to_parallel_rebin(sino, ang, *args, filt=filt))
     grid, _ = rebin_grid(ang, WL["Nu"], WL["sod"], du_iso, 0.0, "flat", ang, WL["Nu"], None, 0.0)
-    src = sino.permute(0, 1, 3, 2, 4).reshape(WL["Nv"], 1, WL["V"], WL["Nu"])
+    src = sino.permute(0, 1, 3, 2, 4).reshape(WL["Nv"], 1, ang.numel(), WL["Nu"])
     g4 = grid[None].expand(WL["Nv"], -1, -1, -1)
     ms_torch = timed(lambda: F.grid_sample(src, g4, mode="bilinear", padding_mode="zeros", align_corners=True))
     del sino, src
     return {"ms": ms, "ms_fused_with_ramp_filter": ms_fused, "torch_grid_sample_ms": ms_torch,
-            "samples": WL["V"] * WL["Nv"] * WL["Nu"]}
+            "samples": ang.numel() * WL["Nv"] * WL["Nu"]}
 
 
 HEL = dict(W=512, H=512, D=128, dx=0.7, dz=0.8, Nu=736, Nv=64, du=1.2858, dv=1.0947, sod=595.0, sdd=1085.6,
