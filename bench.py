@@ -591,7 +591,9 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": algo_bytes_op(wl)},
+                     "algorithmic_bytes_per_launch": algo_bytes_op(wl),
+                     # every voxel and detector cell touched once per operator
+                     "compulsory_bytes_per_launch": (nvox(wl) + wl["V"] * wl["Nu"] * wl["Nv"]) * 4},
         "e2e": None if e2e_value is None else {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": vol_bytes,
                                                "d2h_bytes_per_step": vol_bytes},
         "gpu_launches": launches,
