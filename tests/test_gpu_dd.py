@@ -2,7 +2,7 @@
 with the reference's own outputs.
 
 Tolerances (relative L2):
-* against the FP64 oracle: 1e-5 (the north-star bar for FP32);
+* against the FP64 oracle: 1e-5 (the parity bar for FP32);
 * against the reference fixtures: the oracle's own distance from the
   reference plus 1e-5 (the reference's float32 geometry sits 1e-6..1e-4 away
   from the exact operator, see test_oracle_pin.py);
