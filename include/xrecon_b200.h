@@ -28,7 +28,7 @@ typedef enum {
     XR_ERR_INVALID_ARGUMENT = 1,  /* bad geometry, shape, op or dtype      */
     XR_ERR_WORKSPACE = 2,         /* workspace missing or too small         */
     XR_ERR_CUDA = 3,              /* a CUDA launch or runtime call failed   */
-    XR_ERR_UNSUPPORTED = 4        /* valid request this build does not do  */
+    XR_ERR_UNSUPPORTED = 4        /* valid request the library cannot serve */
 } xr_status;
 
 /* Operators, numbered as the six per-dimension bindings of the reference. */
