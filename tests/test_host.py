@@ -194,3 +194,19 @@ def test_helical_validation_without_gpu():
         HelicalProjector3d(**dict(HELICAL_CASES["one_turn"], helical_view_mode="spiral"))
     with pytest.raises(RuntimeError, match="CUDA"):
         P.projection(torch.zeros(1, 1, 16, 32, 32), torch.zeros(3))
+
+
+def test_helical_projector_object_constructor_matches_legacy():
+    """HelicalProjector3d(Volume3d, HelicalConeBeam3d) packs the same options
+    as the legacy keyword form (projector3d.py:323-345)."""
+    from xrecon_b200 import Detector3d, HelicalConeBeam3d, HelicalProjector3d, Volume3d
+    kw = HELICAL_CASES["one_turn"]
+    legacy = HelicalProjector3d(**kw)
+    vol = Volume3d(kw["image_size"], kw["pix_size"], kw["pixshift"])
+    geo = HelicalConeBeam3d(Detector3d(kw["num_det"], kw["det_size"], kw["binshift"]), kw["iso_source"],
+                            kw["source_detector"], "arc", pitch=kw["pitch"], z0=kw["z0"])
+    obj = HelicalProjector3d(vol, geo)
+    np.testing.assert_array_equal(obj.options.numpy(), legacy.options.numpy())
+    assert (obj.pitch, obj.z0) == (8.0, -8.0)
+    with pytest.raises(TypeError):
+        HelicalProjector3d(vol, Detector3d(kw["num_det"], kw["det_size"]))
