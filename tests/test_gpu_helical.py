@@ -35,6 +35,14 @@ def _angles(V, per_turn=96, start=0.05):
     return (np.arange(V) * (2 * np.pi / per_turn) + start).astype(np.float32)
 
 
+def _case_angles(case, V):
+    """Increasing angles, or for the reverse case the same set walked
+    downwards from 2.5 turns."""
+    if case == "reverse":
+        return (5 * np.pi - np.arange(V) * (2 * np.pi / 96)).astype(np.float32)
+    return _angles(V)
+
+
 CASES = {
     "one_turn": (dict(), False),
     "ffs": (dict(), True),
@@ -42,6 +50,9 @@ CASES = {
                        helical_tang_blend=0.6), True),
     "half_scan": (dict(helical_view_mode="half", helical_halfscan_coef=1.1, pitch=12.0, z0=-12.0), False),
     "turns": (dict(helical_view_mode="turns", helical_view_turns=1.5, pitch=6.0, z0=-9.0), False),
+    # decreasing angles (negative angle step): the source still rises by
+    # pitch per turn of |beta|, through z0 + pitch (beta - beta_0) / (2 pi)
+    "reverse": (dict(pitch=-8.0, z0=-9.0), True),
 }
 
 
@@ -70,7 +81,7 @@ def test_helical_operators_match_oracle(cuda, case):
     over, ffs = CASES[case]
     P = _projector(**over)
     V = 240
-    ang = _angles(V)
+    ang = _case_angles(case, V)
     sp = _source_pos(P, ang, ffs)
     x, y = _inputs(P, V)
     opts = P.options.numpy()
