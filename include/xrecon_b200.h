@@ -63,7 +63,8 @@ typedef struct {
     float shift_x, shift_y, shift_z, shift_u, shift_v;
 } xr_geom3d;
 
-/* Device workspace (bytes) that xr_dd2d / xr_dd3d need for these arguments. */
+/* Device workspace (bytes) that xr_dd2d / xr_dd3d need for these arguments,
+ * for any storage dtype. */
 size_t xr_dd2d_workspace_size(int op, const xr_geom2d* geom, int nbatch, int nview);
 size_t xr_dd3d_workspace_size(int op, const xr_geom3d* geom, int nbatch, int nview);
 

@@ -122,7 +122,7 @@ Geom geom_from(const xr_geom2d* p) {
 }
 
 struct Layout {
-    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, volT, volR, sinoS, total;
+    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, volT, volR, volF, sinoS, total;
 };
 
 // ------------------------------------------------------ TMA staging plans
@@ -280,12 +280,17 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
     l.volR = o;
     if (eff == OP_A || eff == OP_BT || eff == OP_BWT) {
         // flipped transpose with a 16-byte-multiple pitch, plus (when the
-        // input rows are not) a padded copy of the input rows
-        const size_t es = dtype_size(dtype_in);
+        // input rows are not) a padded copy of the input rows.  3D images
+        // stored in half precision are widened to FP32 once (volF) and
+        // staged from there, so their transpose and rows are FP32 too.
+        const bool widen = dim3d && dtype_size(dtype_in) == 2;
+        const size_t es = widen ? 4 : dtype_size(dtype_in);
         o = align256(o + (size_t)nbatch * g.D * g.W * round_up(g.H, 8) * es);
         l.volR = o;
         if (dim3d && ((size_t)g.W * es) % 16 != 0)
             o = align256(o + (size_t)nbatch * g.D * g.H * round_up(g.W, 8) * es);
+        l.volF = o;
+        if (widen) o = align256(o + (size_t)nbatch * g.D * g.H * g.W * sizeof(float));
     }
     // voxel-gather ops: the per-view row prefix tables (float2, Nv + 2 rows);
     // the plain kernels' pre-scaled cone A^T sinogram reuses the region
@@ -407,7 +412,9 @@ template <typename TI, typename TO, bool HEL = false>
 int run_cell_tma(int eff, const Geom& g, const TI* in, TO* out, int nbatch, int nview, char* ws, const Layout& l,
                  const ViewTables& vt, cudaStream_t st, double z0dz, double zd0, double dvv, float cw,
                  const float* zwt = nullptr) {
-    if (!std::is_same<TO, TI>::value && !std::is_same<TO, float>::value) return -1;
+    // FP32 images (also widened half-precision ones) go to any output type
+    if (!std::is_same<TI, float>::value && !std::is_same<TO, TI>::value && !std::is_same<TO, float>::value)
+        return -1;
     if (reinterpret_cast<uintptr_t>(in) % 16 != 0) return -1;
     const CellPlan p = HEL ? plan_cell_helical(g) : plan_cell(g);
     if (!p.ok || !encode_fn()) return -1;
@@ -469,7 +476,19 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
     }
     if (eff == OP_A || eff == OP_BT || eff == OP_BWT) {
         if (!g_force_plain) {
-            const int rc = run_cell_tma(eff, g, in, out, nbatch, nview, ws, l, vt, st, z0dz, zd0, dvv, cw);
+            int rc;
+            if constexpr (sizeof(TI) == 2) {
+                // Widen once: the staged walk then reads FP32, which costs
+                // fewer instructions than widening every staged read (the
+                // values, and so the results, are the same)
+                float* vf = reinterpret_cast<float*>(ws + l.volF);
+                const size_t n = (size_t)nbatch * g.D * g.H * g.W;
+                widen_kernel<TI><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, vf, n);
+                if (int e = check_cuda("widen")) return e;
+                rc = run_cell_tma<float, TO>(eff, g, vf, out, nbatch, nview, ws, l, vt, st, z0dz, zd0, dvv, cw);
+            } else {
+                rc = run_cell_tma(eff, g, in, out, nbatch, nview, ws, l, vt, st, z0dz, zd0, dvv, cw);
+            }
             if (rc >= 0) return rc;
         }
         TI* volT = reinterpret_cast<TI*>(ws + l.volT);
@@ -914,7 +933,9 @@ size_t xr_dd2d_workspace_size(int op, const xr_geom2d* geom, int nbatch, int nvi
 size_t xr_dd3d_workspace_size(int op, const xr_geom3d* geom, int nbatch, int nview) {
     if (!geom) return 0;
     const xr::Geom g = xr::geom_from(geom);
-    return xr::layout(1, op, g, nbatch, nview, xr::DT_F32).total;
+    // enough for every storage type (half-precision images add a widened copy)
+    return std::max(xr::layout(1, op, g, nbatch, nview, xr::DT_F32).total,
+                    xr::layout(1, op, g, nbatch, nview, xr::DT_BF16).total);
 }
 
 int xr_dd2d(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,

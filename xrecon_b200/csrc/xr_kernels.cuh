@@ -135,6 +135,13 @@ __global__ void transpose_flip_kernel(const T* __restrict__ in, T* __restrict__ 
     }
 }
 
+// Half-precision image to FP32, element for element.
+template <typename T>
+__global__ void widen_kernel(const T* __restrict__ in, float* __restrict__ out, const size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = ld(in + i);
+}
+
 // Copy image planes into a row pitch that is a multiple of 16 bytes (TMA
 // stride rule); the padding columns are never read inside the image.
 template <typename T>
