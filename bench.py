@@ -544,27 +544,28 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         e2e_value = world * nvox() * nv / t_e2e / 1e9
     vol_bytes = vol.numel() * 4
 
-    # BF16-stored form of the same step (volume and sinogram in BF16, FP32
-    # accumulation), reported beside the FP32 number.
-    bf = {}
+    # BF16- and FP16-stored forms of the same step (volume and sinogram in
+    # half precision, FP32 accumulation), reported beside the FP32 number.
+    half = {}
     if not args.no_bf16:
-        vol16 = vol.to(torch.bfloat16)
-        for _ in range(1):
-            step(vol16)
-        torch.cuda.synchronize()
-        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        nb = max(1, min(args.steps, 3))
-        g0.record(stream)
-        for _ in range(nb):
-            out16 = step(vol16)
-        g1.record(stream)
-        torch.cuda.synchronize()
-        t16 = g0.elapsed_time(g1) / 1e3 / nb
         ref32 = step(vol)
-        rel = float((out16.float() - ref32).norm() / ref32.norm())
-        bf = {"value": world * nvox() * nv / t16 / 1e9, "unit": UNIT, "ms_per_step": t16 * 1e3,
-              "rel_l2_vs_fp32": rel}
-        del vol16, out16, ref32
+        for name, dt in (("bf16", torch.bfloat16), ("fp16", torch.float16)):
+            vol16 = vol.to(dt)
+            step(vol16)
+            torch.cuda.synchronize()
+            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            nb = max(1, min(args.steps, 3))
+            g0.record(stream)
+            for _ in range(nb):
+                out16 = step(vol16)
+            g1.record(stream)
+            torch.cuda.synchronize()
+            t16 = g0.elapsed_time(g1) / 1e3 / nb
+            rel = float((out16.float() - ref32).norm() / ref32.norm())
+            half[name] = {"value": world * nvox() * nv / t16 / 1e9, "unit": UNIT, "ms_per_step": t16 * 1e3,
+                          "rel_l2_vs_fp32": rel}
+            del vol16, out16
+        del ref32
 
     hbm, src = peaks()
     dom_t = max(t_a, t_b)
@@ -599,8 +600,7 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if bf:
-        line["bf16"] = bf
+    line.update(half)
     if not args.no_ops:
         line["operators"] = operator_times(P, vol, ang, nv)
     if not args.no_ragged and world == 1:
@@ -626,7 +626,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--no-bf16", action="store_true", help="skip the BF16-storage measurement")
+    ap.add_argument("--no-bf16", action="store_true", help="skip the BF16/FP16-storage measurements")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged 2D batch measurement")
     ap.add_argument("--no-ops", action="store_true", help="skip the per-operator timings")
