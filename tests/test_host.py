@@ -92,8 +92,10 @@ def test_workspace_sizes_and_validation_without_gpu():
     g = _native.geom3d_from_values(vals)
     nb_a = lib.xr_dd3d_workspace_size(0, ctypes.byref(g), 1, 1440)
     nb_at = lib.xr_dd3d_workspace_size(1, ctypes.byref(g), 1, 1440)
-    # forward needs the flipped image copy, cone A^T the scaled sinogram
-    assert nb_a > 512 * 512 * 256 * 4
+    # forward needs the flipped image copy (FP32 for every storage type, since
+    # half-precision images are widened once) plus the widened copy itself;
+    # cone A^T the scaled sinogram
+    assert nb_a > 2 * 512 * 512 * 256 * 4
     assert nb_at > 1440 * 256 * 1024 * 4
     bad = _native.geom3d_from_values(vals)
     bad.dx = -1.0
