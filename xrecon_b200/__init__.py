@@ -3,9 +3,11 @@
 Drop-in for the projector path of XRecon: ``Projector2d`` / ``Projector3d``
 with projection, backprojection, weighted backprojection, their transposes
 and filtered backprojection (FBP / FDK) for parallel, fan/cone-flat and
-fan/cone-arc geometries, on hand-written sm_100a CUDA kernels behind the C ABI
-of ``include/xrecon_b200.h``.  ``xrecon_b200.backend`` replaces the native
-module ``xrecon_C``.
+fan/cone-arc geometries, and ``HelicalProjector3d`` (helical arc-detector
+scans with per-view source offsets, helical FDK), on hand-written sm_100a
+CUDA kernels behind the C ABI of ``include/xrecon_b200.h``.
+``xrecon_b200.backend`` replaces the native module ``xrecon_C``;
+``xrecon_b200.rebin`` has the fan/helical -> parallel rebinning.
 """
 from .geometry import (ConeBeam3d, Detector2d, Detector3d, FanBeam2d, HelicalConeBeam3d, ParallelBeam2d,
                        ParallelBeam3d, Volume2d, Volume3d)
