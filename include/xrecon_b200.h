@@ -259,6 +259,30 @@ int xr_ragged2d_run(const xr_ragged2d_plan* plan, int project, int a_cols_log2, 
 int xr_ragged2d_plan_info(const xr_ragged2d_plan* plan, int* grid, int* tiles10);
 void xr_ragged2d_plan_destroy(xr_ragged2d_plan* plan);
 
+/*
+ * DICOM-CT-PD projection series reader (host code; no GPU, no stream).
+ * Replaces the per-file loop of load_projection_stack
+ * (xrecon/utils/mayo.py:145-170, pydicom.dcmread per view): reads the
+ * `nfiles` files, spread over `nthreads` threads (<= 0: one per core), and
+ * writes
+ *   sino  [nfiles, ceil(cols / row_stride), ceil(rows / col_stride)] float32:
+ *         stored pixel [c * col_stride, r * row_stride] rescaled as
+ *         float32(raw) * float32(RescaleSlope) + float32(RescaleIntercept)
+ *         (two float32 roundings), at [view, r, c];
+ *   views [nfiles, 5] float32: angle (7031,1001), source z (7031,1002),
+ *         shift z (7033,100B), shift angle (7033,100C), shift radius
+ *         (7033,100D); absent shifts are 0.
+ * `rows` x `cols` is the stored pixel matrix (Rows = detector columns,
+ * Columns = detector rows) every file must have.  Files in implicit or
+ * explicit VR little endian with native single-frame 8/16/32-bit pixels and
+ * single-valued tags are read; any other file (deflated or compressed
+ * encodings, multi-valued or oddly typed tags, a different matrix, an
+ * unreadable or malformed file) stops the call with XR_ERR_UNSUPPORTED and
+ * its index in *failed_file, for a general reader to handle or reject.
+ */
+int xr_ctpd_load(const char* const* paths, int nfiles, int rows, int cols, int col_stride, int row_stride,
+                 int nthreads, float* sino, float* views, int* failed_file);
+
 /* Number of CUDA kernels this library has launched in this process (all
  * devices and threads). */
 unsigned long long xr_launch_count(void);

@@ -89,6 +89,9 @@ def lib():
     L.xr_helical3d.restype = c_int
     L.xr_helical3d.argtypes = [c_int, ctypes.POINTER(Geom3d), ctypes.POINTER(HelicalOpts), c_void_p, c_void_p,
                                c_void_p, c_void_p, c_int, c_int, c_void_p, c_size_t, c_void_p]
+    L.xr_ctpd_load.restype = c_int
+    L.xr_ctpd_load.argtypes = [ctypes.POINTER(ctypes.c_char_p)] + [c_int] * 6 + [c_void_p, c_void_p,
+                                                                                 ctypes.POINTER(c_int)]
     L.xr_launch_count.restype = ctypes.c_ulonglong
     L.xr_launch_count.argtypes = []
     L.xr_version.restype = ctypes.c_char_p

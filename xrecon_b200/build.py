@@ -14,10 +14,12 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "libxrecon_b200.so"
 SOURCES = [PKG / "csrc" / "xr_abi.cu"]
-DEPS = SOURCES + sorted((PKG / "csrc").glob("*.cuh")) + [ROOT / "include" / "xrecon_b200.h"]
+DEPS = SOURCES + sorted((PKG / "csrc").glob("*.cuh")) + sorted((PKG / "csrc").glob("*.hpp")) + \
+    [ROOT / "include" / "xrecon_b200.h"]
 NVCC = os.environ.get("NVCC", str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "bin" / "nvcc"))
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-         "-Xcompiler", "-fPIC", "-shared", f"-I{ROOT / 'include'}"]
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared", f"-I{ROOT / 'include'}",
+         "-lpthread"]
 
 
 def stale() -> bool:

@@ -22,6 +22,7 @@
 #include "xr_sysmat.cuh"
 #include "xr_rebin.cuh"
 #include "xr_helical.cuh"
+#include "xr_ctpd.hpp"
 #include "../../include/xrecon_b200.h"
 
 
@@ -1276,6 +1277,44 @@ int xr_ragged2d_plan_info(const xr_ragged2d_plan* P, int* grid, int* tiles10) {
 }
 
 void xr_ragged2d_plan_destroy(xr_ragged2d_plan* plan) { delete plan; }
+
+int xr_ctpd_load(const char* const* paths, int nfiles, int rows, int cols, int col_stride, int row_stride,
+                 int nthreads, float* sino, float* views, int* failed_file) {
+    if (failed_file) *failed_file = -1;
+    if (!paths || !sino || !views || nfiles < 1 || rows < 1 || cols < 1 || col_stride < 1 || row_stride < 1)
+        return xr::fail(XR_ERR_INVALID_ARGUMENT, "xr_ctpd_load: null pointer or non-positive size");
+    for (int i = 0; i < nfiles; ++i)
+        if (!paths[i]) return xr::fail(XR_ERR_INVALID_ARGUMENT, "xr_ctpd_load: null path %d", i);
+    ctpd::Job job;
+    job.paths = paths;
+    job.nfiles = nfiles;
+    job.rows = rows;
+    job.cols = cols;
+    job.cs = col_stride;
+    job.rs = row_stride;
+    job.nv = (cols + row_stride - 1) / row_stride;
+    job.nu = (rows + col_stride - 1) / col_stride;
+    job.sino = sino;
+    job.views = views;
+    int T = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
+    T = std::max(1, std::min({T, nfiles, 64}));
+    std::vector<std::thread> pool;
+    pool.reserve(T - 1);
+    try {
+        for (int t = 1; t < T; ++t) pool.emplace_back(ctpd::worker, &job);
+    } catch (const std::exception&) {
+        // fewer threads than asked: the ones started and this one share the files
+    }
+    ctpd::worker(&job);
+    for (auto& th : pool) th.join();
+    const int bad = job.failed.load();
+    if (bad >= 0) {
+        if (failed_file) *failed_file = bad;
+        return xr::fail(XR_ERR_UNSUPPORTED, "xr_ctpd_load: file %d (%s) is not a file this reader takes", bad,
+                        paths[bad]);
+    }
+    return XR_OK;
+}
 
 const char* xr_version(void) { return "xrecon_b200 0.1.0 (sm_100a)"; }
 
