@@ -592,7 +592,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
                     const char* cb = reinterpret_cast<const char*>(
                         reinterpret_cast<uintptr_t>(tvb) +
                         (uintptr_t)((long long)(r0 + 1) * Nu8 + (long long)col * 8 - 0x4B400000ll * (long long)Nu8));
-                    const float wk = wf * lf * __frcp_rn(fib);
+                    const float wk = __fdividef(wf * lf, fib);
                     // rows -1 .. Nv of the detector (table rows 0 .. Nv + 1)
                     const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
                     float gprev = 0.0f;

@@ -221,7 +221,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                 const char* cb = reinterpret_cast<const char*>(
                     reinterpret_cast<uintptr_t>(tvb) +
                     (uintptr_t)((long long)(r0 + 1) * Nu8 + (long long)col * 8 - 0x4B400000ll * (long long)Nu8));
-                const float wk = wf * lf * __frcp_rn(fib);
+                const float wk = __fdividef(wf * lf, fib);
                 // rows the run reaches (local), inside [0, Nv - 1] in every active lane?
                 const bool inside = (u0 >= 0.0) && (u0 + R * ib <= (double)Nv - 1.0);
                 float gprev = 0.0f;
