@@ -115,6 +115,23 @@ def test_workspace_sizes_and_validation_without_gpu():
     assert rc == 1
 
 
+def test_projection_staging_plans_without_gpu():
+    """The host planner of the TMA projection (no GPU needed): the window box
+    the 512x512x256 / 1024x256 cone-flat workload is launched with, the
+    fine-row walk for rows shorter than a voxel and the general walk for rows
+    longer than one."""
+    opts = load_golden("options")
+    c5 = _native.cell_plan(_native.geom3d_from_values(opts["c5_3d_flat"]))
+    assert c5 == dict(ok=True, box_pixels=48, box_z=115, rows_per_thread=16, fine=True), c5
+    c2 = _native.cell_plan(_native.geom3d_from_values(opts["c2_3d_flat"]))
+    assert c2["ok"] and c2["box_pixels"] % 8 == 0 and c2["rows_per_thread"] == 8
+    coarse = _native.cell_plan(_native.geom3d_from_values(
+        G.pack_options3d(G.Volume3d((64, 64, 24), 1.0), G.ConeBeam3d(G.Detector3d((40, 12), 2.5), 300., 600., "flat"))))
+    assert coarse["ok"] and not coarse["fine"], coarse
+    # the plan is a pure function of the geometry
+    assert _native.cell_plan(_native.geom3d_from_values(opts["c5_3d_flat"])) == c5
+
+
 def test_cpu_tensors_are_rejected():
     P = Projector3d(G.Volume3d((8, 8, 4), 1.0), G.ConeBeam3d(G.Detector3d((12, 6), 1.5), 500., 1000., "flat"))
     with pytest.raises(RuntimeError, match="CUDA"):
