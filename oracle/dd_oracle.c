@@ -2,7 +2,7 @@
  * dd_oracle.c -- FP64 CPU restatement of XRecon's distance-driven (DD)
  * operators.  TEST INFRASTRUCTURE ONLY: the product never links, loads or
  * calls this file; tests/, __graft_entry__.smoke() and bench.py's CPU
- * baseline use it as the checker.
+ * baseline use it as the reference result to compare against.
  *
  * What it restates (paths relative to the XRecon project root):
  *   geometry conventions   include/types.h:35-119, include/xrmath.h:8-226

@@ -1,7 +1,7 @@
 """The reference's own CPU operators (XRecon ``src/cpu``), loaded from
 ``oracle/_ref/libxrecon_ref_cpu.so`` built by ``build_oracle.build_ref``.
 
-TEST INFRASTRUCTURE ONLY (checker and CPU reference arm of ``bench.py``).
+TEST INFRASTRUCTURE ONLY (test comparisons and the CPU reference arm of ``bench.py``).
 
 :class:`RefXreconC` mirrors the surface of the reference's ``xrecon_C``
 extension (``src/api/torch_binding.cpp:615-638``) on CPU tensors, so the
