@@ -1,7 +1,7 @@
-"""Multi-rank host logic on CPU: gloo, world size 2, the FP64 oracle as the
-operator.  View-sharded projection + all-gather + slab-sharded
-backprojection equals the single-process result; shards cover everything
-once; slab geometries reproduce the full volume's voxels (to the float32
+"""Multi-rank host logic on CPU: gloo, world sizes 2 and 3, the FP64 oracle
+as the operator.  View-sharded projection + all-gather + slab-sharded
+backprojection equals the single-process result (with 3 ranks the 16 views
+and 11 slices split unevenly); shards cover everything once; slab geometries reproduce the full volume's voxels (to the float32
 rounding of the slab's z shift in the packed options, ~2e-7 relative)."""
 import os
 import socket
@@ -68,13 +68,14 @@ def _worker(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_two_rank_view_and_slab_sharding_matches_single_process():
+@pytest.mark.parametrize("world", [2, 3])
+def test_view_and_slab_sharding_matches_single_process(world):
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     results = [q.get(timeout=120) for _ in procs]
@@ -88,7 +89,7 @@ def test_two_rank_view_and_slab_sharding_matches_single_process():
     for rank, z0, z1, slab, sino, t in results:
         np.testing.assert_allclose(sino, sino_ref, rtol=1e-12, atol=1e-12 * np.abs(sino_ref).max())
         out[:, :, z0:z1] = slab
-        assert t == 2.0  # max over ranks
+        assert t == float(world)  # max over ranks
     np.testing.assert_allclose(out, vol_ref, rtol=1e-6, atol=1e-6 * np.abs(vol_ref).max())
 
 

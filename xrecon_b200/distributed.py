@@ -76,16 +76,26 @@ def project_views(op: Callable, vol: torch.Tensor, options, angles: torch.Tensor
 
 def gather_views(sino_local: torch.Tensor, nview: int, group=None) -> torch.Tensor:
     """All-gather view shards (as produced by ``project_views``) into the
-    full sinogram [B, C, V, ...] on every rank."""
+    full sinogram [B, C, V, ...] on every rank.
+
+    One all-gather of equal-sized buffers: when the views do not split
+    evenly, every shard is padded to the largest one and trimmed after the
+    exchange (collectives such as gloo's all-gather need equal sizes)."""
     world = dist.get_world_size(group)
-    shards = []
-    for r in range(world):
-        vs = view_shard(nview, r, world)
-        shards.append(torch.empty((sino_local.shape[0], sino_local.shape[1], vs.stop - vs.start)
-                                  + tuple(sino_local.shape[3:]), dtype=sino_local.dtype,
-                                  device=sino_local.device))
-    dist.all_gather(shards, sino_local.contiguous(), group=group)
-    return torch.cat(shards, dim=2)
+    rank = dist.get_rank(group)
+    counts = [view_shard(nview, r, world) for r in range(world)]
+    counts = [vs.stop - vs.start for vs in counts]
+    if sino_local.shape[2] != counts[rank]:
+        raise ValueError(f"rank {rank} holds {sino_local.shape[2]} views, its shard has {counts[rank]}")
+    vmax = max(counts)
+    shape = (sino_local.shape[0], sino_local.shape[1], vmax) + tuple(sino_local.shape[3:])
+    send = sino_local.contiguous()
+    if counts[rank] != vmax:
+        send = torch.zeros(shape, dtype=sino_local.dtype, device=sino_local.device)
+        send[:, :, :counts[rank]] = sino_local
+    bufs = [torch.empty(shape, dtype=sino_local.dtype, device=sino_local.device) for _ in range(world)]
+    dist.all_gather(bufs, send, group=group)
+    return torch.cat([b[:, :, :n] for b, n in zip(bufs, counts)], dim=2)
 
 
 def backproject_slab(op: Callable, sino: torch.Tensor, options, angles: torch.Tensor, rank: int,
