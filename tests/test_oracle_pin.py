@@ -77,6 +77,52 @@ def test_oracle_reference_library_when_present():
     assert rel_l2(b, a) < 1e-5
 
 
+def _random_case(rng, dim, scan):
+    """A seeded small geometry: odd sizes, anisotropic spacings, volume and
+    detector shifts, source outside the volume, random angles plus two on
+    the 45-degree axis switch; random image and sinogram."""
+    from xrecon_b200 import geometry as G
+    W, H = (int(v) for v in rng.integers(8, 33, 2))
+    D, Nu, Nv, V = int(rng.integers(4, 13)), int(rng.integers(8, 49)), int(rng.integers(4, 17)), int(rng.integers(4, 13))
+    dx, dy, dz = rng.uniform(0.6, 1.6, 3)
+    du, dv = rng.uniform(0.8, 2.0, 2)
+    sod = rng.uniform(300, 600)
+    sdd = sod * rng.uniform(1.5, 2.5)
+    sh = tuple(rng.uniform(-3, 3, 3))
+    shu, shv = rng.uniform(-2, 2, 2)
+    ang = np.concatenate([rng.uniform(0, 2 * np.pi, V), [np.pi / 4, 5 * np.pi / 4]]).astype(np.float32)
+    if dim == 3:
+        det = G.Detector3d((Nu, Nv), (du, dv), (shu, shv))
+        geo = G.ParallelBeam3d(det) if scan == "parallel" else G.ConeBeam3d(det, sod, sdd, scan)
+        o = np.array(G.pack_options3d(G.Volume3d((W, H, D), (dx, dy, dz), sh), geo), np.float32)
+        img, sino = rng.random((1, 1, D, H, W)), rng.random((1, 1, ang.size, Nv, Nu))
+    else:
+        det = G.Detector2d(Nu, du, shu)
+        geo = G.ParallelBeam2d(det) if scan == "parallel" else G.FanBeam2d(det, sod, sdd, scan)
+        o = np.array(G.pack_options2d(G.Volume2d((W, H), (dx, dy), sh[:2]), geo), np.float32)
+        img, sino = rng.random((1, 1, H, W)), rng.random((1, 1, ang.size, Nu))
+    return o, ang, img.astype(np.float32), sino.astype(np.float32)
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_matches_reference_library_on_random_geometries(dim, scan):
+    """Where oracle/_ref was built: 40 seeded random geometries, all six
+    operators, the oracle against the reference's own CPU kernels, within the
+    reference's float32-geometry distance (TOL)."""
+    from oracle import refcpu
+    if not refcpu.available():
+        pytest.skip("reference CPU library not built")
+    f, g = (O.dd2d, refcpu.dd2d) if dim == 2 else (O.dd3d, refcpu.dd3d)
+    for seed in range(40):
+        o, ang, img, sino = _random_case(np.random.default_rng(1000 + seed), dim, scan)
+        for op in OPS:
+            x = img if op in IMG_IN else sino
+            exact = f(op, x, o, ang)
+            assert np.linalg.norm(exact) > 0, (seed, op)
+            assert rel_l2(g(op, x, o, ang), exact) < TOL[scan], (seed, op)
+
+
 @pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_reference_system_matrix_is_the_oracle_projection(dim, scan):
