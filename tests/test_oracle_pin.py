@@ -125,6 +125,21 @@ def test_oracle_matches_reference_library_on_random_geometries(dim, scan):
 
 @pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
 @pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_adjoint_pairs_on_random_geometries(dim, scan):
+    """The oracle's transposes are exact adjoints (FP64) on 20 seeded random
+    geometries per dimension and scan type, not only on the fixtures'."""
+    fn = O.dd2d if dim == 2 else O.dd3d
+    for seed in range(20):
+        o, ang, img, sino = _random_case(np.random.default_rng(2000 + seed), dim, scan)
+        x, y = img.astype(np.float64), sino.astype(np.float64)
+        for fwd, adj in (("A", "AT"), ("BT", "B"), ("BWT", "BW")):
+            lhs = float(np.sum(fn(fwd, x, o, ang) * y))
+            rhs = float(np.sum(x * fn(adj, y, o, ang)))
+            assert abs(lhs - rhs) <= 1e-12 * abs(lhs), (seed, fwd, adj, lhs, rhs)
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
 def test_reference_system_matrix_is_the_oracle_projection(dim, scan):
     """The reference's sparse projection matrix (fixture) times an image is
     the oracle's projection: pins the matrix conventions (rows: view, detector
