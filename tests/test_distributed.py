@@ -44,6 +44,25 @@ def test_slab_options_reproduce_full_volume():
     np.testing.assert_allclose(parts[2], full[:, :, zs2], rtol=1e-6, atol=1e-6 * np.abs(full).max())
 
 
+def test_more_ranks_than_slices_leaves_empty_slabs():
+    g = load_golden("dd3d_flat")
+    opts, ang, sino = g["options"], torch.from_numpy(g["angles"]), torch.from_numpy(g["sino"])
+    D, H, W = int(opts[2]), int(opts[1]), int(opts[0])
+    world = D + 3
+    calls = []
+
+    def op(x, options, angles):
+        calls.append(int(float(options[2])))
+        return torch.zeros((x.shape[0], x.shape[1], int(float(options[2])), H, W))
+
+    depth = 0
+    for r in range(world):
+        zs, slab = XD.backproject_slab(op, sino, opts, ang, r, world)
+        assert slab.shape == (1, 1, zs.stop - zs.start, H, W)
+        depth += slab.shape[2]
+    assert depth == D and calls == [1] * D
+
+
 def _oracle_op(name):
     def op(x, options, angles):
         o = np.asarray(options.tolist() if isinstance(options, torch.Tensor) else options, np.float32)

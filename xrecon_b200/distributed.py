@@ -101,9 +101,13 @@ def gather_views(sino_local: torch.Tensor, nview: int, group=None) -> torch.Tens
 def backproject_slab(op: Callable, sino: torch.Tensor, options, angles: torch.Tensor, rank: int,
                      world: int) -> tuple[slice, torch.Tensor]:
     """This rank's z-slab of ``op`` (B or Bw) applied to the full sinogram:
-    (slab slice, [B, C, D_rank, H, W])."""
+    (slab slice, [B, C, D_rank, H, W]).  With more ranks than slices, a rank
+    without slices gets an empty slab and ``op`` is not called."""
     D = int(float(options[2]))
     zs = slab_shard(D, rank, world)
+    if zs.stop == zs.start:
+        H, W = int(float(options[1])), int(float(options[0]))
+        return zs, torch.zeros((sino.shape[0], sino.shape[1], 0, H, W), dtype=sino.dtype, device=sino.device)
     opts = slab_options(options, zs)
     if isinstance(options, torch.Tensor):
         opts = torch.tensor(opts, dtype=options.dtype, device=options.device)
