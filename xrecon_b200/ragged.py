@@ -67,6 +67,12 @@ class RaggedFBP2d:
     (radians, 1-D).  ``__call__(images)`` takes a list of [H_i, W_i] (or
     [1, 1, H_i, W_i]) float32 CUDA tensors and returns (sinograms,
     reconstructions), each a list of views into the batch buffers.
+
+    Each reconstruction is ``projectors[i].filtered_backprojection`` of its
+    sinogram with that method's defaults: the projector's own filter and
+    cosine weight, no Parker weights, and the redundant-scan factor 1/2 on
+    the mean angular step.  Short scans that need Parker weights go through
+    ``Projector2d.filtered_backprojection(..., parker=True)`` instead.
     """
 
     def __init__(self, projectors: Sequence[Projector2d], angles: Sequence[torch.Tensor],
