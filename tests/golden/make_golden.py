@@ -25,7 +25,10 @@ from the reference's code path on CPU:
   (xrecon/utils/rebin.py, pure torch) on seeded inputs
   (``python tests/golden/make_golden.py rebin``);
 * helical_host.npz: HelicalProjector3d's packed options, weight, filter and
-  source positions (``python tests/golden/make_golden.py helical_host``).
+  source positions (``python tests/golden/make_golden.py helical_host``);
+* autograd{2,3}d_<geom>.npz: gradients of the reference's twelve autograd
+  Functions (xrecon/projector/functions.py:96-302) for a seeded input and
+  upstream gradient (``python tests/golden/make_golden.py autograd``).
 The reference's helical operators themselves are CUDA only; their outputs
 are recorded on a GPU by tests/golden/make_golden_helical.py.
 """
@@ -258,6 +261,50 @@ def make_helical_host():
     print("helical host fixtures written to", HERE)
 
 
+FUNCTIONS = {"A": "Projection", "AT": "ProjectionTranspose", "B": "BackProjection",
+             "BW": "WeightedBackProjection", "BT": "BackProjectionTranspose",
+             "BWT": "WeightedBackProjectionTranspose"}
+
+
+def make_autograd():
+    """autograd{2,3}d_<geom>.npz: for each of the reference's autograd
+    Functions, a seeded input x, an upstream gradient u and
+    d(sum(F(x) * u))/dx, taken by torch.autograd through the reference's own
+    backward (its partner transpose binding, served here by its CPU
+    kernels)."""
+    P2, P3, G, _ = import_reference()
+    import xrecon.projector.functions as RF
+    rng = np.random.default_rng(20261204)
+    for dim in (2, 3):
+        for scan in ("parallel", "flat", "arc"):
+            if dim == 2:
+                det = G.Detector2d(31, 1.6, 0.3)
+                geo = G.ParallelBeam2d(det) if scan == "parallel" else G.FanBeam2d(det, 450.0, 900.0, scan)
+                P = P2(G.Volume2d((21, 17), (1.0, 1.2), (0.4, -0.3)), geo)
+                img_shape, sino_of = (2, 1, 17, 21), (lambda V: (2, 1, V, 31))
+            else:
+                det = G.Detector3d((27, 9), (1.4, 1.2), (0.3, -0.4))
+                geo = G.ParallelBeam3d(det) if scan == "parallel" else G.ConeBeam3d(det, 450.0, 900.0, scan)
+                P = P3(G.Volume3d((15, 13, 7), (1.0, 1.1, 0.9), (0.2, 0.3, -0.4)), geo)
+                img_shape, sino_of = (1, 1, 7, 13, 15), (lambda V: (1, 1, V, 9, 27))
+            ang = angles_set(9, 0.2)
+            at = torch.from_numpy(ang)
+            out = {"options": P.options.numpy(), "angles": ang}
+            for op, name in FUNCTIONS.items():
+                in_shape, out_shape = ((img_shape, sino_of(ang.size)) if op in ("A", "BT", "BWT")
+                                       else (sino_of(ang.size), img_shape))
+                x = torch.from_numpy(rng.random(in_shape).astype(np.float32)).requires_grad_(True)
+                u = torch.from_numpy(rng.random(out_shape).astype(np.float32))
+                fn = getattr(RF, f"{name}{dim}d")
+                y = fn.apply(x, P.options, at)
+                (grad,) = torch.autograd.grad((y * u).sum(), x)
+                out[f"{op}_x"] = x.detach().numpy()
+                out[f"{op}_u"] = u.numpy()
+                out[f"{op}_grad"] = grad.numpy()
+            np.savez_compressed(HERE / f"autograd{dim}d_{scan}.npz", **out)
+    print("autograd fixtures written to", HERE)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["sysmat"]:
         make_sysmat()
@@ -265,6 +312,8 @@ if __name__ == "__main__":
         make_rebin()
     elif sys.argv[1:] == ["helical_host"]:
         make_helical_host()
+    elif sys.argv[1:] == ["autograd"]:
+        make_autograd()
     else:
         main()
         make_sysmat()

@@ -64,6 +64,25 @@ def test_oracle_fdk_matches_reference(case):
     assert rel_l2(got, g["recon"]) < tol
 
 
+ADJOINT = {"A": "AT", "AT": "A", "B": "BT", "BT": "B", "BW": "BWT", "BWT": "BW"}
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_transposes_are_the_reference_autograd_gradients(dim, scan):
+    """The gradients the reference's own autograd Functions return (their
+    backward is the partner transpose binding, functions.py:96-302; fixtures
+    from tests/golden/make_golden.py autograd) equal the oracle's transposes
+    of the upstream gradient.  The CUDA Functions' backward is checked
+    against the same oracle transposes on the GPU."""
+    g = load_golden(f"autograd{dim}d_{scan}")
+    fn = O.dd2d if dim == 2 else O.dd3d
+    for op, adj in ADJOINT.items():
+        assert g[f"{op}_grad"].shape == g[f"{op}_x"].shape
+        exact = fn(adj, g[f"{op}_u"], g["options"], g["angles"])
+        assert rel_l2(g[f"{op}_grad"], exact) < TOL[scan], (op, adj)
+
+
 def test_oracle_reference_library_when_present():
     """Where oracle/_ref was built, run a fresh seeded case through both."""
     from oracle import refcpu
