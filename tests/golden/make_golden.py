@@ -26,6 +26,9 @@ from the reference's code path on CPU:
   (``python tests/golden/make_golden.py rebin``);
 * helical_host.npz: HelicalProjector3d's packed options, weight, filter and
   source positions (``python tests/golden/make_golden.py helical_host``);
+* filters_sweep.npz: the reference's filter tables (filters.py:19-71) for
+  odd and even detector counts and several spacings
+  (``python tests/golden/make_golden.py filters``);
 * autograd{2,3}d_<geom>.npz: gradients of the reference's twelve autograd
   Functions (xrecon/projector/functions.py:96-302) for a seeded input and
   upstream gradient (``python tests/golden/make_golden.py autograd``).
@@ -261,6 +264,21 @@ def make_helical_host():
     print("helical host fixtures written to", HERE)
 
 
+FILTER_SWEEP = [(n, du) for n in (7, 64, 255, 1024) for du in (0.75, 2.3)]
+
+
+def make_filters():
+    """filters_sweep.npz: filter_generate(Nu, du, name) of the reference for
+    FILTER_SWEEP x the five filter names, keyed "<name>_<Nu>_<du>"."""
+    _, _, _, F = import_reference()
+    out = {}
+    for name in ("ramp", "shepplogan", "cosine", "hamming", "hann"):
+        for n, du in FILTER_SWEEP:
+            out[f"{name}_{n}_{du}"] = F.filter_generate(n, du, name, torch.float32).numpy()
+    np.savez_compressed(HERE / "filters_sweep.npz", **out)
+    print("filter sweep written to", HERE)
+
+
 FUNCTIONS = {"A": "Projection", "AT": "ProjectionTranspose", "B": "BackProjection",
              "BW": "WeightedBackProjection", "BT": "BackProjectionTranspose",
              "BWT": "WeightedBackProjectionTranspose"}
@@ -314,6 +332,8 @@ if __name__ == "__main__":
         make_helical_host()
     elif sys.argv[1:] == ["autograd"]:
         make_autograd()
+    elif sys.argv[1:] == ["filters"]:
+        make_filters()
     else:
         main()
         make_sysmat()

@@ -41,6 +41,19 @@ def test_filter_tables_match_reference():
         np.testing.assert_allclose(got, ref[name], rtol=2e-6, atol=1e-7 * np.abs(ref[name]).max(), err_msg=name)
 
 
+def test_filter_tables_match_reference_across_sizes():
+    """Odd and even detector counts up to 1024 and two spacings: the windowed
+    tables come from an FFT in FP64 on both sides, so they agree to the
+    float32 rounding (1e-7 of the peak)."""
+    ref = load_golden("filters_sweep")
+    assert len(ref) == 40
+    for key in sorted(ref):
+        name, n, du = key.split("_")
+        got = filters.filter_generate(int(n), float(du), name, torch.float32).numpy()
+        assert got.shape == ref[key].shape, key
+        np.testing.assert_allclose(got, ref[key], rtol=0, atol=3e-7 * np.abs(ref[key]).max(), err_msg=key)
+
+
 def test_fbp_host_tables_match_reference():
     for case in ("flat_ramp", "arc_ramp", "parallel_shepplogan", "flat_hann"):
         g = load_golden(f"fbp2d_{case}")
