@@ -84,6 +84,25 @@ def test_parker_full_scan_is_ones():
         parker_weights(ang[:100], torch.linspace(-0.2, 0.2, 16), 16)
 
 
+@pytest.mark.parametrize("gamma_max,overscan", [(0.1, 0.0), (0.3, 0.0), (0.3, 0.2), (0.45, 0.05)])
+def test_parker_weights_sum_to_one_on_conjugate_rays(gamma_max, overscan):
+    """The defining property of the short-scan weights (projector.py:208-246,
+    Parker's sin^2 ramps with the overscan generalisation): a ray (beta,
+    gamma) and its conjugate (beta + pi + 2 gamma, -gamma), both inside the
+    scan, carry weights that add up to one.  FP64, seeded random rays."""
+    rng = np.random.default_rng(17)
+    R = np.pi + 2 * gamma_max + 2 * overscan
+    for _ in range(200):
+        g = rng.uniform(-gamma_max, gamma_max)
+        b = rng.uniform(0, R - np.pi - 2 * g)  # so that the conjugate lies inside the scan too
+        b2 = b + np.pi + 2 * g
+        # the scan runs from 0 to R; the two extra columns fix gamma_max
+        ang = torch.tensor([0.0, b, b2, R], dtype=torch.float64)
+        gam = torch.tensor([g, -g, gamma_max, -gamma_max], dtype=torch.float64)
+        w = parker_weights(ang, gam, 4)
+        assert abs(float(w[1, 0] + w[2, 1]) - 1.0) < 1e-12, (b, g)
+
+
 def _header_functions():
     text = (ROOT / "include" / "xrecon_b200.h").read_text()
     body = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
