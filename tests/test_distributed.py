@@ -44,6 +44,20 @@ def test_slab_options_reproduce_full_volume():
     np.testing.assert_allclose(parts[2], full[:, :, zs2], rtol=1e-6, atol=1e-6 * np.abs(full).max())
 
 
+@pytest.mark.parametrize("geom", ["dd3d_flat", "dd3d_arc", "dd3d_parallel"])
+def test_slab_options_serve_the_projection_transpose(geom):
+    """A^T is voxel-owned like B, so the slab-sharded layout also serves it
+    (the reduce-scatter of a view-sharded A^T is not needed)."""
+    g = load_golden(geom)
+    opts, ang, sino = g["options"], g["angles"], g["sino"]
+    full = O.dd3d("AT", sino, opts, ang)
+    D = int(opts[2])
+    for r in range(3):
+        zs = XD.slab_shard(D, r, 3)
+        part = O.dd3d("AT", sino, XD.slab_options(opts, zs), ang)
+        np.testing.assert_allclose(part, full[:, :, zs], rtol=1e-6, atol=1e-6 * np.abs(full).max())
+
+
 def test_more_ranks_than_slices_leaves_empty_slabs():
     g = load_golden("dd3d_flat")
     opts, ang, sino = g["options"], torch.from_numpy(g["angles"]), torch.from_numpy(g["sino"])

@@ -7,10 +7,10 @@ Two ways to spread the work, matching how the path partitions:
 * one large 3D problem is split inside:
   - the projection A by views: every rank projects the whole volume for its
     own views (``view_shard``); no exchange;
-  - the backprojection B / Bw by z-slabs of the volume: each rank needs every
-    view, so the view-sharded sinogram is all-gathered once (one
-    ``all_gather`` over NCCL / NVLink), then each rank backprojects its own
-    slab.  A slab is itself a volume geometry (``slab_options``), so the
+  - the backprojection B / Bw (and the voxel-owned A^T) by z-slabs of the
+    volume: each rank needs every view, so the view-sharded sinogram is
+    all-gathered once (one ``all_gather`` over NCCL / NVLink), then each
+    rank backprojects its own slab.  A slab is itself a volume geometry (``slab_options``), so the
     voxel-owned backprojection of the slab equals the slab of the full
     backprojection.
 
@@ -100,7 +100,8 @@ def gather_views(sino_local: torch.Tensor, nview: int, group=None) -> torch.Tens
 
 def backproject_slab(op: Callable, sino: torch.Tensor, options, angles: torch.Tensor, rank: int,
                      world: int) -> tuple[slice, torch.Tensor]:
-    """This rank's z-slab of ``op`` (B or Bw) applied to the full sinogram:
+    """This rank's z-slab of ``op`` (B, Bw or A^T: the voxel-owned
+    operators) applied to the full sinogram:
     (slab slice, [B, C, D_rank, H, W]).  With more ranks than slices, a rank
     without slices gets an empty slab and ``op`` is not called."""
     D = int(float(options[2]))
