@@ -458,6 +458,284 @@ def ragged_measure(dev, reps: int = 5):
             "tile_config": {"a_cols": 32 << R.config[0], "view_split": 1 << R.config[1]}}
 
 
+# --------------------------------------------- the other baseline configs
+
+def _timed_ms(fn, reps: int = 3) -> float:
+    """Device time of fn() per call: CUDA events on the current stream,
+    after one untimed call."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _cpu_filter_rows(sino_np, weight, filt):
+    """The reference's FBP/FDK filter step on the host: cosine weight, then
+    torch.nn.functional.conv2d of every detector row with the 2 Nu - 1 taps
+    and Nu - 1 zero padding (projector.py:196-202, projector3d.py:185-191)."""
+    import torch
+    import torch.nn.functional as F
+    x = torch.from_numpy(sino_np) * torch.as_tensor(weight).reshape(-1)
+    Nu = x.shape[-1]
+    rows = x.reshape(-1, 1, 1, Nu)
+    return F.conv2d(rows, torch.as_tensor(filt).reshape(1, 1, 1, -1), padding=(0, Nu - 1)).reshape(x.shape).numpy()
+
+
+def config_c1(dev, cpu: bool):
+    """2D fan-flat 256x256 (1 mm) Shepp-Logan + 10 seeded ellipses, 720
+    views over 2 pi, 256 cells of 2 mm, SOD 500, SDD 1000: projection, then
+    ramp FBP.  value = 256^2 * 720 / (t_A + t_FBP)."""
+    import numpy as np
+    import torch
+    from xrecon_b200 import geometry as G
+    from xrecon_b200.phantom import shepp_logan_plus_ellipses2d
+    from xrecon_b200.projector import Projector2d
+    P = Projector2d(G.Volume2d(256, 1.0), G.FanBeam2d(G.Detector2d(256, 2.0), 500.0, 1000.0, "flat")).to(dev)
+    img = shepp_logan_plus_ellipses2d(256, 10, seed=1).astype(np.float32)
+    ang_np = (np.arange(720) * (2 * np.pi / 720)).astype(np.float32)
+    x = torch.from_numpy(img)[None, None].to(dev)
+    a = torch.from_numpy(ang_np).to(dev)
+    sino = P.projection(x, a)
+    t_a = _timed_ms(lambda: P.projection(x, a), 10)
+    t_f = _timed_ms(lambda: P.filtered_backprojection(sino, a), 10)
+    work = 256 * 256 * 720
+    out = {"workload": "2D fan-flat 256x256, 720 views, 256 cells: A + ramp FBP", "ms_projection": t_a,
+           "ms_fbp": t_f, "value": work / ((t_a + t_f) / 1e3) / 1e9, "unit": UNIT}
+    if cpu:
+        from oracle import refcpu
+        if refcpu.available():
+            opts = P.options.cpu().numpy()
+            t0 = time.perf_counter()
+            s = refcpu.dd2d("A", img[None, None], opts, ang_np)
+            t1 = time.perf_counter()
+            sf = _cpu_filter_rows(s.astype(np.float32), P.weight.cpu().numpy(), P.filter.cpu().numpy())
+            refcpu.dd2d("BW", sf.astype(np.float32), opts, ang_np)
+            t2 = time.perf_counter()
+            out["reference_cpu"] = {"ms_projection": (t1 - t0) * 1e3, "ms_fbp": (t2 - t1) * 1e3,
+                                    "value": work / (t2 - t0) / 1e9, "cores": os.cpu_count() or 1,
+                                    "sample": "the full workload (the reference's CPU operators, torch conv2d filter)"}
+    return out
+
+
+def config_c2(dev, cpu: bool):
+    """3D cone-flat FDK: 256x256x64 (1 mm) 3D Shepp-Logan + 20 seeded
+    ellipsoids, 720 views, flat detector 384x96 of 1.5 mm, SOD 500, SDD 1000:
+    projection, then FDK (cosine weight, ramp filter, weighted
+    backprojection).  value = 256^2 * 64 * 720 / (t_A + t_FDK)."""
+    import numpy as np
+    import torch
+    from xrecon_b200 import geometry as G
+    from xrecon_b200.phantom import shepp_logan_plus_ellipsoids3d
+    from xrecon_b200.projector import Projector3d
+    P = Projector3d(G.Volume3d((256, 256, 64), 1.0),
+                    G.ConeBeam3d(G.Detector3d((384, 96), (1.5, 1.5)), 500.0, 1000.0, "flat")).to(dev)
+    vol = shepp_logan_plus_ellipsoids3d((64, 256, 256), 20, seed=2).astype(np.float32)
+    ang_np = (np.arange(720) * (2 * np.pi / 720)).astype(np.float32)
+    x = torch.from_numpy(vol)[None, None].to(dev)
+    a = torch.from_numpy(ang_np).to(dev)
+    sino = P.projection(x, a)
+    t_a = _timed_ms(lambda: P.projection(x, a), 5)
+    t_f = _timed_ms(lambda: P.filtered_backprojection(sino, a), 5)
+    work = 256 * 256 * 64 * 720
+    out = {"workload": "3D cone-flat 256x256x64, 720 views, 384x96 det: A + FDK", "ms_projection": t_a,
+           "ms_fdk": t_f, "value": work / ((t_a + t_f) / 1e3) / 1e9, "unit": UNIT}
+    del sino
+    if cpu:
+        from oracle import refcpu
+        if refcpu.available():
+            nv = 8
+            sub = ang_np[:: 720 // nv][:nv].copy()
+            opts = P.options.cpu().numpy()
+            t0 = time.perf_counter()
+            s = refcpu.dd3d("A", vol[None, None], opts, sub)
+            t1 = time.perf_counter()
+            sf = _cpu_filter_rows(s.astype(np.float32), P.weight.cpu().numpy(), P.filter.cpu().numpy())
+            refcpu.dd3d("BW", sf.astype(np.float32), opts, sub)
+            t2 = time.perf_counter()
+            k = 720 / nv
+            out["reference_cpu"] = {"ms_projection": (t1 - t0) * k * 1e3, "ms_fdk": (t2 - t1) * k * 1e3,
+                                    "value": work / ((t2 - t0) * k) / 1e9, "cores": os.cpu_count() or 1,
+                                    "sample": f"{nv} of 720 views, scaled by the view count"}
+    return out
+
+
+def config_c3(dev, cpu: bool, steps: int = 50):
+    """Differentiable 3D cone-arc least squares: B=8 volumes of 128x128x32
+    (1 mm) of seeded ellipsoids, 360 views, arc detector 256x64 of 1.5 mm, SOD
+    500, SDD 1000; data = projection + Poisson noise at 1e5 photons.  One
+    gradient step of ||Ax - y||^2 / 2 + 1e-3 TV(x) through the view-chunked
+    Function (A in the forward, A again and A^T in the backward), and the
+    50-step loop.  value = 8 * 128^2 * 32 * 360 / (t_A + t_AT)."""
+    import numpy as np
+    import torch
+    from xrecon_b200 import backend as BK
+    from xrecon_b200 import geometry as G
+    from xrecon_b200.functions import projection_least_squares
+    from xrecon_b200.phantom import ellipsoid_volume_torch, random_ellipsoids3d
+    det = G.Detector3d((256, 64), (1.5, 1.5))
+    opts = torch.tensor(G.pack_options3d(G.Volume3d((128, 128, 32), 1.0), G.ConeBeam3d(det, 500.0, 1000.0, "arc")),
+                        dtype=torch.float32, device=dev)
+    ang = (torch.arange(360, device=dev, dtype=torch.float64) * (2 * np.pi / 360)).float()
+    xs = [ellipsoid_volume_torch((32, 128, 128), random_ellipsoids3d(8, seed=100 + i, density=(0.0, 1.0)), dev)
+          for i in range(8)]
+    x_true = (torch.stack(xs)[:, None] * 0.02).contiguous()
+    g = torch.Generator(device=dev).manual_seed(5)
+    p = BK.forward_projection3d(x_true, opts, ang)
+    counts = torch.poisson(1e5 * torch.exp(-p), generator=g).clamp_min(1.0)
+    y = -torch.log(counts / 1e5)
+    t_a = _timed_ms(lambda: BK.forward_projection3d(x_true, opts, ang), 3)
+    t_at = _timed_ms(lambda: BK.projection_transpose3d(p, opts, ang), 3)
+
+    def tv(v, eps=1e-6):
+        dz = v[:, :, 1:, :-1, :-1] - v[:, :, :-1, :-1, :-1]
+        dy = v[:, :, :-1, 1:, :-1] - v[:, :, :-1, :-1, :-1]
+        dx = v[:, :, :-1, :-1, 1:] - v[:, :, :-1, :-1, :-1]
+        return torch.sqrt(dx * dx + dy * dy + dz * dz + eps).sum()
+
+    # step size 1 / ||A^T A|| by power iteration
+    v = torch.rand(x_true.shape, device=dev, generator=g)
+    for _ in range(6):
+        v = BK.projection_transpose3d(BK.forward_projection3d(v, opts, ang), opts, ang)
+        lam = float(v.norm())
+        v = v / lam
+    step = 1.0 / lam
+    x = torch.zeros_like(x_true, requires_grad=True)
+    losses = []
+
+    def loop(n):
+        for _ in range(n):
+            loss = projection_least_squares(x, y, opts, ang, view_chunk=24) + 1e-3 * tv(x)
+            (gr,) = torch.autograd.grad(loss, x)
+            with torch.no_grad():
+                x.sub_(step * gr)
+            losses.append(loss.detach())
+
+    loop(1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    loop(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    t_loop = e0.elapsed_time(e1)
+    work = 8 * 128 * 128 * 32 * 360
+    out = {"workload": "3D cone-arc B=8 x 128x128x32, 360 views, 256x64 arc det: A + A^T gradient step",
+           "ms_projection": t_a, "ms_projection_t": t_at, "value": work / ((t_a + t_at) / 1e3) / 1e9, "unit": UNIT,
+           "ms_50_step_loop": t_loop * steps / 50.0 if steps != 50 else t_loop,
+           "ms_per_gradient_step": t_loop / steps,
+           "loss_first_last": [float(losses[0]), float(losses[-1])]}
+    del p, counts, y, x
+    if cpu:
+        from oracle import refcpu
+        if refcpu.available():
+            nv = 4
+            sub = ang.cpu().numpy()[:: 360 // nv][:nv].copy()
+            o = opts.cpu().numpy()
+            xt = x_true.cpu().numpy()
+            t0 = time.perf_counter()
+            s = refcpu.dd3d("A", xt, o, sub)
+            t1 = time.perf_counter()
+            refcpu.dd3d("AT", s.astype(np.float32), o, sub)
+            t2 = time.perf_counter()
+            k = 360 / nv
+            out["reference_cpu"] = {"ms_projection": (t1 - t0) * k * 1e3, "ms_projection_t": (t2 - t1) * k * 1e3,
+                                    "value": work / ((t2 - t0) * k) / 1e9, "cores": os.cpu_count() or 1,
+                                    "sample": f"{nv} of 360 views of the B=8 batch, scaled by the view count"}
+    return out
+
+
+def baseline_configs(dev, cpu: bool):
+    """The named configurations besides the headline one (which is the main
+    line), each timed on this GPU and, with cpu, the reference's own CPU
+    operators on a bounded sample of the same workload on this host."""
+    out = {}
+    for name, fn in (("c1_fan_flat_2d_fbp", config_c1), ("c2_cone_flat_fdk", config_c2),
+                     ("c3_cone_arc_least_squares", config_c3)):
+        try:
+            out[name] = fn(dev, cpu)
+        except Exception as exc:  # a side measurement must not cost the main line
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+    return out
+
+
+def run_sharded_arm(args, rank: int, world: int, local_rank: int):
+    """Strong scaling of the headline workload: one problem split over the
+    ranks.  Each rank projects its share of the views, the view shards are
+    all-gathered over NCCL (one collective), and each rank backprojects its
+    z-slab of the volume with the full sinogram.  value = the whole
+    problem's voxel-views / the slowest rank's step time."""
+    import torch
+    import torch.distributed as dist
+    from xrecon_b200 import backend as BK
+    from xrecon_b200 import distributed as XD
+    from xrecon_b200.phantom import ellipsoid_volume_torch, random_ellipsoids3d
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    P = make_projector().to(dev)
+    opts = P.options
+    vol = ellipsoid_volume_torch((WL["D"], WL["H"], WL["W"]), random_ellipsoids3d(20, seed=0, density=(0.0, 1.0)),
+                                 dev)[None, None].contiguous()
+    ang = torch.from_numpy(angles_np(args.views)).to(dev)
+    nv = ang.numel()
+    stream = torch.cuda.current_stream(dev)
+    events = []
+
+    def mark(_name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        events[-1].append(e)
+
+    def step():
+        events.append([torch.cuda.Event(enable_timing=True)])
+        events[-1][0].record(stream)
+        return XD.sharded_projection_backprojection(BK.forward_projection3d, BK.backward_projection3d, vol, opts, ang,
+                                                    rank, world, marks=mark)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    events.clear()
+    clocks = ClockSampler(local_rank)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dist.barrier()
+    t_step = sum(e[0].elapsed_time(e[3]) for e in events) / args.steps / 1e3
+    phases = [sum(e[i].elapsed_time(e[i + 1]) for e in events) / args.steps for i in range(3)]
+    t_step = XD.max_over_ranks(t_step, dev)
+    phases = [XD.max_over_ranks(p, dev) for p in phases]
+    value = nvox() * nv / t_step / 1e9
+    hbm, src = peaks()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random ellipsoids)",
+            "config": {"workload": WORKLOAD_NAME, "views": nv, "parallelism": f"views x{world} for A, "
+                       f"NCCL all_gather of the sinogram, z-slabs x{world} for B",
+                       "ms_projection_max_rank": phases[0], "ms_all_gather_max_rank": phases[1],
+                       "ms_backprojection_max_rank": phases[2],
+                       "l2": "inputs larger than L2 (volume 256 MiB, sinogram 1.41 GiB)"},
+            "roofline": {"bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src,
+                         "achieved": 2 * algo_bytes_op(dict(WL, V=nv)) / t_step / 1e9 / world,
+                         "frac": 2 * algo_bytes_op(dict(WL, V=nv)) / t_step / 1e9 / world / hbm, "traffic": None,
+                         "note": "per GPU: the step's algorithmic bytes / world / step time"},
+            "e2e": None, "gpu_launches": None, "clocks": clk,
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def run_gpu_arm(args, rank: int, world: int, local_rank: int):
     import numpy as np
     import torch
@@ -526,7 +804,7 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         host_out = torch.empty_like(host_vol).pin_memory()
         dvol = torch.empty_like(vol)
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e2e_steps = max(1, min(args.steps, 3))
+        e2e_steps = args.steps
         barrier()
         torch.cuda.synchronize()
         f0.record(stream)
@@ -624,6 +902,8 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
         line["rebin_fan_to_parallel"] = rebin_measure(P, vol, ang)
     if not args.no_helical and world == 1:
         line["helical_arc_512x512x128_736x64_5x1152views"] = helical_measure(dev)
+    if not args.no_configs and world == 1:
+        line["configs"] = baseline_configs(dev, cpu=(rank == 0 and not args.no_cpu))
     if rank == 0 and world == 1 and not args.no_cpu:
         sample = cpu_reference_sample(4, vol.cpu().numpy())
         line["cpu_baseline"] = {k: v for k, v in sample.items() if k != "seconds"} if sample else None
@@ -652,6 +932,11 @@ def main():
                     help="profiling: turns of the helical scan (default 5) with --helical-only")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other named configurations (2D FBP, 3D FDK, cone-arc least squares)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with several GPUs: independent replicas of the workload (weak scaling) instead of one "
+                         "problem split over the GPUs (strong scaling, the default)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -670,6 +955,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
+        if world > 1 and not args.replicas:
+            return run_sharded_arm(args, rank, world, local_rank)
         return run_gpu_arm(args, rank, world, local_rank)
     finally:
         if world > 1:

@@ -139,9 +139,35 @@ int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, i
 /*
  * Read (and optionally clear) the device-wide error word of the current
  * device: 0 when no kernel has reported a problem.  Bit 0 = a bounded wait
- * for a TMA transfer gave up.  Synchronous (reads device memory).
+ * for a TMA transfer gave up (the projection kernel's CTA then left its
+ * line loop and stored nothing); bit 1 = a grid barrier of the ragged batch
+ * kernel gave up (the kernel returned).  The outputs of the launch that set a
+ * bit are not valid.  Synchronous (reads device memory); the operators never
+ * read it themselves, so callers that want the check poll it, for example
+ * after each batch of work.  Replaces the reference's exit() on a CUDA error
+ * (include/utils.h:7-11): the process and its context stay usable.
  */
 int xr_device_error(unsigned int* code, int clear);
+
+/*
+ * Poll limits of the bounded waits on the current device: tma_polls for an
+ * mbarrier wait of the projection kernel (each poll suspends at most about
+ * 1 us; default 2^20), barrier_polls for a grid barrier of the ragged kernel
+ * (polls of about 128 ns; default 2^22).  Values <= 0 restore the defaults.
+ * Synchronous.  No reference counterpart.
+ */
+int xr_set_wait_limits(long long tma_polls, long long barrier_polls);
+
+/*
+ * Testing aid, no reference counterpart: failure injection for the bounded
+ * waits, on the current device (0 = off, the default).  Bit 0: the
+ * projection kernel's producer arms each barrier for a box but issues no
+ * copy, so every consumer wait runs out with nothing in flight.  Bit 1: the
+ * ragged kernel's grid barriers expect one block more than the grid, so every
+ * barrier wait runs out.  Nothing faults; the waits end at their limits
+ * (xr_set_wait_limits) and set the device error word.  Synchronous.
+ */
+int xr_test_hooks(unsigned int hooks);
 
 /* Staging plan of the 3D projection kernel for this geometry: whether the
  * TMA line windows are used, their box size (pixels x z voxels), and whether
@@ -171,8 +197,9 @@ int xr_set_plain_kernels(int on);
  * xr_dd2d_workspace_size) fail with XR_ERR_WORKSPACE.  Every scratch byte a
  * call reads is first written by the same call, so nothing needs clearing.
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and caches it; make that first call before any
- * stream capture.  There is one array per device: calls whose executions
+ * (cudaGetSymbolAddress) and caches it per device and CUDA context (after a
+ * device reset the next call looks it up again); make that first call before
+ * any stream capture.  There is one array per device: calls whose executions
  * overlap on the GPU (different streams, or threads) race on it and must be
  * serialised by the caller.
  */

@@ -53,7 +53,7 @@ def build_oracle(force: bool = False) -> Path:
     src = HERE / "dd_oracle.c"
     LIB_DIR.mkdir(exist_ok=True)
     if force or _stale(ORACLE_SO, [src]):
-        _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-o", str(ORACLE_SO), str(src), "-lm"])
+        _run(["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(ORACLE_SO), str(src), "-lm"])
     return ORACLE_SO
 
 

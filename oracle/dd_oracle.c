@@ -86,6 +86,94 @@ static double map_angle(const view_t* v, double a)
     return v->sy + v->sx / tan(a);
 }
 
+/* Arc boundary and column-centre angles as the reference forms them: in
+ * float32 with every operation rounded, (k - Nu/2) du + shift_u + beta for a
+ * detector kept in order and (Nu/2 - k) du + shift_u + beta for a reversed
+ * one (forward3d.cpp:271-297, system_matrix2d.cpp:280-283).  The rounding of
+ * the last sum (a quantum of 4.8e-7 rad at |beta| ~ 2 pi) moves a boundary by
+ * up to 3e-4 of a detector cell, so the operator follows it; everything
+ * after the angle is FP64.  xo_set_arc_exact(1) switches to the exact angle. */
+static int g_arc_exact = 0;
+
+void xo_set_arc_exact(int on) { g_arc_exact = on; }
+
+/* Axis position of an arc boundary angle as the reference maps it: in
+ * float32, src.x + src.y tanf(a) (x axis) or src.y + src.x / tanf(a) (y axis)
+ * with the float source (-sinf(b) SOD, cosf(b) SOD) (xrmath.h:24-38,
+ * :116-123).  The sum cancels: its rounding, about ulp(|src|), is up to 1e-4
+ * of a column near the 45-degree views and the voxel-driven coefficients
+ * scale with it.  g_tan_cr = 1 takes tan correctly rounded to float instead
+ * of the C library's tanf (which is not always). */
+static int g_tan_cr = 0;
+
+void xo_set_tan_rounding(int correctly_rounded) { g_tan_cr = correctly_rounded; }
+
+static double map_angle_f(const view_t* v, float a, double sod)
+{
+    const float b = (float)v->beta, R = (float)sod;
+    volatile float sx = -sinf(b) * R, sy = cosf(b) * R;
+    volatile float t = g_tan_cr ? (float)tan((double)a) : tanf(a);
+    volatile float r;
+    if (v->use_x) { volatile float m = sy * t; r = sx + m; }
+    else          { volatile float q = sx / t; r = sy + q; }
+    return (double)r;
+}
+
+static double arc_angle(const view_t* v, double k, int nu, double du, double shu)
+{
+    if (g_arc_exact) return sigma(v, k, nu) * du + shu + v->beta;
+    volatile float s = v->keep ? ((float)k - (float)nu * 0.5f) : ((float)nu * 0.5f - (float)k);
+    volatile float a = s * (float)du;
+    a = a + (float)shu;
+    a = a + (float)v->beta;
+    return (double)a;
+}
+
+/* Column overlaps of the pixels of one line for the voxel-driven arc
+ * operators (B, Bw and their transposes).  The reference walks each voxel's
+ * columns with boundary angles chained in float32 from the voxel's first
+ * column (include/cpu3d_common.h:150-196, src/cpu/backward2d.cpp:119-157):
+ * the first angle is that column's (lower, kept detector) or the next
+ * column's plus du (reversed detector), each further one is the previous
+ * plus or minus du, rounded.  The overlaps with the pixel [X[p], X[p+1]]
+ * follow those angles; the column's z magnification uses the mid angle
+ * 0.5 (a + a_next) of the pair.  Entries go to (ia, ib, len, cang) like
+ * overlaps(); D holds the boundaries of arc_angle (the detector ends). */
+static int chain_overlaps(const view_t* v, const double* X, int npix, const double* D, int nu,
+                          double du, double shu, double sod, int* ia, int* ib, double* len, double* cang)
+{
+    int n = 0;
+    const float duf = (float)du;
+    for (int p = 0; p < npix; ++p) {
+        double b0 = X[p] > D[0] ? X[p] : D[0];
+        const double b1 = X[p + 1] < D[nu] ? X[p + 1] : D[nu];
+        if (!(b0 < b1)) continue;
+        int k = 0;
+        while (k < nu - 1 && D[k + 1] <= b0) ++k;
+        volatile float t;
+        if (v->keep) {
+            t = (float)arc_angle(v, k, nu, du, shu);
+        } else {
+            volatile float t1 = (float)arc_angle(v, k + 1, nu, du, shu);
+            t = t1 + duf;
+        }
+        while (b0 < b1 && k < nu) {
+            volatile float tn = v->keep ? t + duf : t - duf;
+            const double Dn = g_arc_exact ? map_angle(v, (double)tn) : map_angle_f(v, tn, sod);
+            const double nb = b1 < Dn ? b1 : Dn;
+            const double ov = nb - b0;
+            if (ov > 0.0) {
+                volatile float sum = t + tn;
+                ia[n] = p; ib[n] = k; len[n] = ov; cang[n] = (double)(0.5f * sum); ++n;
+            }
+            b0 = ov > 0.0 ? nb : Dn;
+            t = tn;
+            ++k;
+        }
+    }
+    return n;
+}
+
 /* Two-pointer merge of the interval sequences [a_i, a_{i+1}] (i < na) and
  * [b_j, b_{j+1}] (j < nb), both increasing.  Writes the overlapping pairs. */
 static int overlaps(const double* a, int na, const double* b, int nb,
@@ -122,8 +210,8 @@ static void view_columns3d(const geo3_t* g, const view_t* v,
             D[k] = map_point(v, u * v->c, u * v->s);
         } else if (g->type == GEO_ARC) {
             /* forward3d.cpp:271-283 */
-            const double a = sigma(v, k, g->Nu) * g->du + g->shu + v->beta;
-            D[k] = map_angle(v, a);
+            const double a = arc_angle(v, k, g->Nu, g->du, g->shu);
+            D[k] = g_arc_exact ? map_angle(v, a) : map_angle_f(v, (float)a, g->sod);
         } else {
             /* forward3d.cpp:53-56 (parallel: u / cos or u / sin) */
             const double u = sigma(v, k, g->Nu) * g->du + g->shu;
@@ -138,7 +226,7 @@ static void view_columns3d(const geo3_t* g, const view_t* v,
             cx = u * v->c; cy = u * v->s;
         } else if (g->type == GEO_ARC) {
             /* forward3d.cpp:285-297 */
-            const double a = sigma(v, k + 0.5, g->Nu) * g->du + g->shu + v->beta;
+            const double a = arc_angle(v, k + 0.5, g->Nu, g->du, g->shu);
             cx = sin(a) * g->sdd + v->sx; cy = -cos(a) * g->sdd + v->sy;
         } else {
             cx = cy = 0.0;
@@ -238,6 +326,9 @@ int xo_dd3d(int op, const int* ni, const double* fv, const double* fg, int type,
     const double z0 = -0.5 * g.D * g.dz + g.shz;
     const double cw = (type == GEO_FLAT) ? g.du * g.sod / g.sdd
                     : (type == GEO_ARC) ? 2.0 * g.sod * tan(0.5 * g.du) : g.du;
+    /* voxel-driven arc operators: columns chained per voxel as the reference does */
+    const int chain = type == GEO_ARC && !g_arc_exact && op != OP_A && op != OP_AT;
+    double* xc = malloc(sizeof(double) * nxo);
 
     for (int view = 0; view < nview; ++view) {
         const view_t v = make_view(ang[view], g.sod);
@@ -248,13 +339,19 @@ int xo_dd3d(int op, const int* ni, const double* fv, const double* fg, int type,
             double Mv, perp;
             const int npix = line_pixels3d(&g, &v, line, X, &Mv, &perp);
             for (int i = 0; i <= g.D; ++i) Zv[i] = Mv * (z0 + i * g.dz);
-            const int nx = overlaps(X, npix, D, g.Nu, xa, xb, xl);
+            const int nx = chain ? chain_overlaps(&v, X, npix, D, g.Nu, g.du, g.shu, g.sod, xa, xb, xl, xc)
+                                 : overlaps(X, npix, D, g.Nu, xa, xb, xl);
             for (int e = 0; e < nx; ++e) {
                 const int p = xa[e], k = xb[e];
                 const int ix = v.use_x ? p : line;
                 const int iy = v.use_x ? line : g.H - 1 - p;
                 const int col = v.keep ? k : g.Nu - 1 - k;
-                for (int r = 0; r <= g.Nv; ++r) Zc[r] = M[k] * zd[r];
+                double Mk = M[k];
+                if (chain) {
+                    const double cx = sin(xc[e]) * g.sdd + v.sx, cy = -cos(xc[e]) * g.sdd + v.sy;
+                    Mk = v.use_x ? v.sy / (v.sy - cy) : v.sx / (v.sx - cx);
+                }
+                for (int r = 0; r <= g.Nv; ++r) Zc[r] = Mk * zd[r];
                 const int nz = overlaps(Zv, g.D, Zc, g.Nv, za, zb, zl);
                 /* voxel-side scale: reference voxel_area = |(X1-X0)(z1-z0)|
                  * (cpu3d_common.h:80) and the FBP weight (:84-85). */
@@ -301,7 +398,7 @@ int xo_dd3d(int op, const int* ni, const double* fv, const double* fg, int type,
         }
     }
     free(D); free(M); free(zd); free(X); free(Zv); free(Zc);
-    free(xa); free(xb); free(xl); free(za); free(zb); free(zl);
+    free(xa); free(xb); free(xl); free(za); free(zb); free(zl); free(xc);
     return 0;
 }
 
@@ -329,6 +426,8 @@ int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
     /* B column width: backward2d.cpp:87 (flat du), :109 (arc 2 SOD tan(du/2)),
      * :185 (parallel du / pixel). */
     const double cw = (type == GEO_ARC) ? 2.0 * sod * tan(0.5 * du) : du;
+    const int chain = type == GEO_ARC && !g_arc_exact && op != OP_A && op != OP_AT;
+    double* xc = malloc(sizeof(double) * nxo);
 
     for (int view = 0; view < nview; ++view) {
         const view_t v = make_view(ang[view], sod);
@@ -340,7 +439,8 @@ int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
                 D[k] = map_point(&v, u * v.c, u * v.s);
             } else if (type == GEO_ARC) {
                 /* system_matrix2d.cpp:280-283 */
-                D[k] = map_angle(&v, sg * du + shu + v.beta);
+                const double a = arc_angle(&v, k, Nu, du, shu);
+                D[k] = g_arc_exact ? map_angle(&v, a) : map_angle_f(&v, (float)a, sod);
             } else {
                 /* system_matrix2d.cpp:104-107 */
                 const double u = sg * du + shu;
@@ -366,7 +466,8 @@ int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
                                                    : map_point(&v, px, y0 + i * dy);
                 npix = H;
             }
-            const int nx = overlaps(X, npix, D, Nu, xa, xb, xl);
+            const int nx = chain ? chain_overlaps(&v, X, npix, D, Nu, du, shu, sod, xa, xb, xl, xc)
+                                 : overlaps(X, npix, D, Nu, xa, xb, xl);
             for (int e = 0; e < nx; ++e) {
                 const int p = xa[e], k = xb[e];
                 const int ix = v.use_x ? p : line;
@@ -400,7 +501,7 @@ int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
             }
         }
     }
-    free(D); free(X); free(xa); free(xb); free(xl);
+    free(D); free(X); free(xa); free(xb); free(xl); free(xc);
     return 0;
 }
 
@@ -730,6 +831,10 @@ int xo_helical3d(int op, const int* ni, const double* fv, const double* fg, cons
     o.view_turns = (float)fo[2]; o.halfscan_coef = (float)fo[3]; o.tang_k = (float)fo[4]; o.tang_blend = (float)fo[5];
     o.window_quotient_up = (int)fo[6];
     if (op < 0 || op > 5 || nview < 1) return 1;
+    /* the helical column angles are evaluated exactly (their reference is
+     * fast-math CUDA, not the float32 CPU arithmetic of arc_angle) */
+    const int arc_exact_saved = g_arc_exact;
+    g_arc_exact = 1;
     const long long nvox = (long long)g.W * g.H * g.D;
     const long long ncell = (long long)g.Nu * g.Nv;
     const int out_is_sino = (op == OP_A || op == OP_BT || op == OP_BWT);
@@ -850,5 +955,6 @@ int xo_helical3d(int op, const int* ni, const double* fv, const double* fg, cons
     free(D); free(M); free(zd); free(X); free(Zv); free(Zc);
     free(xa); free(xb); free(xl); free(za); free(zb); free(zl);
     free(zw); free(scale);
+    g_arc_exact = arc_exact_saved;
     return 0;
 }

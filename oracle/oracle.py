@@ -16,6 +16,7 @@ does.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import math
 from pathlib import Path
@@ -44,6 +45,10 @@ def _load():
                            ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                            ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int]
+        lib.xo_set_arc_exact.restype = None
+        lib.xo_set_arc_exact.argtypes = [ctypes.c_int]
+        lib.xo_set_tan_rounding.restype = None
+        lib.xo_set_tan_rounding.argtypes = [ctypes.c_int]
         dp = ctypes.POINTER(ctypes.c_double)
         lib.xo_helical3d.restype = ctypes.c_int
         lib.xo_helical3d.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp, dp, dp, dp, dp,
@@ -51,6 +56,20 @@ def _load():
                                      ctypes.c_int, ctypes.c_int]
         _lib = lib
     return _lib
+
+
+@contextlib.contextmanager
+def tan_rounding(correctly_rounded: bool):
+    """Within the block, the arc axis mapping takes tan rounded correctly to
+    float32 (the CUDA path's arithmetic) instead of the C library's tanf (the
+    reference CPU path's, the default; glibc's is off by one unit for about 4 %
+    of arguments)."""
+    lib = _load()
+    lib.xo_set_tan_rounding(int(correctly_rounded))
+    try:
+        yield
+    finally:
+        lib.xo_set_tan_rounding(0)
 
 
 def _p(a, ctype):
@@ -72,9 +91,11 @@ def unpack3d(options):
                 shx=o[12], shy=o[13], shz=o[14], shu=o[15], shv=o[16], type=int(o[17]))
 
 
-def dd2d(op: str, x, options, angles):
+def dd2d(op: str, x, options, angles, arc_exact: bool = False):
     """Apply a 2D operator.  x: [B, C, H, W] (image in) or [B, C, V, Nu]
-    (sinogram in); returns float64 ndarray of the output shape."""
+    (sinogram in); returns float64 ndarray of the output shape.  Arc
+    boundary angles are rounded to float32 as the reference forms them
+    (``dd_oracle.c::arc_angle``) unless ``arc_exact``."""
     g = unpack2d(options)
     ang = np.ascontiguousarray(angles, dtype=np.float32)
     V = ang.shape[0]
@@ -85,6 +106,7 @@ def dd2d(op: str, x, options, angles):
     ni = np.array([g["W"], g["H"], g["Nu"]], dtype=np.int32)
     fv = np.array([g["dx"], g["dy"], g["shx"], g["shy"]], dtype=np.float64)
     fg = np.array([g["du"], g["shu"], g["SOD"], g["SDD"]], dtype=np.float64)
+    _load().xo_set_arc_exact(int(arc_exact))
     rc = _load().xo_dd2d(OPS[op], _p(ni, ctypes.c_int), _p(fv, ctypes.c_double), _p(fg, ctypes.c_double),
                          g["type"], _p(x, ctypes.c_double), _p(out, ctypes.c_double),
                          _p(ang, ctypes.c_float), B * C, V)
@@ -93,8 +115,9 @@ def dd2d(op: str, x, options, angles):
     return out
 
 
-def dd3d(op: str, x, options, angles):
-    """Apply a 3D operator.  x: [B, C, D, H, W] or [B, C, V, Nv, Nu]."""
+def dd3d(op: str, x, options, angles, arc_exact: bool = False):
+    """Apply a 3D operator.  x: [B, C, D, H, W] or [B, C, V, Nv, Nu].  Arc
+    boundary angles as in :func:`dd2d`."""
     g = unpack3d(options)
     ang = np.ascontiguousarray(angles, dtype=np.float32)
     V = ang.shape[0]
@@ -105,6 +128,7 @@ def dd3d(op: str, x, options, angles):
     ni = np.array([g["W"], g["H"], g["D"], g["Nu"], g["Nv"]], dtype=np.int32)
     fv = np.array([g["dx"], g["dy"], g["dz"], g["shx"], g["shy"], g["shz"]], dtype=np.float64)
     fg = np.array([g["du"], g["dv"], g["shu"], g["shv"], g["SOD"], g["SDD"]], dtype=np.float64)
+    _load().xo_set_arc_exact(int(arc_exact))
     rc = _load().xo_dd3d(OPS[op], _p(ni, ctypes.c_int), _p(fv, ctypes.c_double), _p(fg, ctypes.c_double),
                          g["type"], _p(x, ctypes.c_double), _p(out, ctypes.c_double),
                          _p(ang, ctypes.c_float), B * C, V)

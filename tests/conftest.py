@@ -36,6 +36,20 @@ def cuda():
 
 
 @pytest.fixture(autouse=True)
+def _oracle_tan_rounding(request):
+    """GPU tests compare the CUDA path with the oracle in the CUDA path's own
+    arithmetic: arc boundaries from tan rounded correctly to float32.  The
+    reference's C library tanf differs from it by one unit for a few percent of
+    arguments; the GPU tests check the reference fixtures separately."""
+    if request.node.get_closest_marker("gpu") is None:
+        yield
+        return
+    from oracle import oracle as O
+    with O.tan_rounding(True):
+        yield
+
+
+@pytest.fixture(autouse=True)
 def _device_error_word(request):
     """After every GPU test: no kernel may have reported a bounded-wait
     timeout through the device error word."""

@@ -130,6 +130,47 @@ def test_view_and_slab_sharding_matches_single_process(world, nview):
     np.testing.assert_allclose(out, vol_ref, rtol=1e-6, atol=1e-6 * np.abs(vol_ref).max())
 
 
+def _step_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g = load_golden("dd3d_flat")
+        opts = torch.from_numpy(g["options"])
+        ang = torch.from_numpy(g["angles"])
+        vol = torch.from_numpy(g["image"]).double()
+        phases = []
+        zs, slab = XD.sharded_projection_backprojection(_oracle_op("A"), _oracle_op("B"), vol, opts, ang, rank,
+                                                        world, marks=phases.append)
+        q.put((rank, zs.start, zs.stop, slab.numpy(), phases))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_step_matches_single_process(world):
+    """The bench's strong-scaling step (view-sharded A, one all-gather,
+    slab-sharded B) reassembles B(A(vol)) of the single process."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_step_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    g = load_golden("dd3d_flat")
+    ref = O.dd3d("B", O.dd3d("A", g["image"], g["options"], g["angles"]), g["options"], g["angles"])
+    out = np.zeros_like(ref)
+    for rank, z0, z1, slab, phases in results:
+        assert phases == ["projection", "gather", "backprojection"]
+        out[:, :, z0:z1] = slab
+    np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-6 * np.abs(ref).max())
+
+
 @pytest.mark.gpu
 def test_gpu_slab_and_view_shards_match_full_operators(cuda):
     """The CUDA operators on view shards and z-slabs reassemble the full

@@ -2,10 +2,11 @@
 with the reference's own outputs.
 
 Tolerances (relative L2):
-* against the FP64 oracle: 1e-5 (the parity bar for FP32);
-* against the reference fixtures: the oracle's own distance from the
-  reference plus 1e-5 (the reference's float32 geometry sits 1e-6..1e-4 away
-  from the exact operator, see test_oracle_pin.py);
+* against the FP64 oracle: 1e-5 (the parity bar for FP32); for the arc
+  detector the oracle takes the CUDA path's float32 boundary arithmetic
+  (tests/conftest.py), which differs from the reference's only where the C
+  library's tanf is off by one unit;
+* against the reference fixtures: 1e-5 for every geometry, arc included;
 * adjoint pairs <Ax, y> = <x, A^T y>: 1e-5;
 * BF16/FP16 storage with FP32 accumulation: 1e-3 against the oracle applied
   to the same (rounded) input; outputs stored in BF16 add their own rounding
@@ -47,8 +48,7 @@ def test_ops_match_oracle_and_reference(cuda, dim, scan):
         e_oracle = rel_l2(got, exact)
         assert e_oracle < 1e-5, f"{dim}D {scan} {op}: vs oracle {e_oracle:.2e}"
         e_ref = rel_l2(got, g[op])
-        bound = rel_l2(exact, g[op]) + 1e-5
-        assert e_ref < bound, f"{dim}D {scan} {op}: vs reference {e_ref:.2e} (bound {bound:.2e})"
+        assert e_ref < 1e-5, f"{dim}D {scan} {op}: vs reference {e_ref:.2e}"
 
 
 def _opts3d(W, H, D, Nu, Nv, dx, dy, dz, du, dv, sod, sdd, sh, shu, shv, scan):

@@ -1,7 +1,7 @@
 """FBP / FDK on the GPU through Projector2d/3d.filtered_backprojection, against
-the FP64 oracle (1e-5) and the reference's own reconstructions (within the
-reference's distance from the oracle plus 1e-5).  The geometries are those of
-tests/golden/make_golden.py, rebuilt with this package's geometry classes."""
+the FP64 oracle (1e-5) and the reference's own reconstructions (1e-5, arc
+included).  The geometries are those of tests/golden/make_golden.py, rebuilt
+with this package's geometry classes."""
 import numpy as np
 import pytest
 import torch
@@ -50,7 +50,7 @@ def test_fbp2d_matches_oracle_and_reference(cuda, case):
     exact = O.filtered_backprojection2d(g["sino"], g["options"], g["angles"], P.weight.cpu().numpy(),
                                         P.filter.cpu().numpy(), redundant=not parker, parker=pk)
     assert rel_l2(recon, exact) < 1e-5
-    assert rel_l2(recon, g["recon"]) < rel_l2(exact, g["recon"]) + 1e-5
+    assert rel_l2(recon, g["recon"]) < 1e-5
 
 
 @pytest.mark.parametrize("scan", ["flat", "arc"])
@@ -64,7 +64,7 @@ def test_fdk3d_matches_oracle_and_reference(cuda, scan):
     exact = O.filtered_backprojection3d(g["sino"], g["options"], g["angles"], P.weight.cpu().numpy(),
                                         P.filter.cpu().numpy())
     assert rel_l2(recon, exact) < 1e-5
-    assert rel_l2(recon, g["recon"]) < rel_l2(exact, g["recon"]) + 1e-5
+    assert rel_l2(recon, g["recon"]) < 1e-5
 
 
 @pytest.mark.parametrize("scan", ["flat", "arc"])

@@ -9,7 +9,12 @@ from conftest import load_golden, rel_l2
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
-TOL = {"parallel": 1e-5, "flat": 1e-5, "arc": 3e-4}
+# Entry-wise distance of the matrices.  Arc coefficients scale with the
+# float32 boundary positions src.x + src.y tan(a), where the reference's C
+# library tanf is one unit off for a few percent of angles (the CUDA path takes
+# tan correctly rounded): those entries differ by up to 1e-4, which the
+# operator comparisons below average out.
+TOL = {"parallel": 1e-5, "flat": 1e-5, "arc": 5e-5}
 
 
 @pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])

@@ -6,6 +6,7 @@ CPU tensor raises immediately.
 from __future__ import annotations
 
 import ctypes
+import os
 from ctypes import c_float, c_int, c_size_t, c_void_p
 from pathlib import Path
 
@@ -76,6 +77,10 @@ def lib():
     L.xr_cell_plan.argtypes = [ctypes.POINTER(Geom3d)] + [ctypes.POINTER(c_int)] * 5
     L.xr_set_plain_kernels.restype = c_int
     L.xr_set_plain_kernels.argtypes = [c_int]
+    L.xr_set_wait_limits.restype = c_int
+    L.xr_set_wait_limits.argtypes = [ctypes.c_longlong, ctypes.c_longlong]
+    L.xr_test_hooks.restype = c_int
+    L.xr_test_hooks.argtypes = [ctypes.c_uint]
     L.xr_last_error.restype = ctypes.c_char_p
     for d, G in ((2, Geom2d), (3, Geom3d)):
         ws = getattr(L, f"xr_sysmat{d}d_workspace_size")
@@ -200,6 +205,7 @@ def apply(dim: int, op: str, x: torch.Tensor, geom, angles: torch.Tensor,
                 ang.data_ptr(), nbatch, V, ws.data_ptr(), ws.numel(), stream)
     if rc != 0:
         _raise(rc, f"xr_dd{dim}d({op})")
+    _after_op()
     return out
 
 
@@ -243,6 +249,7 @@ def helical(op: str, x: torch.Tensor, geom: Geom3d, hopts: HelicalOpts, angles: 
                             torch.cuda.current_stream(dev).cuda_stream)
     if rc != 0:
         _raise(rc, f"xr_helical3d({op})")
+    _after_op()
     return out
 
 
@@ -312,12 +319,54 @@ def system_matrix(dim: int, geom, angles: torch.Tensor, device) -> torch.Tensor:
 
 
 def device_error(clear: bool = True) -> int:
-    """Device-wide error word (0 = no kernel reported a problem)."""
+    """Device-wide error word of the current device (0 = no kernel reported a
+    problem; bit 0: a TMA wait of the projection kernel gave up, bit 1: a grid
+    barrier of the ragged kernel gave up).  Synchronous."""
     code = ctypes.c_uint(0)
     rc = lib().xr_device_error(ctypes.byref(code), int(clear))
     if rc != 0:
         _raise(rc, "xr_device_error")
     return int(code.value)
+
+
+def check_device_error() -> None:
+    """Raise RuntimeError (and clear the word) when a kernel of this library
+    reported a bounded wait that gave up since the last check: the outputs of
+    that launch are not valid.  Synchronous; the operators do not call it
+    themselves unless the environment sets XRECON_B200_CHECK=1."""
+    code = device_error(clear=True)
+    if code:
+        what = []
+        if code & 1:
+            what.append("a TMA transfer wait of the projection kernel gave up")
+        if code & 2:
+            what.append("a grid barrier of the ragged batch kernel gave up")
+        raise RuntimeError(f"xrecon_b200 device error {code:#x}: " + "; ".join(what or ["unknown code"]))
+
+
+_CHECK_EACH = os.environ.get("XRECON_B200_CHECK", "") not in ("", "0")
+
+
+def _after_op() -> None:
+    if _CHECK_EACH:
+        check_device_error()
+
+
+def set_wait_limits(tma_polls: int = 0, barrier_polls: int = 0) -> None:
+    """Poll limits of the bounded waits on the current device (<= 0: the
+    defaults, 2^20 TMA polls of at most ~1 us and 2^22 barrier polls of ~128 ns)."""
+    rc = lib().xr_set_wait_limits(int(tma_polls), int(barrier_polls))
+    if rc != 0:
+        _raise(rc, "xr_set_wait_limits")
+
+
+def test_hooks(bits: int) -> None:
+    """Failure injection for the bounded waits (testing aid; 0 = off): bit 0
+    stalls the projection kernel's TMA copies, bit 1 makes the ragged grid
+    barriers wait for one block too many."""
+    rc = lib().xr_test_hooks(int(bits))
+    if rc != 0:
+        _raise(rc, "xr_test_hooks")
 
 
 def cell_plan(geom: Geom3d) -> dict:

@@ -123,8 +123,15 @@ Geom geom_from(const xr_geom2d* p) {
 }
 
 struct Layout {
-    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, volT, volR, volF, sinoS, total;
+    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, arc, volT, volR, volF, sinoS, total;
+    bool has_arc;
 };
+
+// Voxel-driven operators on a circular arc detector walk chained float32
+// boundary angles, which need the per-boundary entries of ViewTables::arc.
+bool arc_chain_op(const Geom& g, int op) {
+    return g.type == GEO_ARC && (op == OP_B || op == OP_BW || op == OP_BT || op == OP_BWT);
+}
 
 // ------------------------------------------------------ TMA staging plans
 
@@ -260,7 +267,7 @@ bool encode_line_map(CUtensorMap* m, int dt, const void* base, int npix, int nli
 
 // Image-input ops of the cell gather need the flipped transpose of the image
 // (lines of y-axis views); cone A^T needs an FP32 pre-scaled sinogram.
-Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype_in) {
+Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype_in, bool chain_ok = true) {
     Layout l{};
     size_t o = 0;
     const size_t V = (size_t)(nview > 0 ? nview : 1);
@@ -272,6 +279,9 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
     l.colE = o;  o = align256(o + V * g.Nu * sizeof(float));
     l.colF = o;  o = align256(o + V * g.Nu * sizeof(float));
     l.colM = o;  o = align256(o + V * g.Nu * sizeof(float));
+    l.has_arc = chain_ok && arc_chain_op(g, op);
+    l.arc = o;
+    if (l.has_arc) o = align256(o + V * (g.Nu + 1) * sizeof(float4));
     int eff = op;
     if (g.type == GEO_PARALLEL && dim3d) {
         if (op == OP_B || op == OP_BW) eff = OP_AT;
@@ -313,6 +323,7 @@ ViewTables tables_at(char* ws, const Layout& l) {
     t.colF = reinterpret_cast<float*>(ws + l.colF);
     t.colM = reinterpret_cast<float*>(ws + l.colM);
     t.hel = nullptr;
+    t.arc = l.has_arc ? reinterpret_cast<float4*>(ws + l.arc) : nullptr;
     return t;
 }
 
@@ -476,7 +487,8 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
         else if (op == OP_BT || op == OP_BWT) eff = OP_A;
     }
     if (eff == OP_A || eff == OP_BT || eff == OP_BWT) {
-        if (!g_force_plain) {
+        // arc B^T / Bw^T walk chained angles per pixel: the plain cell gather
+        if (!g_force_plain && !vt.arc) {
             int rc;
             if constexpr (sizeof(TI) == 2) {
                 // Widen once: the staged walk then reads FP32, which costs
@@ -538,6 +550,12 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
         dim3 pblock(32, PFX_NWY);
         if (eff == OP_AT)
             vox_prefix3d_kernel<TO, PFX_R, PFX_NWY, OP_AT><<<pgrid, pblock, 0, st>>>(
+                g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, cw, atconst, oscale);
+        else if (vt.arc && eff == OP_B)
+            vox_prefix3d_kernel<TO, PFX_R, PFX_NWY, OP_B, false, true><<<pgrid, pblock, 0, st>>>(
+                g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, cw, atconst, oscale);
+        else if (vt.arc)
+            vox_prefix3d_kernel<TO, PFX_R, PFX_NWY, OP_BW, false, true><<<pgrid, pblock, 0, st>>>(
                 g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, cw, atconst, oscale);
         else if (eff == OP_B)
             vox_prefix3d_kernel<TO, PFX_R, PFX_NWY, OP_B><<<pgrid, pblock, 0, st>>>(
@@ -698,7 +716,7 @@ struct HelLayout {
 
 HelLayout hel_layout(int op, const Geom& g, int nbatch, int nview) {
     HelLayout h;
-    h.l = layout(1, op, g, nbatch, nview, DT_F32);
+    h.l = layout(1, op, g, nbatch, nview, DT_F32, false);
     size_t o = h.l.total;
     const size_t V = (size_t)(nview > 0 ? nview : 1);
     h.hel = o;  o = align256(o + V * sizeof(HelView));
@@ -862,7 +880,7 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
 
 struct RaggedLayout {
     size_t desc, sync;
-    std::vector<size_t> hdr, bA, bB, colQ, colR, colE, colF, colM, imgT, filt;
+    std::vector<size_t> hdr, bA, bB, colQ, colR, colE, colF, colM, arc, imgT, filt;
     size_t total;
 };
 
@@ -902,21 +920,41 @@ int ragged_tiles(const Geom& g, int nview, int list) {
 // nothing is ever allocated for it.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[XR_NOALLOC_SCRATCH_BYTES];
 
+// The address is cached per device and per context: after a device reset
+// the primary context (and the module holding the array) is created anew, and
+// the array gets a new address.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
 int noalloc_scratch(void** ptr) {
     static std::mutex mu;
-    static std::vector<void*> by_device;
+    static std::vector<std::pair<CUcontext, void*>> by_device;
+    static CtxGetCurrentFn ctx_current = nullptr;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return fail(XR_ERR_CUDA, "cudaGetDevice failed");
     std::lock_guard<std::mutex> lock(mu);
-    if ((int)by_device.size() <= dev) by_device.resize(dev + 1, nullptr);
-    if (!by_device[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(XR_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
-        by_device[dev] = p;
+    if (!ctx_current) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return fail(XR_ERR_CUDA, "cuCtxGetCurrent is not available");
+        ctx_current = reinterpret_cast<CtxGetCurrentFn>(fn);
     }
-    *ptr = by_device[dev];
+    if ((int)by_device.size() <= dev) by_device.resize(dev + 1, {nullptr, nullptr});
+    CUcontext ctx = nullptr;
+    if (ctx_current(&ctx) == CUDA_SUCCESS && ctx && by_device[dev].first == ctx && by_device[dev].second) {
+        *ptr = by_device[dev].second;
+        return XR_OK;
+    }
+    // first call on this device or context (the lookup creates the primary
+    // context when there is none yet)
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(XR_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+    if (ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return fail(XR_ERR_CUDA, "no current CUDA context");
+    by_device[dev] = {ctx, p};
+    *ptr = p;
     return XR_OK;
 }
 
@@ -1038,6 +1076,21 @@ int xr_device_error(unsigned int* code, int clear) {
         if (cudaMemcpyToSymbol(xr::g_device_error, &zero, sizeof(unsigned int)) != cudaSuccess)
             return xr::fail(XR_ERR_CUDA, "clearing the device error word failed");
     }
+    return XR_OK;
+}
+
+int xr_set_wait_limits(long long tma_polls, long long barrier_polls) {
+    const long long t = tma_polls > 0 ? tma_polls : xr::XR_WAIT_LIMIT_DEFAULT;
+    const long long b = barrier_polls > 0 ? barrier_polls : xr::XR_BARRIER_LIMIT_DEFAULT;
+    if (cudaMemcpyToSymbol(xr::g_wait_limit, &t, sizeof(t)) != cudaSuccess ||
+        cudaMemcpyToSymbol(xr::g_barrier_limit, &b, sizeof(b)) != cudaSuccess)
+        return xr::fail(XR_ERR_CUDA, "setting the wait limits failed");
+    return XR_OK;
+}
+
+int xr_test_hooks(unsigned int hooks) {
+    if (cudaMemcpyToSymbol(xr::g_test_hooks, &hooks, sizeof(hooks)) != cudaSuccess)
+        return xr::fail(XR_ERR_CUDA, "setting the test hooks failed");
     return XR_OK;
 }
 
@@ -1169,6 +1222,8 @@ int xr_ragged2d_plan_create(const xr_ragged2d_instance* inst, int ninst, xr_ragg
         L.colE.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
         L.colF.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
         L.colM.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
+        L.arc.push_back(o);
+        if (g.type == GEO_ARC) o = align256(o + Vs * (g.Nu + 1) * sizeof(float4));  // Bw's chained walks
         L.imgT.push_back(o); o = align256(o + (size_t)g.H * g.W * sizeof(float));
         L.filt.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
     }
@@ -1219,6 +1274,7 @@ int xr_ragged2d_plan_bind(xr_ragged2d_plan* P, const float* images, float* sino,
         r.vt.colF = reinterpret_cast<float*>(ws + L.colF[i]);
         r.vt.colM = reinterpret_cast<float*>(ws + L.colM[i]);
         r.vt.hel = nullptr;
+        r.vt.arc = r.g.type == GEO_ARC ? reinterpret_cast<float4*>(ws + L.arc[i]) : nullptr;
         r.nview = in.nview;
         r.cw = column_width(r.g, 0);
         r.scale = in.scale;
@@ -1253,6 +1309,10 @@ int xr_ragged2d_run(const xr_ragged2d_plan* P, int project, int a_cols_log2, int
     const int4 lists = make_int4(0, 2 + a_cols_log2, 1, 6 + view_split_log2);
     const int ninst = (int)P->inst.size();
     const int CW = 32 << a_cols_log2, VS = 1 << view_split_log2;
+    // barrier word and tile counters start at zero on every launch (also in
+    // a captured graph), even after a launch whose barrier gave up
+    if (cudaMemsetAsync(ws + P->lay.sync, 0, 64, static_cast<cudaStream_t>(stream)) != cudaSuccess)
+        return fail(XR_ERR_CUDA, "resetting the ragged kernel's sync words failed");
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P->grid);
     cfg.blockDim = dim3(256);

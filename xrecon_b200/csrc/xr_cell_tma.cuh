@@ -88,6 +88,14 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
     return w;
 }
 
+// After a wait gave up: lines L and L + 1 may still have copies in flight.
+// The issuing thread lets them land (or gives up once more) before it exits,
+// which keeps the CTA's shared memory allocated until then.
+__device__ __noinline__ void drain_stages(uint64_t* bar, int L, int nlines) {
+    for (int Lp = L; Lp < min(L + 2, nlines); ++Lp)
+        mbar_wait_bounded(&bar[Lp & 1], (unsigned)((Lp >> 1) & 1));
+}
+
 // FINE: the geometry's detector rows are (nearly) all shorter than a voxel,
 // so only the fine-row walk is compiled; lines where it does not apply take
 // the global path.  Less code and fewer live registers than the full kernel.
@@ -170,20 +178,24 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     const TI* __restrict__ fbb = fb + (size_t)b * g.D * fb_plane;
     const unsigned box_bytes = (unsigned)((size_t)BP * BZ * sizeof(TI));
 
+    // test hook: arm the barrier for a box but issue no copy (the consumers'
+    // bounded waits then run out with nothing in flight)
+    const bool stall = (*(volatile unsigned*)&g_test_hooks & XR_HOOK_TMA_STALL) != 0;
     auto issue = [&](int L, int s) {
         const int4 w = wins[L];
         if (w.w >> 1) {
             mbar_arrive_expect_tx(&bar[s], box_bytes);
-            tma_load_4d(stage + (size_t)s * stage_elems, map, w.x, L, w.y, b, &bar[s]);
+            if (!stall) tma_load_4d(stage + (size_t)s * stage_elems, map, w.x, L, w.y, b, &bar[s]);
         } else {
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar[s])) : "memory");
         }
     };
-
+    __shared__ int s_abort[2];
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         fence_barrier_init();
+        s_abort[0] = s_abort[1] = 0;
     }
     // the line windows, evaluated by all threads in parallel (FP64)
     for (int L = tid; L < nlines; L += blockDim.x * blockDim.y) {
@@ -206,10 +218,15 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     const double zr0 = zd0 + r0 * dvv;
     const float dpdz = (float)(h.dpix * g.dz);
 
+    // A wait that gives up sets the stage's abort flag; after the line's
+    // barrier every thread sees it and the CTA returns: no further copy is
+    // issued, nothing is stored.  Two flags alternate with the stages, so a
+    // flag is only read after the barrier that closes its own line, before
+    // any thread can reach the next line that writes it.
     for (int L = 0; L < nlines; ++L) {
         const int s = L & 1;
         const unsigned parity = (unsigned)((L >> 1) & 1);
-        mbar_wait_bounded(&bar[s], parity);
+        if (!mbar_wait_bounded(&bar[s], parity)) s_abort[s] = 1;  // the stage's values then go unused
         CellWindow win;
         {
             const int4 wi = wins[L];
@@ -344,6 +361,10 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
             }
         }
         __syncthreads();
+        if (s_abort[s]) {
+            if (tid == 0) drain_stages(bar, L, nlines);
+            return;
+        }
         if (tid == 0 && L + 2 < nlines) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             issue(L + 2, s);

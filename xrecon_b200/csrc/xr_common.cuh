@@ -51,6 +51,7 @@ struct ViewHdr {
     double q0, q1;          // 1 / Mv(L) = q0 + q1 * L   (1 for parallel)
     double dpix;            // pixel size along the line (dx or dy)
     float dcx, dcy;         // arc detector: central ray direction (column guesses)
+    float sxf, syf;         // the source as the reference holds it in float32
 };
 
 // Per-view tables, structure of arrays, view-major.
@@ -85,6 +86,11 @@ struct ViewTables {
     float* colF;
     float* colM;
     HelView* hel;  // helical scans only, else null
+    // circular arc detectors, voxel-driven operators (B, Bw and their
+    // transposes) only, else null: per boundary k = 0..Nu of each view
+    // {float32 angle, tan(angle) as a float pair hi + lo, float32 axis
+    // position}, the inputs of the chained column walk (arc_chain_delta)
+    float4* arc;
 };
 
 // ---------------------------------------------------------------- dtype io
@@ -141,7 +147,76 @@ __host__ __device__ inline void make_view_hdr(const Geom& g, float ang, ViewHdr&
     h.dpix = h.use_x ? g.dx : g.dy;
     h.dcx = (float)sin(h.beta + g.shu);
     h.dcy = (float)(-cos(h.beta + g.shu));
+    // View2d.source = (-sinf(b) SOD, cosf(b) SOD) in float (xrmath.h:116-123)
+    const float sodf = (float)g.sod;
+#ifdef __CUDA_ARCH__
+    h.sxf = __fmul_rn(-__double2float_rn(h.s), sodf);
+    h.syf = __fmul_rn(__double2float_rn(h.c), sodf);
+#else
+    h.sxf = -(float)h.s * sodf;
+    h.syf = (float)h.c * sodf;
+#endif
 }
+
+// ------------------------------------------------ arc detector, float32
+
+// Angle of arc boundary k (k + 1/2 for a column centre) as the reference
+// forms it, every operation rounded to float32:
+//     (k - Nu/2) du + shift_u + beta   (kept order),
+//     (Nu/2 - k) du + shift_u + beta   (reversed)
+// (src/cpu/forward3d.cpp:271-297, src/cpu/system_matrix2d.cpp:280-283,
+// include/cpu3d_common.h:150-166).  The last sum rounds to a quantum of
+// 4.8e-7 rad at |beta| ~ 2 pi, up to 5e-4 of a column at du = 1e-3, so the
+// operator follows the rounded angle; everything after it is FP64.
+__device__ __forceinline__ float arc_angle_f(const Geom& g, int keep, float kf, float ang) {
+    const float half = __fmul_rn((float)g.Nu, 0.5f);
+    const float sg = keep ? __fsub_rn(kf, half) : __fsub_rn(half, kf);
+    return __fadd_rn(__fadd_rn(__fmul_rn(sg, (float)g.du), (float)g.shu), ang);
+}
+
+// Axis position of a ray at float angle t from the float source, as the
+// reference computes it: src.x + src.y tan(t) on the x axis, src.y + src.x /
+// tan(t) on the y axis, each step rounded to float32 (xrmath.h:24-38).  The
+// sum cancels to about ulp(|src|), up to 1e-4 of a column near the 45-degree
+// views, and the voxel-driven coefficients scale with it.  tf is tan(t)
+// rounded to float (the C library's tanf of the reference's CPU path is
+// within one unit of it).
+__device__ __forceinline__ float arc_axis_f(const ViewHdr& h, float tf) {
+    return h.use_x ? __fadd_rn(h.sxf, __fmul_rn(h.syf, tf)) : __fadd_rn(h.syf, __fdiv_rn(h.sxf, tf));
+}
+
+// Offset, on the common axis, of the boundary at the chained angle t from
+// the direct boundary e = {t_d, tan hi, tan lo, axis} of the same index:
+// tan(t) to float from tan(t_d + d) = T + d (1 + T^2)(1 + d T) + O(d^3),
+// d = t - t_d (exact: both are floats a few units apart), then the float
+// axis mapping.  Zero when t == t_d.
+__device__ __forceinline__ float arc_chain_delta(const ViewHdr& h, const float4 e, float t) {
+    const float d = __fsub_rn(t, e.x);
+    const float S = fmaf(e.y, e.y, 1.0f);
+    const float c = fmaf(d * S, fmaf(d, e.y, 1.0f), e.z);
+    return __fsub_rn(arc_axis_f(h, __fadd_rn(e.y, c)), e.w);
+}
+
+// The column walk of a voxel-driven arc operator, chained in float32 as the
+// reference walks it (include/cpu3d_common.h:160-196,
+// src/cpu/backward2d.cpp:142-157): it starts at the column k0 holding the
+// voxel's first edge, at that column's lower angle (detector kept in order)
+// or at the next column's angle plus du (reversed), and each further
+// boundary angle is the previous one plus du (kept) or minus du (reversed).
+// next() steps to the following boundary and returns its axis offset from
+// the direct boundary.  Boundaries far from k0 drift from the direct ones by
+// the accumulated roundings, which the reference's results carry.
+struct ArcChain {
+    float t, step;
+    __device__ __forceinline__ void start(const float4* __restrict__ e, int k0, int keep, float du) {
+        step = keep ? du : -du;
+        t = keep ? e[k0].x : __fadd_rn(e[k0 + 1].x, du);
+    }
+    __device__ __forceinline__ float next(const ViewHdr& h, const float4 e) {
+        t = __fadd_rn(t, step);
+        return arc_chain_delta(h, e, t);
+    }
+};
 
 // Column-centre z magnification M_k onto the axis plane (forward3d.cpp:258-297).
 __host__ __device__ inline double column_mag(const Geom& g, const ViewHdr& h, int k, double uscale) {

@@ -55,36 +55,51 @@ __device__ __forceinline__ float row_value(const TI* __restrict__ colbase, int m
 
 // ------------------------------------------------------------------ setup
 
-// One thread per (view, boundary k in 0..Nu).  FP64 throughout.
+// One thread per (view, boundary k in 0..Nu).  FP64 throughout, except the
+// float32 boundary angles of circular arc detectors (arcf; see arc_angle_f).
 __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d, const float angle, const int v,
-                                                 const int k, const ViewTables& vt);
+                                                 const int k, const ViewTables& vt, const bool arcf = false);
 
 __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* __restrict__ ang,
                                    const int nview, const ViewTables vt) {
     const int v = blockIdx.y;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nview || k > g.Nu) return;
-    setup_view_entry(g, dim3d, ang[v], v, k, vt);
+    setup_view_entry(g, dim3d, ang[v], v, k, vt, g.type == GEO_ARC);
+}
+
+// Axis position of arc boundary k with the reference's float32 rounding, and
+// its {angle, tan hi, tan lo, axis} entry.
+__device__ __forceinline__ double arc_boundary_f(const Geom& g, const ViewHdr& h, int k, float angle, float4& e) {
+    const float tk = arc_angle_f(g, h.keep, (float)k, angle);
+    const double T = tan((double)tk);
+    const float hi = __double2float_rn(T);
+    const float lo = __double2float_rn(T - (double)hi);
+    const float Df = arc_axis_f(h, hi);
+    e = make_float4(tk, hi, lo, Df);
+    return (double)Df;
 }
 
 // Per-view tables of view v, boundary / column k (k = 0..Nu).
 __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d, const float angle, const int v,
-                                                 const int k, const ViewTables& vt) {
+                                                 const int k, const ViewTables& vt, const bool arcf) {
     ViewHdr h;
     make_view_hdr(g, angle, h);
     if (k == 0) vt.hdr[v] = h;
 
     const double uscale = (dim3d && g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
-    const double Dk = boundary_axis(g, h, (double)k, uscale);
+    const size_t ob = (size_t)v * (g.Nu + 1) + k;
+    float4 e;
+    const double Dk = arcf ? arc_boundary_f(g, h, k, angle, e) : boundary_axis(g, h, (double)k, uscale);
+    if (arcf && vt.arc) vt.arc[ob] = e;
     double A, B;
     boundary_line_coeffs(g, h, Dk, A, B);
-    const size_t ob = (size_t)v * (g.Nu + 1) + k;
     vt.bA[ob] = A;
     vt.bB[ob] = B;
     if (k >= g.Nu) return;
 
     const size_t oc = (size_t)v * g.Nu + k;
-    const double Dk1 = boundary_axis(g, h, (double)k + 1.0, uscale);
+    const double Dk1 = arcf ? arc_boundary_f(g, h, k + 1, angle, e) : boundary_axis(g, h, (double)k + 1.0, uscale);
     const double dperp = h.use_x ? g.dy : g.dx;
     if (g.type == GEO_PARALLEL) {
         // forward3d.cpp:58,98 (xy_scale / dv) and system_matrix2d.cpp:109.
@@ -95,7 +110,15 @@ __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d,
         vt.colM[oc] = 0.0f;
         return;
     }
-    const double M = column_mag(g, h, k, uscale);
+    double M;
+    if (arcf) {
+        // column centre at the float32 centre angle (forward3d.cpp:285-297)
+        const double ac = (double)arc_angle_f(g, h.keep, (float)k + 0.5f, angle);
+        const double cx = sin(ac) * g.sdd + h.sx, cy = -cos(ac) * g.sdd + h.sy;
+        M = h.use_x ? h.sy / (h.sy - cy) : h.sx / (h.sx - cx);
+    } else {
+        M = column_mag(g, h, k, uscale);
+    }
     vt.colQ[oc] = M / g.dz;
     vt.colR[oc] = g.dz / M;
     const double aa = 0.5 * (Dk + Dk1) - h.spar;
@@ -153,6 +176,30 @@ __global__ void pad_rows_kernel(const T* __restrict__ in, T* __restrict__ out, i
     out[row * pitch + x] = in[i];
 }
 
+// Arc detector, cell-owned B^T / Bw^T: bounds of column k over the band's
+// first pixel pa of line L when that pixel starts left of the column
+// (pk > pa).  The reference walks that pixel's columns from the one holding
+// its first edge, k0 < k, with chained angles (ArcChain): column k spans the
+// chain's boundaries k and k + 1, s - 1 and s steps from k0.  u0, u1 are
+// written relative to pa; qd converts axis offsets to pixels on line L.
+__device__ __forceinline__ void arc_first_pixel_bounds(const Geom& g, const ViewTables& vt, const ViewHdr& h,
+                                                       const float4* __restrict__ ea, int v, int k, int L, int pa,
+                                                       double pk, double pk1, float qd, float& u0, float& u1) {
+    const int Nu = g.Nu;
+    const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
+    const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
+    int k0 = k - 1;
+    while (k0 > 0 && fma(bB[k0], (double)L, bA[k0]) > (double)pa) --k0;
+    ArcChain ch;
+    ch.start(ea, k0, h.keep, (float)g.du);
+    for (int j = k0 + 1; j < k; ++j) ch.t = __fadd_rn(ch.t, ch.step);
+    const float dk = ch.next(h, ea[k]);
+    float dk1 = ch.next(h, ea[k + 1]);
+    if (k + 1 == Nu) dk1 = fminf(dk1, 0.0f);
+    u0 = fmaf(dk, qd, (float)(pk - (double)pa));
+    u1 = fmaf(dk1, qd, (float)(pk1 - (double)pa));
+}
+
 // ------------------------------------------------------------- 3D kernels
 
 // Cell gather: lane = detector column (traversal order), warp = run of R
@@ -183,6 +230,16 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
     const size_t plane = (size_t)nlines * npix;
     const TI* __restrict__ vol = (h.use_x ? vol_rows : vol_cols) + (size_t)b * g.D * plane;
     const double zr0 = zd0 + r0 * dvv;
+    // arc detector, B^T / Bw^T: chained column walks (see cell2d_sum)
+    const bool chain = (MODE == OP_BT || MODE == OP_BWT) && !HEL && vt.arc;
+    const float4* __restrict__ ea = chain ? vt.arc + (size_t)v * (Nu + 1) : nullptr;
+    float d1 = 0.0f;
+    if (chain) {
+        ArcChain ch;
+        ch.start(ea, k, h.keep, (float)g.du);
+        d1 = ch.next(h, ea[k + 1]);
+        if (k + 1 == Nu) d1 = fminf(d1, 0.0f);
+    }
 
     float acc[R];
 #pragma unroll
@@ -211,7 +268,15 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
             lf = dpdz / (qf * qf);
         }
         // band edges relative to the first pixel: small FP32 numbers
-        const float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
+        float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
+        float u1b = u1;  // upper edge for the band's later pixels
+        if (chain) {
+            const float qd = (float)(q / h.dpix);
+            u1b = fmaf(d1, qd, u1);
+            u1 = u1b;
+            if (k > 0 && pk > (double)pa)
+                arc_first_pixel_bounds(g, vt, h, ea, v, k, L, pa, pk, pk1, qd, u0, u1);
+        }
         const TI* __restrict__ line = vol + (size_t)L * npix;
         for (int pc = pa; pc <= pb; pc += MAXB) {
             const int np = min(MAXB, pb - pc + 1);
@@ -221,7 +286,7 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
             for (int i = 0; i < MAXB; ++i) {
                 float wi = 0.0f;
                 if (i < np) {
-                    wi = (fminf(off + (float)(i + 1), u1) - fmaxf(off + (float)i, u0)) * lf;
+                    wi = (fminf(off + (float)(i + 1), (pc + i == pa) ? u1 : u1b) - fmaxf(off + (float)i, u0)) * lf;
                     if (MODE == OP_BWT) {
                         float px, py;
                         pixel_center(g, h, L, pc + i, px, py);
@@ -401,17 +466,13 @@ vox_gather3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const TI*
         const double* __restrict__ Q = vt.colQ + (size_t)v * Nu;
         const TI* __restrict__ sv = sinob + (size_t)v * Nv * Nu;
         const double dp = (double)p;
-        double pk = fma(bB[ka], (double)L, bA[ka]);
-        for (int k = ka; k <= kb; ++k) {
-            const double pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
-            const float wf = (float)(fmin(dp + 1.0, pk1) - fmax(dp, pk));
-            pk = pk1;
-            if (!(wf > 0.0f)) continue;
+        // z merge of column k, overlapping the pixel by wf
+        auto column = [&](const int k, const float wf) {
             const double gq = Q[k] * q;
             const double T0 = fma(gq, zd0, -z0dz);
             const double bt = gq * dvv;
-            if (!(bt > 1.0e-4 && bt < 1.0e4)) continue;  // bounds every merge loop
-            if (T0 >= dj0 + R || T0 + Nv * bt <= dj0) continue;
+            if (!(bt > 1.0e-4 && bt < 1.0e4)) return;  // bounds every merge loop
+            if (T0 >= dj0 + R || T0 + Nv * bt <= dj0) return;
             const float bf = (float)bt;
             const int col = keep ? k : Nu - 1 - k;
             const TI* __restrict__ yp;
@@ -453,6 +514,40 @@ vox_gather3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const TI*
                 pos = top;
                 acc[i] = fmaf(wk, a, acc[i]);
             }
+        };
+        if (MODE != OP_AT && vt.arc) {
+            // arc detector: the pixel's columns walked with chained angles
+            const float4* __restrict__ ea = vt.arc + (size_t)v * (Nu + 1);
+            const double qd = q / h.dpix;  // pixels per axis unit
+            int k = ka;
+            double pkl = fma(bB[k], (double)L, bA[k]);
+            double pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
+            while (!(pk1 > dp) && k < kb) {
+                ++k;
+                pkl = pk1;
+                pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
+            }
+            ArcChain ch;
+            ch.start(ea, k, h.keep, (float)g.du);
+            for (;;) {
+                float d = ch.next(h, ea[k + 1]);
+                if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
+                pk1 = fma((double)d, qd, pk1);
+                const float wf = (float)(fmin(dp + 1.0, pk1) - fmax(dp, pkl));
+                if (wf > 0.0f) column(k, wf);
+                if (++k > kb) break;
+                pkl = pk1;
+                if (pkl >= dp + 1.0) break;
+                pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
+            }
+            continue;
+        }
+        double pk = fma(bB[ka], (double)L, bA[ka]);
+        for (int k = ka; k <= kb; ++k) {
+            const double pk1 = fma(bB[k + 1], (double)L, bA[k + 1]);
+            const float wf = (float)(fmin(dp + 1.0, pk1) - fmax(dp, pk));
+            pk = pk1;
+            if (wf > 0.0f) column(k, wf);
         }
     }
 #pragma unroll
@@ -503,6 +598,18 @@ __device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt,
     const int nlines = h.nlines, npix = h.npix;
     const TI* __restrict__ img = h.use_x ? img_rows : img_cols;
     const float dpixf = (float)h.dpix;
+    // arc detector, B^T / Bw^T: the column's upper boundary on the chained
+    // walk of a pixel whose first edge lies in this column (every pixel but
+    // the band's first); the same on every line
+    const bool chain = (MODE == OP_BT || MODE == OP_BWT) && vt.arc;
+    const float4* __restrict__ ea = chain ? vt.arc + (size_t)v * (Nu + 1) : nullptr;
+    float d1 = 0.0f;
+    if (chain) {
+        ArcChain ch;
+        ch.start(ea, k, h.keep, (float)g.du);
+        d1 = ch.next(h, ea[k + 1]);
+        if (k + 1 == Nu) d1 = fminf(d1, 0.0f);
+    }
     float acc = 0.0f;
     for (int L = l0; L < nlines; L += ls) {
         const double pk = fma(bB0, (double)L, bA0);
@@ -515,10 +622,18 @@ __device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt,
         else lf = cw;
         const TI* __restrict__ line = img + (size_t)L * npix;
         // boundaries relative to the first pixel, so FP32 keeps them exact
-        const float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
+        float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
+        float u1b = u1;  // upper boundary for the band's later pixels
+        if (chain) {
+            const float qd = (float)(fma(h.q1, (double)L, h.q0) / h.dpix);
+            u1b = fmaf(d1, qd, u1);
+            u1 = u1b;
+            if (k > 0 && pk > (double)pa)
+                arc_first_pixel_bounds(g, vt, h, ea, v, k, L, pa, pk, pk1, qd, u0, u1);
+        }
         for (int pp = pa; pp <= pb; ++pp) {
             const float o = (float)(pp - pa);
-            float w = (fminf(o + 1.0f, u1) - fmaxf(o, u0)) * lf;
+            float w = (fminf(o + 1.0f, pp == pa ? u1 : u1b) - fmaxf(o, u0)) * lf;
             if (MODE == OP_BWT) {
                 float px, py;
                 pixel_center(g, h, L, pp, px, py);
@@ -614,6 +729,36 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
         const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
         const TI* __restrict__ sv = sinob + (size_t)v * Nu;
         const double dp = (double)p, dL = (double)L;
+        if (MODE != OP_AT && vt.arc) {
+            // arc detector: the pixel's columns walked with chained angles
+            const float4* __restrict__ ea = vt.arc + (size_t)v * (Nu + 1);
+            const float qd = (float)(fma(h.q1, dL, h.q0) / h.dpix);  // pixels per axis unit
+            int k = ka;
+            float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
+            float pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            while (!(pk1 > 0.0f) && k < kb) {
+                ++k;
+                pkl = pk1;
+                pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            }
+            ArcChain ch;
+            ch.start(ea, k, h.keep, (float)g.du);
+            for (;;) {
+                float d = ch.next(h, ea[k + 1]);
+                if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
+                pk1 = fmaf(d, qd, pk1);
+                const float wd = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
+                if (wd > 0.0f) {
+                    const int col = h.keep ? k : Nu - 1 - k;
+                    acc = fmaf(wd * lf, ld(sv + col), acc);
+                }
+                if (++k > kb) break;
+                pkl = pk1;
+                if (pkl >= 1.0f) break;
+                pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            }
+            continue;
+        }
         // boundaries relative to the pixel (pixel units)
         float pkl = (float)(fma(bB[ka], dL, bA[ka]) - dp);
         for (int k = ka; k <= kb; ++k) {

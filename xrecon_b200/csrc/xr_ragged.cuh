@@ -27,7 +27,9 @@
 namespace xr {
 
 constexpr unsigned XR_DEVERR_BARRIER_TIMEOUT = 2u;
-constexpr long long XR_BARRIER_LIMIT = 1ll << 24;  // polls of ~128 ns: a few seconds
+// polls of ~128 ns: about half a second by default (xr_set_wait_limits)
+constexpr long long XR_BARRIER_LIMIT_DEFAULT = 1ll << 22;
+__device__ long long g_barrier_limit = XR_BARRIER_LIMIT_DEFAULT;
 
 // One instance, device side (pointers already resolved).
 struct RaggedDev {
@@ -60,6 +62,9 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks) {
         const unsigned gen = *vgen;
         __threadfence();
         const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+        const long long limit = *(volatile long long*)&g_barrier_limit;
+        // test hook: one block more than the grid is expected, nobody releases
+        if (*(volatile unsigned*)&g_test_hooks & XR_HOOK_BARRIER_EXTRA) ++nblocks;
         int ok = 1;
         if (arrived == nblocks) {
             atomicExch(bar, 0u);
@@ -68,7 +73,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks) {
         } else {
             long long i = 0;
             while (*vgen == gen) {
-                if (++i > XR_BARRIER_LIMIT) {
+                if (++i > limit) {
                     atomicOr(&g_device_error, XR_DEVERR_BARRIER_TIMEOUT);
                     ok = 0;
                     break;
@@ -115,7 +120,7 @@ ragged2d_fbp_kernel(const RaggedDev* __restrict__ inst, const int ninst, const i
         const int lt = t - I.t0[lists.x];
         const Geom& g = I.g;
         if (lt < I.nview) {
-            for (int k = tid; k <= g.Nu; k += blockDim.x) setup_view_entry(g, 0, I.ang[lt], lt, k, I.vt);
+            for (int k = tid; k <= g.Nu; k += blockDim.x) setup_view_entry(g, 0, I.ang[lt], lt, k, I.vt, g.type == GEO_ARC);
         } else {
             const int base = (lt - I.nview) * 1024;
             for (int e = tid; e < 1024; e += blockDim.x) {

@@ -19,7 +19,20 @@ namespace xr {
 __device__ unsigned int g_device_error = 0;
 
 constexpr unsigned XR_DEVERR_TMA_TIMEOUT = 1u;
-constexpr long long XR_WAIT_LIMIT = 1ll << 24;
+
+// Poll limits of the bounded waits, per device (xr_set_wait_limits).  A poll
+// of an mbarrier suspends for at most about a microsecond, so the default
+// gives up after roughly 0.02 to 1 s; a TMA box lands in microseconds.
+constexpr long long XR_WAIT_LIMIT_DEFAULT = 1ll << 20;
+__device__ long long g_wait_limit = XR_WAIT_LIMIT_DEFAULT;
+
+// Test hooks (xr_test_hooks), zero in normal use.  Bit 0: TMA producers arm
+// their barriers for a box but issue no copy, so every consumer wait runs out
+// with nothing in flight.  Bit 1: the ragged kernel's grid barriers expect
+// one block more than the grid, so every barrier wait runs out.
+constexpr unsigned XR_HOOK_TMA_STALL = 1u;
+constexpr unsigned XR_HOOK_BARRIER_EXTRA = 2u;
+__device__ unsigned int g_test_hooks = 0;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -40,12 +53,13 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
                  : "memory");
 }
 
+// One poll: suspends until the phase completes or about 1000 ns pass.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     unsigned ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
         : "memory");
     return ok != 0;
 }
@@ -53,7 +67,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 // Bounded wait for phase `parity` of `bar`; false (and the device error word
 // set) when the limit is reached.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-    for (long long i = 0; i < XR_WAIT_LIMIT; ++i)
+    const long long limit = *(volatile long long*)&g_wait_limit;
+    for (long long i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     atomicOr(&g_device_error, XR_DEVERR_TMA_TIMEOUT);
     return false;

@@ -106,7 +106,10 @@ __device__ __forceinline__ float col_guess_fast(const GeomF& gf, const ViewHdr& 
 #endif
 //   HEL        : helical scan; the view's z placement, column width and
 //                angular column pitch come from vt.hel
-template <typename TO, int R, int NWY, int MODE, bool HEL = false>
+//   CHAIN      : circular arc detector, B / Bw: the pixel's columns are
+//                walked with the reference's chained float32 angles
+//                (ArcChain, vt.arc)
+template <typename TO, int R, int NWY, int MODE, bool HEL = false, bool CHAIN = false>
 __global__ void __launch_bounds__(32 * NWY, XR_PFX_MINB)
 vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const float2* __restrict__ tab,
                     TO* __restrict__ vol, const int nview, const int nzg, const double z0dz, const double zd0,
@@ -197,6 +200,17 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             pkl = pk1;
             pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
         }
+        ArcChain ch;
+        float qd = 0.0f;
+        const float4* __restrict__ ea = nullptr;
+        if (CHAIN) {
+            ea = vt.arc + (size_t)v * (Nu + 1);
+            qd = (float)(q / h.dpix);  // pixels per axis unit on this line
+            ch.start(ea, k, keep, gf.du);
+            float d = ch.next(h, ea[k + 1]);
+            if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
+            pk1 = fmaf(d, qd, pk1);
+        }
         // lanes now walk their overlapping columns in step, one per iteration
         for (;;) {
             const float wf = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
@@ -276,6 +290,11 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             pkl = pk1;
             if (pkl >= 1.0f) break;  // column k starts right of the pixel
             pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            if (CHAIN) {
+                float d = ch.next(h, ea[k + 1]);
+                if (k + 1 == Nu) d = fminf(d, 0.0f);
+                pk1 = fmaf(d, qd, pk1);
+            }
         }
     }
 #pragma unroll

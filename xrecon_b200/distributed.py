@@ -122,3 +122,25 @@ def max_over_ranks(seconds: float, device=None, group=None) -> float:
     t = torch.tensor([seconds], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def sharded_projection_backprojection(fwd: Callable, back: Callable, vol: torch.Tensor, options,
+                                      angles: torch.Tensor, rank: int, world: int, group=None,
+                                      marks: Callable | None = None) -> tuple[slice, torch.Tensor]:
+    """One A-then-B step of a single problem split over the ranks: this
+    rank's views of A(vol), the view shards all-gathered (one collective),
+    then this rank's z-slab of B applied to the full sinogram.  Returns
+    (slab slice, slab of B(A(vol))).  ``vol`` is the full volume on every
+    rank.  ``marks(name)``, when given, is called after each phase
+    ("projection", "gather", "backprojection") so a caller can time them on
+    its stream."""
+    local = project_views(fwd, vol, options, angles, rank, world)
+    if marks:
+        marks("projection")
+    full = gather_views(local, angles.numel(), group) if world > 1 else local
+    if marks:
+        marks("gather")
+    zs, slab = backproject_slab(back, full, options, angles, rank, world)
+    if marks:
+        marks("backprojection")
+    return zs, slab

@@ -130,13 +130,12 @@ class ProjectionLeastSquares(Function):
         adj = _B.projection_transpose2d if dim == 2 else _B.projection_transpose3d
         xc = _c(x)
         V = angles.numel()
-        grad = None
+        grad = torch.zeros_like(x)  # also the gradient of a scan with no views
         for v0 in range(0, V, ctx.view_chunk):
             v1 = min(V, v0 + ctx.view_chunk)
             a = angles[v0:v1].contiguous()
             r = fwd(xc, ctx.option, a) - y[:, :, v0:v1]
-            g = adj(_c(r), ctx.option, a)
-            grad = g if grad is None else grad.add_(g)
+            grad.add_(adj(_c(r), ctx.option, a))
         return grad * grad_output, None, None, None, None
 
 
