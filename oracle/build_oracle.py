@@ -30,7 +30,11 @@ REF_DIR = HERE / "_ref"
 ORACLE_SO = LIB_DIR / "libxr_oracle.so"
 REF_SO = REF_DIR / "libxrecon_ref_cpu.so"
 REF_HELICAL_SO = REF_DIR / "libxrecon_ref_helical.so"
-REFERENCE_ROOT = Path(os.environ.get("XRECON_REFERENCE_ROOT", "/root/reference"))
+# Root of the XRecon reference tree, from the environment; unset: the
+# reference libraries are not built (prebuilt ones are used when present).
+def reference_root() -> Path | None:
+    r = os.environ.get("XRECON_REFERENCE_ROOT")
+    return Path(r) if r else None
 REF_CPU_SOURCES = ["forward2d.cpp", "backward2d.cpp", "system_matrix2d.cpp", "system_matrix3d.cpp",
                    "forward3d.cpp", "backward3d.cpp"]
 CUDA_INCLUDE = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "include"
@@ -60,15 +64,16 @@ def build_oracle(force: bool = False) -> Path:
 def build_ref(force: bool = False) -> Path | None:
     """Compile the reference CPU operators; returns None when the reference
     tree is absent (the prebuilt .so, if shipped, is then used as is)."""
-    cpu_dir = REFERENCE_ROOT / "src" / "cpu"
-    if not cpu_dir.is_dir():
+    root = reference_root()
+    cpu_dir = root / "src" / "cpu" if root else None
+    if cpu_dir is None or not cpu_dir.is_dir():
         return REF_SO if REF_SO.exists() else None
     srcs = [cpu_dir / s for s in REF_CPU_SOURCES] + [HERE / "ref_shim.cpp"]
     REF_DIR.mkdir(exist_ok=True)
     if force or _stale(REF_SO, srcs):
         # -O3 matches the reference's own C++ flags (setup.py:15).
         _run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread",
-              f"-I{REFERENCE_ROOT / 'include'}", f"-I{CUDA_INCLUDE}",
+              f"-I{root / 'include'}", f"-I{CUDA_INCLUDE}",
               "-o", str(REF_SO)] + [str(s) for s in srcs])
     return REF_SO
 
@@ -76,7 +81,10 @@ def build_ref(force: bool = False) -> Path | None:
 def build_ref_helical(force: bool = False) -> Path | None:
     """Compile the reference's helical CUDA launchers with the shim; returns
     None when the reference tree is absent (a prebuilt .so is used as is)."""
-    src = REFERENCE_ROOT / "src" / "kernels" / "helical_arc3d.cu"
+    root = reference_root()
+    if root is None:
+        return REF_HELICAL_SO if REF_HELICAL_SO.exists() else None
+    src = root / "src" / "kernels" / "helical_arc3d.cu"
     if not src.is_file():
         return REF_HELICAL_SO if REF_HELICAL_SO.exists() else None
     shim = HERE / "ref_helical_shim.cu"
@@ -84,7 +92,7 @@ def build_ref_helical(force: bool = False) -> Path | None:
     if force or _stale(REF_HELICAL_SO, [src, shim]):
         nvcc = str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "bin" / "nvcc")
         _run([nvcc, "-O3", "--use_fast_math", "-lineinfo", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
-              "-Xcompiler", "-fPIC", "-shared", f"-I{REFERENCE_ROOT / 'include'}", "-o", str(REF_HELICAL_SO),
+              "-Xcompiler", "-fPIC", "-shared", f"-I{root / 'include'}", "-o", str(REF_HELICAL_SO),
               str(src), str(shim)])
     return REF_HELICAL_SO
 

@@ -103,7 +103,9 @@ void xo_set_arc_exact(int on) { g_arc_exact = on; }
  * :116-123).  The sum cancels: its rounding, about ulp(|src|), is up to 1e-4
  * of a column near the 45-degree views and the voxel-driven coefficients
  * scale with it.  g_tan_cr = 1 takes tan correctly rounded to float instead
- * of the C library's tanf (which is not always). */
+ * of the C library's tanf (which is not always), and the voxel-driven B and Bw
+ * take the chained boundaries linearised around the direct ones
+ * (chain_overlaps): the CUDA path's arithmetic. */
 static int g_tan_cr = 0;
 
 void xo_set_tan_rounding(int correctly_rounded) { g_tan_cr = correctly_rounded; }
@@ -140,7 +142,8 @@ static double arc_angle(const view_t* v, double k, int nu, double du, double shu
  * 0.5 (a + a_next) of the pair.  Entries go to (ia, ib, len, cang) like
  * overlaps(); D holds the boundaries of arc_angle (the detector ends). */
 static int chain_overlaps(const view_t* v, const double* X, int npix, const double* D, int nu,
-                          double du, double shu, double sod, int* ia, int* ib, double* len, double* cang)
+                          double du, double shu, double sod, int linear, int* ia, int* ib, double* len,
+                          double* cang)
 {
     int n = 0;
     const float duf = (float)du;
@@ -159,7 +162,15 @@ static int chain_overlaps(const view_t* v, const double* X, int npix, const doub
         }
         while (b0 < b1 && k < nu) {
             volatile float tn = v->keep ? t + duf : t - duf;
-            const double Dn = g_arc_exact ? map_angle(v, (double)tn) : map_angle_f(v, tn, sod);
+            double Dn = g_arc_exact ? map_angle(v, (double)tn) : map_angle_f(v, tn, sod);
+            if (linear && !g_arc_exact) {
+                /* direct boundary k + 1 and the derivative of the axis map there */
+                const double td = arc_angle(v, k + 1, nu, du, shu);
+                const double Dd = map_angle_f(v, (float)td, sod);
+                const double tt = tan(td);
+                const double dDdt = v->use_x ? v->sy * (1.0 + tt * tt) : -v->sx * (1.0 + tt * tt) / (tt * tt);
+                Dn = Dd + ((double)tn - td) * dDdt;
+            }
             const double nb = b1 < Dn ? b1 : Dn;
             const double ov = nb - b0;
             if (ov > 0.0) {
@@ -339,7 +350,7 @@ int xo_dd3d(int op, const int* ni, const double* fv, const double* fg, int type,
             double Mv, perp;
             const int npix = line_pixels3d(&g, &v, line, X, &Mv, &perp);
             for (int i = 0; i <= g.D; ++i) Zv[i] = Mv * (z0 + i * g.dz);
-            const int nx = chain ? chain_overlaps(&v, X, npix, D, g.Nu, g.du, g.shu, g.sod, xa, xb, xl, xc)
+            const int nx = chain ? chain_overlaps(&v, X, npix, D, g.Nu, g.du, g.shu, g.sod, g_tan_cr && (op == OP_B || op == OP_BW), xa, xb, xl, xc)
                                  : overlaps(X, npix, D, g.Nu, xa, xb, xl);
             for (int e = 0; e < nx; ++e) {
                 const int p = xa[e], k = xb[e];
@@ -466,7 +477,7 @@ int xo_dd2d(int op, const int* ni, const double* fv, const double* fg, int type,
                                                    : map_point(&v, px, y0 + i * dy);
                 npix = H;
             }
-            const int nx = chain ? chain_overlaps(&v, X, npix, D, Nu, du, shu, sod, xa, xb, xl, xc)
+            const int nx = chain ? chain_overlaps(&v, X, npix, D, Nu, du, shu, sod, g_tan_cr && (op == OP_B || op == OP_BW), xa, xb, xl, xc)
                                  : overlaps(X, npix, D, Nu, xa, xb, xl);
             for (int e = 0; e < nx; ++e) {
                 const int p = xa[e], k = xb[e];

@@ -60,10 +60,11 @@ def _load():
 
 @contextlib.contextmanager
 def tan_rounding(correctly_rounded: bool):
-    """Within the block, the arc axis mapping takes tan rounded correctly to
-    float32 (the CUDA path's arithmetic) instead of the C library's tanf (the
-    reference CPU path's, the default; glibc's is off by one unit for about 4 %
-    of arguments)."""
+    """Within the block, the arc operators take the CUDA path's arithmetic:
+    the axis mapping uses tan rounded correctly to float32 instead of the C
+    library's tanf (the reference CPU path's, the default; glibc's is off by
+    one unit for about 4 % of arguments), and B / Bw take their chained
+    column boundaries linearised around the direct ones."""
     lib = _load()
     lib.xo_set_tan_rounding(int(correctly_rounded))
     try:

@@ -1,9 +1,9 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-Run in a container where the XRecon reference tree is importable (default
-/root/reference, override with XRECON_REFERENCE_ROOT):
+Run where the XRecon reference tree is importable, naming its root in
+XRECON_REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py
+    XRECON_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden.py
 
 The reference's own Python package (xrecon/projector/*.py, pure Python) is
 imported from the reference tree with its native module ``xrecon_C`` served
@@ -47,7 +47,9 @@ import torch
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF_ROOT = Path(os.environ.get("XRECON_REFERENCE_ROOT", "/root/reference"))
+if not os.environ.get("XRECON_REFERENCE_ROOT"):
+    sys.exit("set XRECON_REFERENCE_ROOT to the XRecon reference tree")
+REF_ROOT = Path(os.environ["XRECON_REFERENCE_ROOT"])
 sys.path.insert(0, str(ROOT))
 
 from oracle import refcpu  # noqa: E402

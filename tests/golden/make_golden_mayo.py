@@ -1,9 +1,9 @@
 """Generate tests/golden/mayo_ref.npz from the reference's own Mayo loader.
 
-Run where the XRecon reference tree is importable (default /root/reference,
-override with XRECON_REFERENCE_ROOT):
+Run where the XRecon reference tree is importable, naming its root in
+XRECON_REFERENCE_ROOT:
 
-    python tests/golden/make_golden_mayo.py
+    XRECON_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden_mayo.py
 
 The reference's xrecon/utils/mayo.py and xrecon/utils/mayo_fdk.py import
 pydicom, which is not installed here.  A stand-in ``pydicom`` module serves
@@ -38,7 +38,9 @@ import torch
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF_ROOT = Path(os.environ.get("XRECON_REFERENCE_ROOT", "/root/reference"))
+if not os.environ.get("XRECON_REFERENCE_ROOT"):
+    sys.exit("set XRECON_REFERENCE_ROOT to the XRecon reference tree")
+REF_ROOT = Path(os.environ["XRECON_REFERENCE_ROOT"])
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(HERE))
 

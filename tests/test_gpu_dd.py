@@ -184,3 +184,33 @@ def test_tma_and_plain_paths_match_oracle(cuda, scan):
                 assert rel_l2(plain, exact) < 1e-5, (scan, op, "plain")
     finally:
         _native.set_plain_kernels(False)
+
+
+@pytest.mark.parametrize("scan", ["flat", "arc", "parallel"])
+def test_backprojection_long_column_walks(cuda, scan):
+    """B, Bw and A^T (prefix-table and plain gathers) against the oracle when
+    pixels are much wider than the detector cells: pixels of 4 mm over cells
+    of 0.5 mm put about 16 columns on every pixel (long column walks; on the
+    arc detector, chains that drift several float units from the direct
+    angles); 40 x 44 pixels leave partial CTA tiles at both edges; the second
+    geometry has pixels finer than cells."""
+    from xrecon_b200 import _native
+    cases = [
+        _opts3d(40, 44, 20, 600, 24, 4.0, 4.0, 1.0, 0.5, 1.0, 500., 1000., (1.0, -2.0, 0.5), 0.2, 0.1, scan),
+        _opts3d(72, 56, 33, 40, 20, 0.5, 0.5, 0.6, 2.0, 2.0, 400., 800., (0.3, 0.2, -0.4), -0.5, 0.3, scan),
+    ]
+    ang = np.concatenate([(np.arange(12) * (2 * np.pi / 12) + 0.1), [np.pi / 4, 3 * np.pi / 4]]).astype(np.float32)
+    rng = np.random.default_rng(11)
+    try:
+        for opts in cases:
+            sino = rng.random((1, 1, ang.size, int(opts[4]), int(opts[3]))).astype(np.float32)
+            for op in ("B", "BW", "AT"):
+                exact = O.dd3d(op, sino, opts, ang)
+                _native.set_plain_kernels(False)
+                staged = run(3, op, sino, opts, ang, cuda)
+                _native.set_plain_kernels(True)
+                plain = run(3, op, sino, opts, ang, cuda)
+                assert rel_l2(staged, exact) < 1e-5, (scan, op, "prefix tables")
+                assert rel_l2(plain, exact) < 1e-5, (scan, op, "plain")
+    finally:
+        _native.set_plain_kernels(False)

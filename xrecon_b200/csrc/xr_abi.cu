@@ -281,7 +281,7 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
     l.colM = o;  o = align256(o + V * g.Nu * sizeof(float));
     l.has_arc = chain_ok && arc_chain_op(g, op);
     l.arc = o;
-    if (l.has_arc) o = align256(o + V * (g.Nu + 1) * sizeof(float4));
+    if (l.has_arc) o = align256(o + 2 * V * (g.Nu + 1) * sizeof(float4));
     int eff = op;
     if (g.type == GEO_PARALLEL && dim3d) {
         if (op == OP_B || op == OP_BW) eff = OP_AT;
@@ -1223,7 +1223,7 @@ int xr_ragged2d_plan_create(const xr_ragged2d_instance* inst, int ninst, xr_ragg
         L.colF.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
         L.colM.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
         L.arc.push_back(o);
-        if (g.type == GEO_ARC) o = align256(o + Vs * (g.Nu + 1) * sizeof(float4));  // Bw's chained walks
+        if (g.type == GEO_ARC) o = align256(o + 2 * Vs * (g.Nu + 1) * sizeof(float4));  // Bw's chained walks
         L.imgT.push_back(o); o = align256(o + (size_t)g.H * g.W * sizeof(float));
         L.filt.push_back(o); o = align256(o + Vs * g.Nu * sizeof(float));
     }

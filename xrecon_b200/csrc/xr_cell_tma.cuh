@@ -274,35 +274,43 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                     float pos = f, jn = 1.0f, vj;
                     if (win.ok && bf < 0.999f) {
                         // Rows shorter than a voxel: each row crosses at most
-                        // one voxel boundary, so the walk is a fixed sequence
-                        // of R steps with one predicated advance each.  t is
-                        // clamped to the staged voxels win.z0 .. win.zlast
-                        // (rows -1 and D of the volume arrive as zeros, and
-                        // the window covers every t of the CTA otherwise).
-                        const float tlo = (float)(win.z0 - j0);
-                        const float thi = (float)(win.zlast - j0) + 0.999f;
-                        float tcur = fminf(fmaxf(f, tlo), thi);
-                        const float jlf = floorf(tcur);
-                        float jn = jlf + 1.0f;
-                        const TI* ptr = stage + (size_t)s * stage_elems + (pc - win.p0) +
-                                        (size_t)(j0 + (int)jlf - win.z0) * BP;
-                        int jb = j0 + (int)jlf;  // slice of bcur (bnext: jb + 1)
-                        float bcur = band_smem<TI, NB>(ptr, w, np) * slice_w(jb);
-                        float bnext = band_smem<TI, NB>(ptr + BP, w, np) * slice_w(jb + 1);
+                        // one voxel boundary.  In window slice coordinates
+                        // u = t - (win.z0 - j0) (staged row = floor u), row i
+                        // spans [u_i, u_{i+1}]; with n = floor(u_{i+1}) its
+                        // part below n lies in slice n - 1, the slice of the
+                        // previous row's top, and the rest in slice n:
+                        //   row_i = band(n - 1) max(0, n - u_i)
+                        //         + band(n) (u_{i+1} - max(n, u_i)).
+                        // When the row does not cross, the first term is zero
+                        // whatever band(n - 1) is, so each row forms one band
+                        // and keeps it for the next; floor comes from an FP32
+                        // add of 1.5 * 2^23 to u - 1/2 (at an integer u either
+                        // neighbour gives the same sum).  u is clamped to the
+                        // staged slices 0 .. win.zlast - win.z0 (slices -1 and
+                        // D of the volume arrive as zeros, and the window
+                        // covers every t of the CTA otherwise).
+                        const float fu = f + (float)(j0 - win.z0);
+                        const float uhi = (float)(win.zlast - win.z0) + 0.999f;
+                        const TI* sb = stage + (size_t)s * stage_elems + (pc - win.p0);
+                        constexpr float MAGIC = 12582912.0f;  // 1.5 * 2^23
+                        auto slice_at = [&](float u, float& n) -> float {
+                            const float r = (u - 0.5f) + MAGIC;
+                            n = r - MAGIC;
+                            const int ri = __float_as_int(r) - __float_as_int(MAGIC);
+                            return band_smem<TI, NB>(sb + ri * BP, w, np) * slice_w(win.z0 + ri);
+                        };
+                        float up = fminf(fmaxf(fu, 0.0f), uhi);
+                        float np0;
+                        float bp = slice_at(up, np0);
 #pragma unroll
                         for (int i = 0; i < R; ++i) {
-                            const float t1 = fminf(fmaxf(fmaf(bf, (float)(i + 1), f), tlo), thi);
-                            const float sp = fminf(t1, jn);
-                            // the second term vanishes unless the row crosses jn
-                            const float a = fmaf(bnext, t1 - sp, bcur * (sp - tcur));
-                            const bool adv = t1 > jn;
-                            bcur = adv ? bnext : bcur;
-                            jn = adv ? jn + 1.0f : jn;
-                            ptr = adv ? ptr + BP : ptr;
-                            if (ZW) jb = adv ? jb + 1 : jb;
-                            bnext = band_smem<TI, NB>(ptr + BP, w, np) * slice_w(jb + 1);
-                            acc[i] += a;
-                            tcur = t1;
+                            const float u1 = fminf(fmaxf(fmaf(bf, (float)(i + 1), fu), 0.0f), uhi);
+                            float n;
+                            const float bn = slice_at(u1, n);
+                            acc[i] = fmaf(bp, fmaxf(0.0f, n - up), acc[i]);
+                            acc[i] = fmaf(bn, u1 - fmaxf(n, up), acc[i]);
+                            bp = bn;
+                            up = u1;
                         }
                     } else if (!FINE && win.ok) {
                         // Staged voxels win.z0 .. win.zlast; below the window a

@@ -87,9 +87,10 @@ struct ViewTables {
     float* colM;
     HelView* hel;  // helical scans only, else null
     // circular arc detectors, voxel-driven operators (B, Bw and their
-    // transposes) only, else null: per boundary k = 0..Nu of each view
-    // {float32 angle, tan(angle) as a float pair hi + lo, float32 axis
-    // position}, the inputs of the chained column walk (arc_chain_delta)
+    // transposes) only, else null: two float4 per boundary k = 0..Nu of each
+    // view, [2 (v (Nu + 1) + k)]: {float32 angle t, d(axis)/dt, tan(t) as a
+    // float pair hi + lo} and {float32 axis position, 0, 0, 0}: the inputs of
+    // the chained column walk (ArcChain)
     float4* arc;
 };
 
@@ -203,18 +204,32 @@ __device__ __forceinline__ float arc_chain_delta(const ViewHdr& h, const float4 
 // voxel's first edge, at that column's lower angle (detector kept in order)
 // or at the next column's angle plus du (reversed), and each further
 // boundary angle is the previous one plus du (kept) or minus du (reversed).
-// next() steps to the following boundary and returns its axis offset from
-// the direct boundary.  Boundaries far from k0 drift from the direct ones by
-// the accumulated roundings, which the reference's results carry.
+// The step to boundary j returns its axis offset from the direct boundary:
+//   next_exact:  the float axis mapping of the chained angle (arc_chain_delta);
+//   next_linear: (t - t_j) d(axis)/dt at the direct angle t_j.
+// The chained angle drifts from the direct one by the accumulated roundings
+// (several float units after a few columns), which the reference's results
+// carry.  The voxel-owned gathers (B, Bw) take the linear step: it leaves
+// out only the float rounding of the chained axis positions, which their
+// sums over columns and views average away (within 4e-6 of the reference
+// where the exact step is within 3.9e-6); the cell-owned transposes, which
+// do not average it, take the exact step.
 struct ArcChain {
     float t, step;
+    // e: the view's arc entries (two float4 per boundary)
     __device__ __forceinline__ void start(const float4* __restrict__ e, int k0, int keep, float du) {
         step = keep ? du : -du;
-        t = keep ? e[k0].x : __fadd_rn(e[k0 + 1].x, du);
+        t = keep ? e[2 * k0].x : __fadd_rn(e[2 * (k0 + 1)].x, du);
     }
-    __device__ __forceinline__ float next(const ViewHdr& h, const float4 e) {
+    __device__ __forceinline__ float next_linear(const float4* __restrict__ e, int j) {
         t = __fadd_rn(t, step);
-        return arc_chain_delta(h, e, t);
+        const float4 a = e[2 * j];
+        return __fsub_rn(t, a.x) * a.y;
+    }
+    __device__ __forceinline__ float next_exact(const ViewHdr& h, const float4* __restrict__ e, int j) {
+        t = __fadd_rn(t, step);
+        const float4 a = e[2 * j];
+        return arc_chain_delta(h, make_float4(a.x, a.z, a.w, e[2 * j + 1].x), t);
     }
 };
 

@@ -69,14 +69,19 @@ __global__ void setup_views_kernel(const Geom g, const int dim3d, const float* _
 }
 
 // Axis position of arc boundary k with the reference's float32 rounding, and
-// its {angle, tan hi, tan lo, axis} entry.
-__device__ __forceinline__ double arc_boundary_f(const Geom& g, const ViewHdr& h, int k, float angle, float4& e) {
+// its two entries of ViewTables::arc (see there).
+__device__ __forceinline__ double arc_boundary_f(const Geom& g, const ViewHdr& h, int k, float angle, float4& ea,
+                                                 float4& eb) {
     const float tk = arc_angle_f(g, h.keep, (float)k, angle);
     const double T = tan((double)tk);
     const float hi = __double2float_rn(T);
     const float lo = __double2float_rn(T - (double)hi);
     const float Df = arc_axis_f(h, hi);
-    e = make_float4(tk, hi, lo, Df);
+    // derivative of the axis map: x axis sy (1 + T^2), y axis -sx (1 + T^2) / T^2
+    const double sec2 = 1.0 + T * T;
+    const double dD = h.use_x ? (double)h.syf * sec2 : -(double)h.sxf * sec2 / (T * T);
+    ea = make_float4(tk, (float)dD, hi, lo);
+    eb = make_float4(Df, 0.0f, 0.0f, 0.0f);
     return (double)Df;
 }
 
@@ -89,9 +94,12 @@ __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d,
 
     const double uscale = (dim3d && g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
     const size_t ob = (size_t)v * (g.Nu + 1) + k;
-    float4 e;
-    const double Dk = arcf ? arc_boundary_f(g, h, k, angle, e) : boundary_axis(g, h, (double)k, uscale);
-    if (arcf && vt.arc) vt.arc[ob] = e;
+    float4 ea, eb;
+    const double Dk = arcf ? arc_boundary_f(g, h, k, angle, ea, eb) : boundary_axis(g, h, (double)k, uscale);
+    if (arcf && vt.arc) {
+        vt.arc[2 * ob] = ea;
+        vt.arc[2 * ob + 1] = eb;
+    }
     double A, B;
     boundary_line_coeffs(g, h, Dk, A, B);
     vt.bA[ob] = A;
@@ -99,7 +107,7 @@ __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d,
     if (k >= g.Nu) return;
 
     const size_t oc = (size_t)v * g.Nu + k;
-    const double Dk1 = arcf ? arc_boundary_f(g, h, k + 1, angle, e) : boundary_axis(g, h, (double)k + 1.0, uscale);
+    const double Dk1 = arcf ? arc_boundary_f(g, h, k + 1, angle, ea, eb) : boundary_axis(g, h, (double)k + 1.0, uscale);
     const double dperp = h.use_x ? g.dy : g.dx;
     if (g.type == GEO_PARALLEL) {
         // forward3d.cpp:58,98 (xy_scale / dv) and system_matrix2d.cpp:109.
@@ -193,8 +201,8 @@ __device__ __forceinline__ void arc_first_pixel_bounds(const Geom& g, const View
     ArcChain ch;
     ch.start(ea, k0, h.keep, (float)g.du);
     for (int j = k0 + 1; j < k; ++j) ch.t = __fadd_rn(ch.t, ch.step);
-    const float dk = ch.next(h, ea[k]);
-    float dk1 = ch.next(h, ea[k + 1]);
+    const float dk = ch.next_exact(h, ea, k);
+    float dk1 = ch.next_exact(h, ea, k + 1);
     if (k + 1 == Nu) dk1 = fminf(dk1, 0.0f);
     u0 = fmaf(dk, qd, (float)(pk - (double)pa));
     u1 = fmaf(dk1, qd, (float)(pk1 - (double)pa));
@@ -232,12 +240,12 @@ cell_gather3d_kernel(const Geom g, const ViewTables vt, const TI* __restrict__ v
     const double zr0 = zd0 + r0 * dvv;
     // arc detector, B^T / Bw^T: chained column walks (see cell2d_sum)
     const bool chain = (MODE == OP_BT || MODE == OP_BWT) && !HEL && vt.arc;
-    const float4* __restrict__ ea = chain ? vt.arc + (size_t)v * (Nu + 1) : nullptr;
+    const float4* __restrict__ ea = chain ? vt.arc + 2 * (size_t)v * (Nu + 1) : nullptr;
     float d1 = 0.0f;
     if (chain) {
         ArcChain ch;
         ch.start(ea, k, h.keep, (float)g.du);
-        d1 = ch.next(h, ea[k + 1]);
+        d1 = ch.next_exact(h, ea, k + 1);
         if (k + 1 == Nu) d1 = fminf(d1, 0.0f);
     }
 
@@ -517,7 +525,7 @@ vox_gather3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const TI*
         };
         if (MODE != OP_AT && vt.arc) {
             // arc detector: the pixel's columns walked with chained angles
-            const float4* __restrict__ ea = vt.arc + (size_t)v * (Nu + 1);
+            const float4* __restrict__ ea = vt.arc + 2 * (size_t)v * (Nu + 1);
             const double qd = q / h.dpix;  // pixels per axis unit
             int k = ka;
             double pkl = fma(bB[k], (double)L, bA[k]);
@@ -530,7 +538,7 @@ vox_gather3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const TI*
             ArcChain ch;
             ch.start(ea, k, h.keep, (float)g.du);
             for (;;) {
-                float d = ch.next(h, ea[k + 1]);
+                float d = ch.next_linear(ea, k + 1);
                 if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
                 pk1 = fma((double)d, qd, pk1);
                 const float wf = (float)(fmin(dp + 1.0, pk1) - fmax(dp, pkl));
@@ -602,12 +610,12 @@ __device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt,
     // walk of a pixel whose first edge lies in this column (every pixel but
     // the band's first); the same on every line
     const bool chain = (MODE == OP_BT || MODE == OP_BWT) && vt.arc;
-    const float4* __restrict__ ea = chain ? vt.arc + (size_t)v * (Nu + 1) : nullptr;
+    const float4* __restrict__ ea = chain ? vt.arc + 2 * (size_t)v * (Nu + 1) : nullptr;
     float d1 = 0.0f;
     if (chain) {
         ArcChain ch;
         ch.start(ea, k, h.keep, (float)g.du);
-        d1 = ch.next(h, ea[k + 1]);
+        d1 = ch.next_exact(h, ea, k + 1);
         if (k + 1 == Nu) d1 = fminf(d1, 0.0f);
     }
     float acc = 0.0f;
@@ -731,7 +739,7 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
         const double dp = (double)p, dL = (double)L;
         if (MODE != OP_AT && vt.arc) {
             // arc detector: the pixel's columns walked with chained angles
-            const float4* __restrict__ ea = vt.arc + (size_t)v * (Nu + 1);
+            const float4* __restrict__ ea = vt.arc + 2 * (size_t)v * (Nu + 1);
             const float qd = (float)(fma(h.q1, dL, h.q0) / h.dpix);  // pixels per axis unit
             int k = ka;
             float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
@@ -744,7 +752,7 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
             ArcChain ch;
             ch.start(ea, k, h.keep, (float)g.du);
             for (;;) {
-                float d = ch.next(h, ea[k + 1]);
+                float d = ch.next_linear(ea, k + 1);
                 if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
                 pk1 = fmaf(d, qd, pk1);
                 const float wd = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);

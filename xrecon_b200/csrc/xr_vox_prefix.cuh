@@ -204,10 +204,10 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         float qd = 0.0f;
         const float4* __restrict__ ea = nullptr;
         if (CHAIN) {
-            ea = vt.arc + (size_t)v * (Nu + 1);
+            ea = vt.arc + 2 * (size_t)v * (Nu + 1);
             qd = (float)(q / h.dpix);  // pixels per axis unit on this line
             ch.start(ea, k, keep, gf.du);
-            float d = ch.next(h, ea[k + 1]);
+            float d = ch.next_linear(ea, k + 1);
             if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
             pk1 = fmaf(d, qd, pk1);
         }
@@ -291,7 +291,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             if (pkl >= 1.0f) break;  // column k starts right of the pixel
             pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
             if (CHAIN) {
-                float d = ch.next(h, ea[k + 1]);
+                float d = ch.next_linear(ea, k + 1);
                 if (k + 1 == Nu) d = fminf(d, 0.0f);
                 pk1 = fmaf(d, qd, pk1);
             }
