@@ -409,6 +409,7 @@ def helical_measure(dev, reps: int = 2, turns=None):
         out["B_ms"] = timed(lambda: P.backprojection(sino, ang))
         out["Bw_ms"] = timed(lambda: P.backprojection_weighted(sino, ang))
         out["fdk_ms"] = timed(lambda: P.filtered_backprojection(sino, ang))
+        out["BwT_ms"] = timed(lambda: P.backprojection_weighted_t(vol, ang))
     nvox = h["W"] * h["H"] * h["D"]
     out["gvoxel_views_per_turn_per_s_fdk"] = nvox * h["views_per_turn"] / (out["fdk_ms"] / 1e3) / 1e9
     out["views"] = int(ang.numel())
@@ -861,6 +862,11 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
     hbm, src = peaks()
     dom_t = max(t_a, t_b)
     dom = "cell_tma3d_kernel (projection A)" if t_a >= t_b else "vox_prefix3d_kernel (backprojection B)"
+    # what holds the kernel below the HBM roofline, from its ncu profile
+    # (profiles/cell_tma3d_A_cone_flat_64views.md, vox_prefix3d_B_cone_flat_64views.md)
+    limiter = ("instruction issue: ~74 % issue active, 'not selected' stalls, DRAM ~32 % of peak"
+               if t_a >= t_b else
+               "table-lookup latency and issue: ~68 % issue active, long-scoreboard (L1 hit) stalls, DRAM idle")
     wl = dict(WL, V=nv)
     achieved = algo_bytes_op(wl) / dom_t / 1e9
     traffic = None
@@ -881,7 +887,7 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
                    "ms_backprojection": t_b * 1e3,
                    "l2": "inputs larger than L2 (volume 256 MiB, sinogram 1.41 GiB)",
                    "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "limiter": limiter, "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
                      "algorithmic_bytes_per_launch": algo_bytes_op(wl),
                      # every voxel and detector cell touched once per operator
@@ -934,6 +940,10 @@ def main():
                     help="profiling: an evenly strided subset of the workload's views")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other named configurations (2D FBP, 3D FDK, cone-arc least squares)")
+    ap.add_argument("--only", choices=["c1", "c2", "c3"], default=None,
+                    help="profiling: only one of the other named configurations (one JSON line)")
+    ap.add_argument("--plain", action="store_true",
+                    help="profiling: run every operator through the plain (non-staged) kernels")
     ap.add_argument("--replicas", action="store_true",
                     help="with several GPUs: independent replicas of the workload (weak scaling) instead of one "
                          "problem split over the GPUs (strong scaling, the default)")
@@ -943,6 +953,14 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank)
+    if args.plain:
+        from xrecon_b200 import _native
+        _native.set_plain_kernels(True)
+    if args.only:
+        import torch
+        fn = {"c1": config_c1, "c2": config_c2, "c3": config_c3}[args.only]
+        print(json.dumps({args.only: fn(torch.device("cuda:0"), not args.no_cpu)}))
+        return 0
     if args.helical_only:
         import torch
         print(json.dumps({"helical_arc_512x512x128_736x64_5x1152views":
