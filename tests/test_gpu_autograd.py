@@ -44,6 +44,30 @@ def test_function_backward_is_oracle_transpose(cuda, name, op, adj):
     assert rel_l2(g.cpu().numpy(), exact) < 1e-5
 
 
+FN2 = {"A": "Projection2d", "AT": "ProjectionTranspose2d", "B": "BackProjection2d", "BT": "BackProjectionTranspose2d",
+       "BW": "WeightedBackProjection2d", "BWT": "WeightedBackProjectionTranspose2d"}
+
+
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_function_gradients_equal_the_reference_autograd_gradients(cuda, dim, scan):
+    """The gradient each CUDA Function returns for the reference fixtures'
+    input and upstream gradient equals the gradient the reference's own
+    autograd Function returned (tests/golden/make_golden.py autograd, its
+    CPU kernels behind functions.py:96-302), to 1e-5."""
+    from conftest import load_golden
+    from xrecon_b200 import functions as F
+    g = load_golden(f"autograd{dim}d_{scan}")
+    opts = torch.from_numpy(g["options"]).to(cuda)
+    ang = torch.from_numpy(g["angles"]).to(cuda)
+    for op in ("A", "AT", "B", "BT", "BW", "BWT"):
+        name = FN2[op] if dim == 2 else FN2[op][:-2] + "3d"
+        x = torch.from_numpy(g[f"{op}_x"]).to(cuda).requires_grad_(True)
+        out = getattr(F, name).apply(x, opts, ang)
+        (grad,) = torch.autograd.grad((out * torch.from_numpy(g[f"{op}_u"]).to(cuda)).sum(), x)
+        assert rel_l2(grad.cpu().numpy(), g[f"{op}_grad"]) < 1e-5, (dim, scan, op)
+
+
 def _small_problem(cuda, B=2):
     opts = _opts3d_arc(32, 28, 8, 48, 12)
     ang = np.linspace(0, 2 * np.pi, 40, endpoint=False).astype(np.float32)

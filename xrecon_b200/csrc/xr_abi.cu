@@ -496,7 +496,9 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
                 // values, and so the results, are the same)
                 float* vf = reinterpret_cast<float*>(ws + l.volF);
                 const size_t n = (size_t)nbatch * g.D * g.H * g.W;
-                widen_kernel<TI><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, vf, n);
+                const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(vf)) & 15) == 0;
+                const size_t nt = vec ? (n + 7) / 8 : n;
+                widen_kernel<TI><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(in, vf, n, vec);
                 if (int e = check_cuda("widen")) return e;
                 rc = run_cell_tma<float, TO>(eff, g, vf, out, nbatch, nview, ws, l, vt, st, z0dz, zd0, dvv, cw);
             } else {

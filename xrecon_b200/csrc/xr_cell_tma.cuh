@@ -88,11 +88,13 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
     return w;
 }
 
-// After a wait gave up: lines L and L + 1 may still have copies in flight.
-// The issuing thread lets them land (or gives up once more) before it exits,
-// which keeps the CTA's shared memory allocated until then.
-__device__ __noinline__ void drain_stages(uint64_t* bar, int L, int nlines) {
-    for (int Lp = L; Lp < min(L + 2, nlines); ++Lp)
+// After a wait gave up: only the last two lines issued, `last` - 1 and
+// `last`, may still have copies in flight (each earlier line's copy was seen
+// to land by the issuing thread before it issued the next line into that
+// stage).  The issuing thread lets them land, or gives up once more, before
+// the CTA exits, which keeps its shared memory allocated until then.
+__device__ __noinline__ void drain_stages(uint64_t* bar, int last) {
+    for (int Lp = max(last - 1, 0); Lp <= last; ++Lp)
         mbar_wait_bounded(&bar[Lp & 1], (unsigned)((Lp >> 1) & 1));
 }
 
@@ -190,12 +192,15 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar[s])) : "memory");
         }
     };
-    __shared__ int s_abort[2];
+    // Set (0 -> 1, never back) by a wait that runs out.  Waits that find it
+    // set give up at once, no further line is issued, nothing is stored.
+    __shared__ int s_abort;
+    volatile int* abort = &s_abort;
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         fence_barrier_init();
-        s_abort[0] = s_abort[1] = 0;
+        s_abort = 0;
     }
     // the line windows, evaluated by all threads in parallel (FP64)
     for (int L = tid; L < nlines; L += blockDim.x * blockDim.y) {
@@ -207,9 +212,10 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     for (int i = tid; i < 2 * BP; i += blockDim.x * blockDim.y)
         stage[(size_t)(i / BP) * stage_elems + (size_t)BZ * BP + (i % BP)] = TI(0.0f);
     __syncthreads();
+    int last = -1;  // last line issued (issuing thread)
     if (tid == 0) {
-        issue(0, 0);
-        if (nlines > 1) issue(1, 1);
+        if (nlines > 0) issue(0, 0), last = 0;
+        if (nlines > 1) issue(1, 1), last = 1;
     }
 
     float acc[R];
@@ -218,15 +224,13 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     const double zr0 = zd0 + r0 * dvv;
     const float dpdz = (float)(h.dpix * g.dz);
 
-    // A wait that gives up sets the stage's abort flag; after the line's
-    // barrier every thread sees it and the CTA returns: no further copy is
-    // issued, nothing is stored.  Two flags alternate with the stages, so a
-    // flag is only read after the barrier that closes its own line, before
-    // any thread can reach the next line that writes it.
+    // After a wait gave up, the CTA still walks its remaining lines (every
+    // read stays inside the staged windows, whatever they hold) so that all
+    // threads meet every barrier; the results are dropped at the end.
     for (int L = 0; L < nlines; ++L) {
         const int s = L & 1;
         const unsigned parity = (unsigned)((L >> 1) & 1);
-        if (!mbar_wait_bounded(&bar[s], parity)) s_abort[s] = 1;  // the stage's values then go unused
+        mbar_wait_bounded(&bar[s], parity, abort);
         CellWindow win;
         {
             const int4 wi = wins[L];
@@ -369,14 +373,16 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
             }
         }
         __syncthreads();
-        if (s_abort[s]) {
-            if (tid == 0) drain_stages(bar, L, nlines);
-            return;
-        }
-        if (tid == 0 && L + 2 < nlines) {
+        if (tid == 0 && L + 2 < nlines && !*abort) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             issue(L + 2, s);
+            last = L + 2;
         }
+    }
+    // every wait ended before the last barrier, so all threads read the same
+    if (*abort) {
+        if (tid == 0) drain_stages(bar, last);
+        return;
     }
 
     if (!active) return;

@@ -102,6 +102,9 @@ template <> __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat
     return __bfloat162float(__ldg(p));
 }
 template <> __device__ __forceinline__ float ld<__half>(const __half* p) { return __half2float(__ldg(p)); }
+// value conversions (registers, no load)
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
 
 template <typename T> __device__ __forceinline__ void st(T* p, float v);
 template <> __device__ __forceinline__ void st<float>(float* p, float v) { *p = v; }

@@ -20,8 +20,8 @@ __device__ unsigned int g_device_error = 0;
 
 constexpr unsigned XR_DEVERR_TMA_TIMEOUT = 1u;
 
-// Poll limits of the bounded waits, per device (xr_set_wait_limits).  A poll
-// of an mbarrier suspends for at most about a microsecond, so the default
+// Poll limits of the bounded waits, per device (xr_set_wait_limits).  After
+// its first poll an mbarrier wait polls with a 1 us time hint, so the default
 // gives up after roughly 0.02 to 1 s; a TMA box lands in microseconds.
 constexpr long long XR_WAIT_LIMIT_DEFAULT = 1ll << 20;
 __device__ long long g_wait_limit = XR_WAIT_LIMIT_DEFAULT;
@@ -53,25 +53,50 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
                  : "memory");
 }
 
-// One poll: suspends until the phase completes or about 1000 ns pass.
+// One poll.  Without a time hint it suspends the thread until the phase
+// completes or a system-dependent limit passes; with one, for at most about
+// `ns` nanoseconds.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity, unsigned ns) {
     unsigned ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
         : "memory");
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`; false (and the device error word
-// set) when the limit is reached.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+// The rest of a wait whose first poll failed: polls of at most about a
+// microsecond up to the limit, giving up early once `abort` (a CTA-wide flag
+// in shared memory, or null) is set.  A wait that runs out sets the device
+// error word and `abort`.
+__device__ __forceinline__ bool mbar_wait_slow(uint64_t* bar, unsigned parity, volatile int* abort) {
     const long long limit = *(volatile long long*)&g_wait_limit;
-    for (long long i = 0; i < limit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
+    for (long long i = 1; i < limit; ++i) {
+        if (abort && *abort) return false;
+        if (mbar_try_wait(bar, parity, 1000u)) return true;
+    }
     atomicOr(&g_device_error, XR_DEVERR_TMA_TIMEOUT);
+    if (abort) *abort = 1;
     return false;
+}
+
+// Bounded wait for phase `parity` of `bar`; false when it gives up.  The
+// first poll is usually the whole wait; it takes no time hint (a hinted first
+// poll made the helical projection 4 % slower) and reads nothing but the
+// barrier.  Only a longer wait reads the poll limit.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, volatile int* abort = nullptr) {
+    if (mbar_try_wait(bar, parity)) return true;
+    return mbar_wait_slow(bar, parity, abort);
 }
 
 // 4D tiled TMA load of one box into shared memory, completing on `bar`.
