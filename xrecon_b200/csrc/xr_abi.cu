@@ -22,6 +22,7 @@
 #include "xr_sysmat.cuh"
 #include "xr_rebin.cuh"
 #include "xr_helical.cuh"
+#include "xr_fft_filter.cuh"
 #include "xr_ctpd.hpp"
 #include "../../include/xrecon_b200.h"
 
@@ -961,6 +962,27 @@ int noalloc_scratch(void** ptr) {
 }
 
 }  // namespace
+
+// FFT filter (xr_fft_filter.cuh) of `nrows` rows from `rows_src`: one wave of
+// CTAs, each transforming the filter once and then a share of the row pairs.
+template <typename RowsT>
+int launch_fft_filter(const RowsT& rows_src, float* out, int nrows, int Nu, const float* filt, cudaStream_t st) {
+    const int m = fft_log2_for(Nu);
+    const size_t smem = fft_filter_smem(m);
+    auto k = fft_filter_kernel<RowsT>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
+    int dev = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, XR_FFT_THREADS, smem) != cudaSuccess || per_sm < 1)
+        return fail(XR_ERR_CUDA, "cannot size the FFT filter grid");
+    const int npairs = (nrows + 1) / 2;
+    const int grid = std::min(npairs, per_sm * nsm);
+    k<<<grid, XR_FFT_THREADS, smem, st>>>(rows_src, out, nrows, Nu, filt, m);
+    return XR_OK;
+}
+
 }  // namespace xr
 
 extern "C" {
@@ -1022,6 +1044,18 @@ int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, i
         return xr::fail(XR_ERR_INVALID_ARGUMENT, "bad filter sizes");
     if (nrows == 0) return XR_OK;
     if (!xr::dtype_ok(dtype_in)) return xr::fail(XR_ERR_INVALID_ARGUMENT, "unsupported dtype %d", dtype_in);
+    if (!xr::g_force_plain && xr::fft_log2_for(Nu) <= xr::XR_FFT_MAX_LOG) {
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        int rc;
+        if (dtype_in == xr::DT_F32)
+            rc = xr::launch_fft_filter(xr::SinoRows<float>{static_cast<const float*>(in), cosw, parker, Nu, nview, rows_per_view}, out, nrows, Nu, filt, st);
+        else if (dtype_in == xr::DT_BF16)
+            rc = xr::launch_fft_filter(xr::SinoRows<__nv_bfloat16>{static_cast<const __nv_bfloat16*>(in), cosw, parker, Nu, nview, rows_per_view}, out, nrows, Nu, filt, st);
+        else
+            rc = xr::launch_fft_filter(xr::SinoRows<__half>{static_cast<const __half*>(in), cosw, parker, Nu, nview, rows_per_view}, out, nrows, Nu, filt, st);
+        if (rc) return rc;
+        return xr::check_cuda("fft_filter");
+    }
     constexpr int OUTS = 8;
     // threads per row (a warp multiple covering Nu / 8 outputs), rows per CTA
     const int tpr = std::min(256, ((Nu + OUTS - 1) / OUTS + 31) / 32 * 32);
@@ -1145,6 +1179,14 @@ int xr_rebin_parallel(const void* in, int dtype_in, float* out, int nbatch, int 
     // rebinning fused into the filter kernel's row loads
     constexpr int OUTS = 8;
     const int nrows = (int)((long long)nbatch * nview_out * Nv);
+    if (!g_force_plain && fft_log2_for(Nt) <= XR_FFT_MAX_LOG) {
+        int rc;
+        if (dtype_in == DT_F32) rc = launch_fft_filter(RebinRows<float>{static_cast<const float*>(in), r}, out, nrows, Nt, filt, st);
+        else if (dtype_in == DT_BF16) rc = launch_fft_filter(RebinRows<__nv_bfloat16>{static_cast<const __nv_bfloat16*>(in), r}, out, nrows, Nt, filt, st);
+        else rc = launch_fft_filter(RebinRows<__half>{static_cast<const __half*>(in), r}, out, nrows, Nt, filt, st);
+        if (rc) return rc;
+        return check_cuda("rebin_fft_filter");
+    }
     const int tpr = std::min(256, ((Nt + OUTS - 1) / OUTS + 31) / 32 * 32);
     const int rpc = std::max(1, 256 / tpr);
     const size_t smem = ((size_t)(filt_taps_smem(Nt) + 3) / 4 * 4 + (size_t)rpc * filt_row_pitch(Nt)) * sizeof(float);
