@@ -964,7 +964,7 @@ int noalloc_scratch(void** ptr) {
 }  // namespace
 
 // FFT filter (xr_fft_filter.cuh) of `nrows` rows from `rows_src`: one wave of
-// CTAs, each transforming the filter once and then a share of the row pairs.
+// CTAs, each transforming the filter once and then a share of the rows.
 template <typename RowsT>
 int launch_fft_filter(const RowsT& rows_src, float* out, int nrows, int Nu, const float* filt, cudaStream_t st) {
     const int m = fft_log2_for(Nu);
@@ -977,8 +977,8 @@ int launch_fft_filter(const RowsT& rows_src, float* out, int nrows, int Nu, cons
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, XR_FFT_THREADS, smem) != cudaSuccess || per_sm < 1)
         return fail(XR_ERR_CUDA, "cannot size the FFT filter grid");
-    const int npairs = (nrows + 1) / 2;
-    const int grid = std::min(npairs, per_sm * nsm);
+    const int nquad = (nrows + 3) / 4;  // four rows per CTA iteration
+    const int grid = std::min(nquad, per_sm * nsm);
     k<<<grid, XR_FFT_THREADS, smem, st>>>(rows_src, out, nrows, Nu, filt, m);
     return XR_OK;
 }

@@ -10,10 +10,11 @@
 // transform of a real sequence, so the real and imaginary parts of
 // IFFT(FFT(z) FFT(g)) are the two filtered rows.
 //
-// One CTA owns a row pair at a time in shared memory.  The forward transform
-// is decimation in frequency (natural order in, bit-reversed out), the
-// inverse decimation in time (bit-reversed in, natural out), so no pass
-// permutes: the spectrum of g is kept in the same bit-reversed order.  The
+// One CTA owns four rows (two transforms) at a time in shared memory.  The
+// forward transform is decimation in frequency (natural order in,
+// bit-reversed out), the inverse decimation in time (bit-reversed in, natural
+// out), so no pass permutes: the spectrum of g is kept in the same
+// bit-reversed order.  The
 // inverse is a forward transform of the conjugate, IFFT(Y) = conj(FFT(conj
 // Y)) / M.  Stages are fused in pairs (radix 4); an odd power of two adds one
 // radix-2 stage.  Rows are FP32 with FP32 twiddles (rounded from FP64); each
@@ -34,11 +35,22 @@ __host__ __device__ inline int fft_log2_for(int Nu) {
     return m;
 }
 
-// data (double2 while g is transformed, float2 rows after), FP64 and FP32
-// twiddles, the spectrum of g
+// Radix-4 stage pairs of a length-2^m transform work on groups of 4h with
+// h = h0, 4 h0, ..., M / 4 (h0 = 2 for odd m, else 1); both directions use
+// the same h.  Their FP32 twiddles {W_2h^j, W_4h^j}, j < h, are stored per
+// stage, contiguous in j, at fft_tw_offset(h): a warp's lanes then read
+// neighbouring entries instead of entries M / 2h apart, which fall on one
+// shared-memory bank.
+__host__ __device__ inline int fft_h0(int m) { return (m & 1) ? 2 : 1; }
+__host__ __device__ inline int fft_tw_offset(int h, int m) { return (h - fft_h0(m)) / 3; }
+__host__ __device__ inline int fft_tw_count(int m) { return ((1 << m) - fft_h0(m)) / 3; }
+
+// Shared memory: the data (double2 while g is transformed, then two float2
+// row buffers), the FP64 twiddles of that transform (then the spectrum of
+// g, the same size), the per-stage FP32 twiddles.
 __host__ __device__ inline size_t fft_filter_smem(int m) {
     const size_t M = (size_t)1 << m;
-    return M * sizeof(double2) + (M / 2) * sizeof(double2) + M * sizeof(float2) + (M / 2) * sizeof(float2);
+    return M * sizeof(double2) + (M / 2) * sizeof(double2) + (size_t)fft_tw_count(m) * sizeof(float4);
 }
 
 __device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -121,19 +133,86 @@ __device__ void fft_dit(C* a, const C* __restrict__ tw, const int m) {
     }
 }
 
-// One CTA per row pair at a time (grid-stride over pairs).  Rows is a row
-// source as for fbp_filter_kernel (weights applied on load).
+// fft_dif / fft_dit on NB consecutive FP32 arrays of length M at once (one
+// barrier per stage pair for all of them), with the per-stage twiddles.
+template <int NB>
+__device__ void fft_dif_rows(float2* a, const float4* __restrict__ tws, const int m) {
+    const int M = 1 << m;
+    for (int h = M / 4; h >= 1; h /= 4) {
+        const float4* __restrict__ th = tws + fft_tw_offset(h, m);
+        for (int i = threadIdx.x; i < NB * (M / 4); i += blockDim.x) {
+            const int f = i >> (m - 2), ii = i & (M / 4 - 1);
+            const int j = ii & (h - 1), base = f * M + (ii - j) * 4 + j;
+            const float2 x0 = a[base], x1 = a[base + h], x2 = a[base + 2 * h], x3 = a[base + 3 * h];
+            const float4 w = th[j];
+            const float2 w1 = make_float2(w.x, w.y), w2 = make_float2(w.z, w.w);
+            const float2 y0 = c_add(x0, x2), y2 = c_mul(c_sub(x0, x2), w2);
+            const float2 y1 = c_add(x1, x3), y3 = c_mul(c_mul_mi(c_sub(x1, x3)), w2);
+            a[base] = c_add(y0, y1);
+            a[base + h] = c_mul(c_sub(y0, y1), w1);
+            a[base + 2 * h] = c_add(y2, y3);
+            a[base + 3 * h] = c_mul(c_sub(y2, y3), w1);
+        }
+        __syncthreads();
+    }
+    if (m & 1) {
+        for (int i = threadIdx.x; i < NB * (M / 2); i += blockDim.x) {
+            const float2 x0 = a[2 * i], x1 = a[2 * i + 1];
+            a[2 * i] = c_add(x0, x1);
+            a[2 * i + 1] = c_sub(x0, x1);
+        }
+        __syncthreads();
+    }
+}
+
+template <int NB>
+__device__ void fft_dit_rows(float2* a, const float4* __restrict__ tws, const int m) {
+    const int M = 1 << m;
+    int h = 1;
+    if (m & 1) {
+        for (int i = threadIdx.x; i < NB * (M / 2); i += blockDim.x) {
+            const float2 x0 = a[2 * i], x1 = a[2 * i + 1];
+            a[2 * i] = c_add(x0, x1);
+            a[2 * i + 1] = c_sub(x0, x1);
+        }
+        __syncthreads();
+        h = 2;
+    }
+    for (; h < M; h *= 4) {
+        const float4* __restrict__ th = tws + fft_tw_offset(h, m);
+        for (int i = threadIdx.x; i < NB * (M / 4); i += blockDim.x) {
+            const int f = i >> (m - 2), ii = i & (M / 4 - 1);
+            const int j = ii & (h - 1), base = f * M + (ii - j) * 4 + j;
+            const float2 x0 = a[base], x1 = a[base + h], x2 = a[base + 2 * h], x3 = a[base + 3 * h];
+            const float4 w = th[j];
+            const float2 w1 = make_float2(w.x, w.y), w2 = make_float2(w.z, w.w);
+            const float2 t1 = c_mul(x1, w1), t3 = c_mul(x3, w1);
+            const float2 y0 = c_add(x0, t1), y1 = c_sub(x0, t1);
+            const float2 y2 = c_add(x2, t3), y3 = c_sub(x2, t3);
+            const float2 u2 = c_mul(y2, w2), u3 = c_mul_mi(c_mul(y3, w2));
+            a[base] = c_add(y0, u2);
+            a[base + 2 * h] = c_sub(y0, u2);
+            a[base + h] = c_add(y1, u3);
+            a[base + 3 * h] = c_sub(y1, u3);
+        }
+        __syncthreads();
+    }
+}
+
+// One CTA per four rows at a time (grid-stride): two complex transforms
+// side by side.  Rows is a row source as for fbp_filter_kernel (weights
+// applied on load).
 template <typename Rows>
 __global__ void __launch_bounds__(XR_FFT_THREADS)
 fft_filter_kernel(const Rows src, float* __restrict__ out, const int nrows, const int Nu,
                   const float* __restrict__ filt, const int m) {
     extern __shared__ __align__(16) unsigned char fsm[];
     const int M = 1 << m;
-    double2* d64 = reinterpret_cast<double2*>(fsm);             // [M], FP64 setup
-    float2* rows = reinterpret_cast<float2*>(fsm);               // [M], aliases d64 afterwards
-    double2* tw64 = reinterpret_cast<double2*>(fsm + (size_t)M * sizeof(double2));
-    float2* spec = reinterpret_cast<float2*>(fsm + (size_t)M * sizeof(double2) + (size_t)(M / 2) * sizeof(double2));
-    float2* tw32 = spec + M;
+    double2* d64 = reinterpret_cast<double2*>(fsm);              // [M], FP64 setup
+    float2* rows = reinterpret_cast<float2*>(fsm);                // [2][M], aliases d64 afterwards
+    double2* tw64 = reinterpret_cast<double2*>(fsm + (size_t)M * sizeof(double2));  // [M / 2], setup
+    float2* spec = reinterpret_cast<float2*>(tw64);               // [M], aliases tw64 afterwards
+    float4* tws = reinterpret_cast<float4*>(fsm + (size_t)M * sizeof(double2) + (size_t)(M / 2) * sizeof(double2));
     const int tid = threadIdx.x, nt = blockDim.x;
 
     // twiddles, and g in natural order
@@ -141,7 +220,14 @@ fft_filter_kernel(const Rows src, float* __restrict__ out, const int nrows, cons
         double s, c;
         sincospi(-2.0 * (double)k / (double)M, &s, &c);
         tw64[k] = make_double2(c, s);
-        tw32[k] = make_float2((float)c, (float)s);
+    }
+    for (int h = fft_h0(m); h <= M / 4; h *= 4) {
+        for (int j = tid; j < h; j += nt) {
+            double s1, c1, s2, c2;
+            sincospi(-(double)j / (double)h, &s1, &c1);          // W_2h^j
+            sincospi(-(double)j / (double)(2 * h), &s2, &c2);    // W_4h^j
+            tws[fft_tw_offset(h, m) + j] = make_float4((float)c1, (float)s1, (float)c2, (float)s2);
+        }
     }
     for (int n = tid; n < M; n += nt) {
         const int t = (n <= Nu - 1) ? Nu - 1 - n : M + Nu - 1 - n;  // (Nu - 1 - n) mod M
@@ -149,37 +235,44 @@ fft_filter_kernel(const Rows src, float* __restrict__ out, const int nrows, cons
     }
     __syncthreads();
     fft_dif(d64, tw64, m);
-    // spectrum of g, bit-reversed, with the inverse's 1 / M
+    // spectrum of g, bit-reversed, with the inverse's 1 / M, over tw64 (no
+    // longer read: fft_dif ended with a barrier); the row buffers take d64's
+    // place only after the next barrier
     const double inv_m = 1.0 / (double)M;
     for (int k = tid; k < M; k += nt) spec[k] = make_float2((float)(d64[k].x * inv_m), (float)(d64[k].y * inv_m));
     __syncthreads();
 
-    const int npairs = (nrows + 1) / 2;
-    for (int pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
-        const int r0 = 2 * pr, r1 = r0 + 1;
-        const bool two = r1 < nrows;
+    const int nquad = (nrows + 3) / 4;
+    for (int q = blockIdx.x; q < nquad; q += gridDim.x) {
+        const int r0 = 4 * q;
         for (int n = tid; n < M; n += nt) {
-            float x0 = 0.0f, x1 = 0.0f;
+            float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             if (n < Nu) {
-                x0 = src(r0, n);
-                if (two) x1 = src(r1, n);
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (r0 + e < nrows) x[e] = src(r0 + e, n);
             }
-            rows[n] = make_float2(x0, x1);
+            rows[n] = make_float2(x[0], x[1]);
+            rows[M + n] = make_float2(x[2], x[3]);
         }
         __syncthreads();
-        fft_dif(rows, tw32, m);
-        for (int k = tid; k < M; k += nt) {
-            const float2 y = c_mul(rows[k], spec[k]);
+        fft_dif_rows<2>(rows, tws, m);
+        for (int k = tid; k < 2 * M; k += nt) {
+            const float2 y = c_mul(rows[k], spec[k & (M - 1)]);
             rows[k] = make_float2(y.x, -y.y);
         }
         __syncthreads();
-        fft_dit(rows, tw32, m);
-        // out = conj(FFT(conj Y)): row r0 the real part, row r1 minus the imaginary part
-        float* o0 = out + (size_t)r0 * Nu;
-        for (int n = tid; n < Nu; n += nt) {
-            const float2 v = rows[n];
-            o0[n] = v.x;
-            if (two) o0[Nu + n] = -v.y;
+        fft_dit_rows<2>(rows, tws, m);
+        // out = conj(FFT(conj Y)): even rows the real part, odd rows minus
+        // the imaginary part
+        for (int e = 0; e < 4; ++e) {
+            if (r0 + e >= nrows) break;
+            float* o = out + (size_t)(r0 + e) * Nu;
+            const float2* b = rows + (e >> 1) * M;
+            for (int n = tid; n < Nu; n += nt) {
+                const float2 v = b[n];
+                o[n] = (e & 1) ? -v.y : v.x;
+            }
         }
         __syncthreads();
     }
