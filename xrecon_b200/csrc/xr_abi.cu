@@ -124,8 +124,8 @@ Geom geom_from(const xr_geom2d* p) {
 }
 
 struct Layout {
-    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, arc, volT, volR, volF, sinoS, total;
-    bool has_arc;
+    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, arc, colWR, volT, volR, volF, sinoS, total;
+    bool has_arc, has_pfx;
 };
 
 // Voxel-driven operators on a circular arc detector walk chained float32
@@ -288,6 +288,10 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
         if (op == OP_B || op == OP_BW) eff = OP_AT;
         else if (op == OP_BT || op == OP_BWT) eff = OP_A;
     }
+    // the prefix gathers' FP32 column steps
+    l.has_pfx = dim3d && (eff == OP_AT || eff == OP_B || eff == OP_BW);
+    l.colWR = o;
+    if (l.has_pfx) o = align256(o + V * g.Nu * sizeof(float4));
     l.volT = o;
     l.volR = o;
     if (eff == OP_A || eff == OP_BT || eff == OP_BWT) {
@@ -325,6 +329,7 @@ ViewTables tables_at(char* ws, const Layout& l) {
     t.colM = reinterpret_cast<float*>(ws + l.colM);
     t.hel = nullptr;
     t.arc = l.has_arc ? reinterpret_cast<float4*>(ws + l.arc) : nullptr;
+    t.colWR = l.has_pfx ? reinterpret_cast<float4*>(ws + l.colWR) : nullptr;
     return t;
 }
 
@@ -1319,6 +1324,7 @@ int xr_ragged2d_plan_bind(xr_ragged2d_plan* P, const float* images, float* sino,
         r.vt.colM = reinterpret_cast<float*>(ws + L.colM[i]);
         r.vt.hel = nullptr;
         r.vt.arc = r.g.type == GEO_ARC ? reinterpret_cast<float4*>(ws + L.arc[i]) : nullptr;
+        r.vt.colWR = nullptr;
         r.nview = in.nview;
         r.cw = column_width(r.g, 0);
         r.scale = in.scale;

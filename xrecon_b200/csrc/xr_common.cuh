@@ -92,6 +92,13 @@ struct ViewTables {
     // float pair hi + lo} and {float32 axis position, 0, 0, 0}: the inputs of
     // the chained column walk (ArcChain)
     float4* arc;
+    // voxel gathers through the row prefix tables only, else null; per column
+    // k of each view, [v Nu + k]: {dA, dB, R hi, R lo}: A and B of boundary
+    // k + 1 minus those of boundary k in FP32 (the column's width on line L
+    // is dA + dB L pixels), and colR as a float pair.  The gather evaluates
+    // one boundary and one colR per (pixel, view) in FP64 and steps to the
+    // neighbouring columns in FP32 from these.
+    float4* colWR;
 };
 
 // ---------------------------------------------------------------- dtype io

@@ -108,11 +108,20 @@ __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d,
 
     const size_t oc = (size_t)v * g.Nu + k;
     const double Dk1 = arcf ? arc_boundary_f(g, h, k + 1, angle, ea, eb) : boundary_axis(g, h, (double)k + 1.0, uscale);
+    auto put_R = [&](double R) {
+        vt.colR[oc] = R;
+        if (vt.colWR) {
+            double A1, B1;
+            boundary_line_coeffs(g, h, Dk1, A1, B1);
+            const float hi = (float)R;
+            vt.colWR[oc] = make_float4((float)(A1 - A), (float)(B1 - B), hi, (float)(R - (double)hi));
+        }
+    };
     const double dperp = h.use_x ? g.dy : g.dx;
     if (g.type == GEO_PARALLEL) {
         // forward3d.cpp:58,98 (xy_scale / dv) and system_matrix2d.cpp:109.
         vt.colQ[oc] = 1.0 / g.dz;
-        vt.colR[oc] = g.dz;
+        put_R(g.dz);
         vt.colE[oc] = (float)(dim3d ? dperp / (g.du * g.dv) : dperp / g.du);
         vt.colF[oc] = 1.0f;
         vt.colM[oc] = 0.0f;
@@ -128,7 +137,7 @@ __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d,
         M = column_mag(g, h, k, uscale);
     }
     vt.colQ[oc] = M / g.dz;
-    vt.colR[oc] = g.dz / M;
+    put_R(g.dz / M);
     const double aa = 0.5 * (Dk + Dk1) - h.spar;
     const double F = aa * aa + h.sperp * h.sperp;
     if (dim3d) {

@@ -185,21 +185,23 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         const int ka = max(0, (int)floorf(lo - margin));
         const int kb = min(Nu - 1, (int)floorf(hi + margin));
         if (ka > kb) continue;
-        const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
-        const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
-        const double* __restrict__ Rq = vt.colR + (size_t)v * Nu;
         const char* __restrict__ tvb = reinterpret_cast<const char*>(tb + (size_t)v * vstride);
-        const double dp = (double)p, dL = (double)L;
-        // first column whose right boundary lies right of the pixel's left edge
-        // (boundaries relative to the pixel, in pixel units)
+        const float4* __restrict__ cWR = vt.colWR + (size_t)v * Nu;
+        const float Lf = (float)L;
+        // Boundaries relative to the pixel, in pixel units: boundary ka in
+        // FP64, the next ones by adding the columns' widths on this line in
+        // FP32 (pd: the direct boundary k + 1).  First column whose right
+        // boundary lies right of the pixel's left edge:
         int k = ka;
-        float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
-        float pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
-        while (!(pk1 > 0.0f) && k < kb) {
+        float pkl = (float)(fma(vt.bB[(size_t)v * (Nu + 1) + k], (double)L, vt.bA[(size_t)v * (Nu + 1) + k]) - (double)p);
+        auto width = [&](int c) { const float4 w = cWR[c]; return fmaf(w.y, Lf, w.x); };
+        float pd = pkl + width(k);
+        while (!(pd > 0.0f) && k < kb) {
             ++k;
-            pkl = pk1;
-            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            pkl = pd;
+            pd += width(k);
         }
+        float pk1 = pd;
         ArcChain ch;
         float qd = 0.0f;
         const float4* __restrict__ ea = nullptr;
@@ -209,35 +211,48 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             ch.start(ea, k, keep, gf.du);
             float d = ch.next_linear(ea, k + 1);
             if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
-            pk1 = fmaf(d, qd, pk1);
+            pk1 = fmaf(d, qd, pd);
         }
+        // The run's rows at column k: its bottom boundary minus half a row is
+        // u0 = zs ib + zoffh, ib = mvdv colR[k] rows per voxel.  Evaluated in
+        // FP64 at this first column (kr) and split into an integer row r0
+        // and f0 = u0 - r0; at the others u0 - r0 = f0 + zs (ib - ib_kr) and
+        // ib - ib_kr = mvdv (colR[k] - colR[kr]), both small, in FP32 (the
+        // colR difference from the hi + lo pairs, hi - hi exact).
+        const float4 Wr = cWR[k];
+        const float2 Rr = make_float2(Wr.z, Wr.w);
+        const double ibr = mvdv * ((double)Rr.x + (double)Rr.y);
+        const double u0r = fma(zs, ibr, zoffh);
+        const double tr0 = u0r + 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer
+        const int r0 = __double2loint(tr0);
+        const float f0r = (float)(u0r - (tr0 - 6755399441055744.0));
+        const float fibr = (float)ibr, mvdvf = (float)mvdv, zsf = (float)zs, r0f = (float)r0;
+        // Address of the entry for local row n of column col:
+        //   tvb + ((r0 + 1 + n) Nu + col) 8 = rb + col 8 + bits(n + 1.5 * 2^23) Nu8
+        // with bits() read as unsigned: one wide multiply-add per lookup.
+        const uintptr_t rb =
+            reinterpret_cast<uintptr_t>(tvb) + (uintptr_t)((long long)(r0 + 1) * Nu8 - 0x4B400000ll * (long long)Nu8);
         // lanes now walk their overlapping columns in step, one per iteration
         for (;;) {
             const float wf = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
             do {
                 if (!(wf > 0.0f)) break;
-                const double ib = mvdv * Rq[k];  // detector rows per voxel
+                const float4 Wk = cWR[k];
+                const float dib = mvdvf * ((Wk.z - Rr.x) + (Wk.w - Rr.y));
+                const float fib = fibr + dib;  // detector rows per voxel
                 // keeps every local row index below 2^17, where the FP32
                 // round-to-nearest below is exact (geometries this extreme
                 // are far outside any scanner's)
-                if (!((float)ib < 4096.0f)) break;
-                // row coordinate of the run's bottom boundary, minus half a row
-                const double u0 = fma(zs, ib, zoffh);
-                if (u0 >= (double)Nv - 0.5 || u0 + R * ib <= -0.5) break;
-                const double t0 = u0 + 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer
-                const double n0 = t0 - 6755399441055744.0;
-                const int r0 = __double2loint(t0);
-                const float f0 = (float)(u0 - n0), fib = (float)ib;
+                if (!(fib < 4096.0f)) break;
+                const float f0 = fmaf(zsf, dib, f0r);
+                const float ub = f0 + r0f;                 // the run's rows, detector coordinates
+                const float ut = fmaf((float)R, fib, ub);
+                if (ub >= (float)Nv - 0.5f || ut <= -0.5f) break;
                 const int col = keep ? k : Nu - 1 - k;
-                // Address of the entry for local row n:
-                //   tvb + ((r0 + 1 + n) Nu + col) 8 = cb + bits(n + 1.5 * 2^23) Nu8
-                // with bits() read as unsigned: one wide multiply-add per lookup.
-                const char* cb = reinterpret_cast<const char*>(
-                    reinterpret_cast<uintptr_t>(tvb) +
-                    (uintptr_t)((long long)(r0 + 1) * Nu8 + (long long)col * 8 - 0x4B400000ll * (long long)Nu8));
+                const char* cb = reinterpret_cast<const char*>(rb + (uintptr_t)col * 8u);
                 const float wk = __fdividef(wf * lf, fib);
-                // rows the run reaches (local), inside [0, Nv - 1] in every active lane?
-                const bool inside = (u0 >= 0.0) && (u0 + R * ib <= (double)Nv - 1.0);
+                // rows the run reaches, inside [0, Nv - 1] in every active lane?
+                const bool inside = (ub >= 0.0f) && (ut <= (float)(Nv - 1));
                 float gprev = 0.0f;
                 if (__all_sync(__activemask(), inside)) {
                     // boundaries in pairs: the index arithmetic on packed FP32x2
@@ -272,7 +287,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                         }
                     }
                 } else {
-                    const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
+                    const float ulo = -1.0f - r0f, uhi = (float)Nv - 0.5f - r0f;
 #pragma unroll
                     for (int i = 0; i <= R; ++i) {
                         const float uc = fminf(fmaxf(fmaf((float)i, fib, f0), ulo), uhi);
@@ -289,11 +304,12 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
             if (++k > kb) break;
             pkl = pk1;
             if (pkl >= 1.0f) break;  // column k starts right of the pixel
-            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            pd += width(k);
+            pk1 = pd;
             if (CHAIN) {
                 float d = ch.next_linear(ea, k + 1);
                 if (k + 1 == Nu) d = fminf(d, 0.0f);
-                pk1 = fmaf(d, qd, pk1);
+                pk1 = fmaf(d, qd, pd);
             }
         }
     }
