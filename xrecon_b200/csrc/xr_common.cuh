@@ -88,9 +88,12 @@ struct ViewTables {
     HelView* hel;  // helical scans only, else null
     // circular arc detectors, voxel-driven operators (B, Bw and their
     // transposes) only, else null: two float4 per boundary k = 0..Nu of each
-    // view, [2 (v (Nu + 1) + k)]: {float32 angle t, d(axis)/dt, tan(t) as a
-    // float pair hi + lo} and {float32 axis position, 0, 0, 0}: the inputs of
-    // the chained column walk (ArcChain)
+    // view, [2 (v (Nu + 1) + k)]: {float32 angle t, d(axis)/dt, dA, dB} and
+    // {float32 axis position, tan(t) as a float pair hi + lo, 0}: the inputs
+    // of the chained column walk (ArcChain); dA, dB are the boundary's line
+    // coefficients minus those of boundary k - 1 (zero for k = 0), so the
+    // walk's step to boundary k also reads column k - 1's width on line L,
+    // dA + dB L pixels.
     float4* arc;
     // voxel gathers through the row prefix tables only, else null; per column
     // k of each view, [v Nu + k]: {dA, dB, R hi, R lo}: A and B of boundary
@@ -236,10 +239,17 @@ struct ArcChain {
         const float4 a = e[2 * j];
         return __fsub_rn(t, a.x) * a.y;
     }
-    __device__ __forceinline__ float next_exact(const ViewHdr& h, const float4* __restrict__ e, int j) {
+    // the same, and the width of column j - 1 on line Lf (pixels)
+    __device__ __forceinline__ float next_linear(const float4* __restrict__ e, int j, float Lf, float& width) {
         t = __fadd_rn(t, step);
         const float4 a = e[2 * j];
-        return arc_chain_delta(h, make_float4(a.x, a.z, a.w, e[2 * j + 1].x), t);
+        width = fmaf(a.w, Lf, a.z);
+        return __fsub_rn(t, a.x) * a.y;
+    }
+    __device__ __forceinline__ float next_exact(const ViewHdr& h, const float4* __restrict__ e, int j) {
+        t = __fadd_rn(t, step);
+        const float4 a = e[2 * j], b = e[2 * j + 1];
+        return arc_chain_delta(h, make_float4(a.x, b.y, b.z, b.x), t);
     }
 };
 

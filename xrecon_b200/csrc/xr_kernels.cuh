@@ -80,8 +80,8 @@ __device__ __forceinline__ double arc_boundary_f(const Geom& g, const ViewHdr& h
     // derivative of the axis map: x axis sy (1 + T^2), y axis -sx (1 + T^2) / T^2
     const double sec2 = 1.0 + T * T;
     const double dD = h.use_x ? (double)h.syf * sec2 : -(double)h.sxf * sec2 / (T * T);
-    ea = make_float4(tk, (float)dD, hi, lo);
-    eb = make_float4(Df, 0.0f, 0.0f, 0.0f);
+    ea = make_float4(tk, (float)dD, 0.0f, 0.0f);  // .z, .w: the column width, filled by the caller
+    eb = make_float4(Df, hi, lo, 0.0f);
     return (double)Df;
 }
 
@@ -96,12 +96,20 @@ __device__ __forceinline__ void setup_view_entry(const Geom& g, const int dim3d,
     const size_t ob = (size_t)v * (g.Nu + 1) + k;
     float4 ea, eb;
     const double Dk = arcf ? arc_boundary_f(g, h, k, angle, ea, eb) : boundary_axis(g, h, (double)k, uscale);
+    double A, B;
+    boundary_line_coeffs(g, h, Dk, A, B);
     if (arcf && vt.arc) {
+        if (k > 0) {
+            // boundary k - 1 as its own thread evaluates it
+            float4 pa, pb;
+            double Ap, Bp;
+            boundary_line_coeffs(g, h, arc_boundary_f(g, h, k - 1, angle, pa, pb), Ap, Bp);
+            ea.z = (float)(A - Ap);
+            ea.w = (float)(B - Bp);
+        }
         vt.arc[2 * ob] = ea;
         vt.arc[2 * ob + 1] = eb;
     }
-    double A, B;
-    boundary_line_coeffs(g, h, Dk, A, B);
     vt.bA[ob] = A;
     vt.bB[ob] = B;
     if (k >= g.Nu) return;
@@ -715,6 +723,7 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
         pcy = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);
     }
     const float sodf = (float)g.sod, shuf = (float)g.shu, inv_du = (float)(1.0 / g.du);
+    const float inv_dx = (float)(1.0 / g.dx), inv_dy = (float)(1.0 / g.dy);
     // column bracket margin: half a column, plus the arc guess's angle error
     const float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * inv_du : 0.0f);
     float acc = 0.0f;
@@ -766,23 +775,28 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
         const TI* __restrict__ sv = sinob + (size_t)v * Nu;
         const double dp = (double)p, dL = (double)L;
         if (MODE != OP_AT && vt.arc) {
-            // arc detector: the pixel's columns walked with chained angles
+            // arc detector: the pixel's columns walked with chained angles.
+            // Boundary ka relative to the pixel in FP64, the next direct
+            // boundaries (pd) by adding the columns' widths on this line in
+            // FP32, which the walk's arc entries carry.
             const float4* __restrict__ ea = vt.arc + 2 * (size_t)v * (Nu + 1);
-            const float qd = (float)(fma(h.q1, dL, h.q0) / h.dpix);  // pixels per axis unit
+            const float Lf = (float)L;
+            const float qd = (float)fma(h.q1, dL, h.q0) * (h.use_x ? inv_dx : inv_dy);  // pixels per axis unit
+            auto width = [&](int j) { const float4 a = ea[2 * j]; return fmaf(a.w, Lf, a.z); };
             int k = ka;
             float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
-            float pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
-            while (!(pk1 > 0.0f) && k < kb) {
+            float pd = pkl + width(k + 1);
+            while (!(pd > 0.0f) && k < kb) {
                 ++k;
-                pkl = pk1;
-                pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+                pkl = pd;
+                pd += width(k + 1);
             }
             ArcChain ch;
             ch.start(ea, k, h.keep, (float)g.du);
+            float d = ch.next_linear(ea, k + 1);
+            if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
+            float pk1 = fmaf(d, qd, pd);
             for (;;) {
-                float d = ch.next_linear(ea, k + 1);
-                if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
-                pk1 = fmaf(d, qd, pk1);
                 const float wd = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
                 if (wd > 0.0f) {
                     const int col = h.keep ? k : Nu - 1 - k;
@@ -791,7 +805,11 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
                 if (++k > kb) break;
                 pkl = pk1;
                 if (pkl >= 1.0f) break;
-                pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+                float w;
+                d = ch.next_linear(ea, k + 1, Lf, w);
+                if (k + 1 == Nu) d = fminf(d, 0.0f);
+                pd += w;
+                pk1 = fmaf(d, qd, pd);
             }
             continue;
         }

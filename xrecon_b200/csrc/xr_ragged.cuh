@@ -107,7 +107,7 @@ __device__ __forceinline__ int next_tile(int* ctr) {
     return t_s;
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 ragged2d_fbp_kernel(const RaggedDev* __restrict__ inst, const int ninst, const int4 totals, const int4 lists,
                     const int project, const int CW, const int VS, unsigned* bar, int* ctr) {
     extern __shared__ float sm[];

@@ -207,7 +207,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         const float4* __restrict__ ea = nullptr;
         if (CHAIN) {
             ea = vt.arc + 2 * (size_t)v * (Nu + 1);
-            qd = (float)(q / h.dpix);  // pixels per axis unit on this line
+            qd = __fdividef((float)q, h.use_x ? gf.dx : gf.dy);  // pixels per axis unit on this line (scales the chain's small offsets)
             ch.start(ea, k, keep, gf.du);
             float d = ch.next_linear(ea, k + 1);
             if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
