@@ -186,6 +186,26 @@ def test_tma_and_plain_paths_match_oracle(cuda, scan):
         _native.set_plain_kernels(False)
 
 
+@pytest.mark.parametrize("scan", ["parallel", "flat", "arc"])
+def test_backprojection_deep_volumes(cuda, scan):
+    """B, Bw and A^T against the oracle on volumes 640 and 900 slices deep
+    (one shifted 300 mm along z, with a detector offset along v): the prefix
+    gather evaluates each (pixel, view)'s first column in FP64 and the next
+    columns' run offsets as that value plus z times the change of rows per
+    voxel in FP32, which grows with the run's distance from z = 0."""
+    cases = [
+        _opts3d(12, 10, 640, 48, 800, 1.0, 1.0, 1.0, 1.1, 1.0, 500., 1000., (0.5, -0.3, 0.0), 0.2, 0.3, scan),
+        _opts3d(10, 12, 900, 40, 700, 1.2, 1.1, 0.8, 1.4, 1.6, 450., 900., (0.2, 0.4, 300.0), -0.3, 120.0, scan),
+    ]
+    ang = (np.arange(16) * (2 * np.pi / 16) + 0.07).astype(np.float32)
+    rng = np.random.default_rng(21)
+    for opts in cases:
+        sino = rng.random((1, 1, ang.size, int(opts[4]), int(opts[3]))).astype(np.float32)
+        for op in ("B", "BW", "AT"):
+            got = run(3, op, sino, opts, ang, cuda)
+            assert rel_l2(got, O.dd3d(op, sino, opts, ang)) < 1e-5, (scan, op)
+
+
 @pytest.mark.parametrize("scan", ["flat", "arc", "parallel"])
 def test_backprojection_long_column_walks(cuda, scan):
     """B, Bw and A^T (prefix-table and plain gathers) against the oracle when
