@@ -560,41 +560,50 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
         const int ka = max(0, (int)floorf(lo - margin));
         const int kb = min(Nu - 1, (int)floorf(hi + margin));
         if (ka > kb) continue;
-        const double* __restrict__ bA = vt.bA + (size_t)v * (Nu + 1);
-        const double* __restrict__ bB = vt.bB + (size_t)v * (Nu + 1);
-        const double* __restrict__ Rq = vt.colR + (size_t)v * Nu;
         const char* __restrict__ tvb = reinterpret_cast<const char*>(tab + ((size_t)b * nview + v) * vstride);
         const unsigned Nu8 = (unsigned)Nu * 8u;
-        const double dp = (double)p, dL = (double)L;
+        // Boundaries relative to the pixel: boundary ka in FP64, the next ones
+        // by the columns' widths on this line in FP32; the run's row offset
+        // and rows per voxel in FP64 at the first column, at the next ones
+        // plus their FP32 changes (as in vox_prefix3d_kernel).
+        const float4* __restrict__ cWR = vt.colWR + (size_t)v * Nu;
+        const float Lf = (float)L;
+        auto width = [&](int c) { const float4 wc = cWR[c]; return fmaf(wc.y, Lf, wc.x); };
         int k = ka;
-        float pkl = (float)(fma(bB[k], dL, bA[k]) - dp);
-        float pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+        float pkl = (float)(fma(vt.bB[(size_t)v * (Nu + 1) + k], (double)L, vt.bA[(size_t)v * (Nu + 1) + k]) - (double)p);
+        float pk1 = pkl + width(k);
         while (!(pk1 > 0.0f) && k < kb) {
             ++k;
             pkl = pk1;
-            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            pk1 += width(k);
         }
+        const float4 Wr = cWR[k];
+        const double ibr = mvdv * ((double)Wr.z + (double)Wr.w);
+        const double u0r = fma(zs, ibr, zoffh);
+        const double tr0 = u0r + 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer
+        const int r0 = __double2loint(tr0);
+        const float f0r = (float)(u0r - (tr0 - 6755399441055744.0));
+        const float fibr = (float)ibr, mvdvf = (float)mvdv, zsf = (float)zs, r0f = (float)r0;
+        // entry of local row n: tvb + ((r0 + 1 + n) Nu + col) 8
+        //   = rb + col 8 + bits(n + 1.5 * 2^23) Nu8, bits read as unsigned
+        const uintptr_t rb =
+            reinterpret_cast<uintptr_t>(tvb) + (uintptr_t)((long long)(r0 + 1) * Nu8 - 0x4B400000ll * (long long)Nu8);
+        // rows -1 .. Nv of the detector (table rows 0 .. Nv + 1)
+        const float ulo = -1.0f - r0f, uhi = (float)Nv - 0.5f - r0f;
         for (;;) {
             const float wf = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
             if (wf > 0.0f) {
-                const double ib = mvdv * Rq[k];  // detector rows per voxel
-                const double u0 = fma(zs, ib, zoffh);
+                const float4 Wk = cWR[k];
+                const float dib = mvdvf * ((Wk.z - Wr.z) + (Wk.w - Wr.w));
+                const float fib = fibr + dib;  // detector rows per voxel
+                const float f0 = fmaf(zsf, dib, f0r);
+                const float ub = f0 + r0f;
                 // the guard keeps local row indices far below 2^22, where the
                 // FP32 round-to-nearest by 1.5 * 2^23 below is exact
-                if ((float)ib < 4096.0f && u0 < (double)Nv - 0.5 && u0 + R * ib > -0.5) {
-                    const double t0 = u0 + 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer
-                    const double n0 = t0 - 6755399441055744.0;
-                    const int r0 = __double2loint(t0);
-                    const float f0 = (float)(u0 - n0), fib = (float)ib;
+                if (fib < 4096.0f && ub < (float)Nv - 0.5f && fmaf((float)R, fib, ub) > -0.5f) {
                     const int col = keep ? k : Nu - 1 - k;
-                    // entry of local row n: tvb + ((r0 + 1 + n) Nu + col) 8
-                    //   = cb + bits(n + 1.5 * 2^23) Nu8, bits read as unsigned
-                    const char* cb = reinterpret_cast<const char*>(
-                        reinterpret_cast<uintptr_t>(tvb) +
-                        (uintptr_t)((long long)(r0 + 1) * Nu8 + (long long)col * 8 - 0x4B400000ll * (long long)Nu8));
+                    const char* cb = reinterpret_cast<const char*>(rb + (uintptr_t)col * 8u);
                     const float wk = __fdividef(wf * lf, fib);
-                    // rows -1 .. Nv of the detector (table rows 0 .. Nv + 1)
-                    const float ulo = (float)(-1 - r0), uhi = (float)Nv - 0.5f - (float)r0;
                     float gprev = 0.0f;
 #pragma unroll
                     for (int i = 0; i <= R; ++i) {
@@ -612,7 +621,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
             if (++k > kb) break;
             pkl = pk1;
             if (pkl >= 1.0f) break;
-            pk1 = (float)(fma(bB[k + 1], dL, bA[k + 1]) - dp);
+            pk1 += width(k);
         }
     }
     const float ideal_db = (fabsf(s.db) > 1.0e-8f) ? __fdiv_rn(XR_PI_F, fabsf(s.db)) : -1.0f;
