@@ -132,6 +132,11 @@ int xr_helical3d(int op, const xr_geom3d* geom, const xr_helical_opts* opts, con
  *   filt   : device float32 [2*Nu-1] spatial filter
  *   parker : device float32 [nview, Nu] short-scan weight or NULL
  *   rows_per_view : Nv (3D) or 1 (2D), to index `parker` by view.
+ * Rows of up to 2048 cells are filtered by FFT (a circular convolution of
+ * length 2^ceil(log2(2 Nu - 1)), FP32 rows, the filter's spectrum in FP64):
+ * within a few 1e-6 of the exact correlation, relative L2, on projection
+ * rows with the ramp filter.  Wider rows, and every row while
+ * xr_set_plain_kernels is on, take the direct correlation (FP32 sums).
  */
 int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, int nview, int rows_per_view,
                   const float* cosw, const float* filt, const float* parker, void* stream);
