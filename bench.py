@@ -59,13 +59,16 @@ def make_projector():
                           xr.ConeBeam3d(xr.Detector3d((WL["Nu"], WL["Nv"]), WL["du"]), WL["sod"], WL["sdd"], "flat"))
 
 
-def angles_np(nviews=None):
+def angles_np(nviews=None, contiguous=False):
     """The workload's views, uniform over 2 pi; with ``nviews`` an evenly
-    strided subset (profiling cases)."""
+    strided subset, or with ``contiguous`` the first ``nviews`` neighbouring
+    views (profiling cases)."""
     import numpy as np
     a = (np.arange(WL["V"]) * (2 * np.pi / WL["V"])).astype(np.float32)
     if nviews is None or nviews >= WL["V"]:
         return a
+    if contiguous:
+        return a[:nviews].copy()
     return a[:: WL["V"] // nviews][:nviews].copy()
 
 
@@ -682,7 +685,7 @@ def run_sharded_arm(args, rank: int, world: int, local_rank: int):
     opts = P.options
     vol = ellipsoid_volume_torch((WL["D"], WL["H"], WL["W"]), random_ellipsoids3d(20, seed=0, density=(0.0, 1.0)),
                                  dev)[None, None].contiguous()
-    ang = torch.from_numpy(angles_np(args.views)).to(dev)
+    ang = torch.from_numpy(angles_np(args.views, args.contiguous_views)).to(dev)
     nv = ang.numel()
     stream = torch.cuda.current_stream(dev)
     events = []
@@ -749,7 +752,7 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
     D, H, W = WL["D"], WL["H"], WL["W"]
     vol = ellipsoid_volume_torch((D, H, W), random_ellipsoids3d(20, seed=rank, density=(0.0, 1.0)), dev)
     vol = vol[None, None].contiguous()
-    ang = torch.from_numpy(angles_np(args.views)).to(dev)
+    ang = torch.from_numpy(angles_np(args.views, args.contiguous_views)).to(dev)
     nv = ang.numel()
 
     def step(x):
@@ -971,6 +974,8 @@ def main():
                     help="profiling: turns of the helical scan (default 5) with --helical-only")
     ap.add_argument("--views", type=int, default=None,
                     help="profiling: an evenly strided subset of the workload's views")
+    ap.add_argument("--contiguous-views", action="store_true",
+                    help="profiling: with --views, the first neighbouring views instead of a strided subset")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other named configurations (2D FBP, 3D FDK, cone-arc least squares)")
     ap.add_argument("--only", choices=["c1", "c2", "c3"], default=None,

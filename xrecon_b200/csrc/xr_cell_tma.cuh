@@ -104,6 +104,9 @@ __device__ __noinline__ void drain_stages(uint64_t* bar, int last) {
 #ifndef XR_CELL_MINB
 #define XR_CELL_MINB 2  // CTAs per SM the register budget is sized for
 #endif
+#ifndef XR_CELL_VGROUP
+#define XR_CELL_VGROUP 8  // views per group of the block order (below)
+#endif
 //
 // HEL: helical scan, the view's z placement and column width come from
 // vt.hel (the volume and detector rows measured from the view's source z).
@@ -132,13 +135,26 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
 
     const int lane = threadIdx.x, tid = threadIdx.y * 32 + threadIdx.x;
     const int Nu = g.Nu;
-    const int k0 = blockIdx.x * 32;
+    // Block order: XR_CELL_VGROUP consecutive views of each (column block,
+    // row block) run next to each other, so that their nearly equal line
+    // windows are read from DRAM once and from L2 after.
+    unsigned bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+    if (XR_CELL_VGROUP > 1) {
+        const unsigned nx = gridDim.x, ny = gridDim.y, nz = gridDim.z;
+        const unsigned id = blockIdx.x + nx * (blockIdx.y + ny * blockIdx.z);
+        const unsigned grp = id / (XR_CELL_VGROUP * nx * ny), rem = id % (XR_CELL_VGROUP * nx * ny);
+        const unsigned gsize = min((unsigned)XR_CELL_VGROUP, nz - grp * XR_CELL_VGROUP);  // the last group may be short
+        bz = grp * XR_CELL_VGROUP + rem % gsize;
+        bx = (rem / gsize) % nx;
+        by = (rem / gsize) / nx;
+    }
+    const int k0 = (int)bx * 32;
     const int k = k0 + lane;
     const int kc = min(k, Nu - 1);
     const int rows_per_cta = blockDim.y * R;
-    const int rg0 = blockIdx.y * rows_per_cta;
+    const int rg0 = (int)by * rows_per_cta;
     const int r0 = rg0 + threadIdx.y * R;
-    const int vb = blockIdx.z + view0;
+    const int vb = (int)bz + view0;
     const int v = vb % nview, b = vb / nview;
     const bool active = (k < Nu) && (r0 < g.Nv);
 
