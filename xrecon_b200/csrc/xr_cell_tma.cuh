@@ -326,8 +326,10 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                             const float u1 = fminf(fmaxf(fmaf(bf, (float)(i + 1), fu), 0.0f), uhi);
                             float n;
                             const float bn = slice_at(u1, n);
-                            acc[i] = fmaf(bp, fmaxf(0.0f, n - up), acc[i]);
-                            acc[i] = fmaf(bn, u1 - fmaxf(n, up), acc[i]);
+                            // max(0, n - u_i) = max(n, u_i) - u_i exactly
+                            const float m = fmaxf(n, up);
+                            acc[i] = fmaf(bp, m - up, acc[i]);
+                            acc[i] = fmaf(bn, u1 - m, acc[i]);
                             bp = bn;
                             up = u1;
                         }
