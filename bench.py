@@ -900,9 +900,9 @@ def run_gpu_arm(args, rank: int, world: int, local_rank: int):
     dom = "cell_tma3d_kernel (projection A)" if t_a >= t_b else "vox_prefix3d_kernel (backprojection B)"
     # what holds the kernel below the HBM roofline, from its ncu profile
     # (profiles/cell_tma3d_A_cone_flat_64views.md, vox_prefix3d_B_cone_flat_64views.md)
-    limiter = ("instruction issue: ~74 % issue active, 'not selected' stalls, DRAM ~32 % of peak"
+    limiter = ("instruction issue: ~70 % issue active, 'not selected' stalls, DRAM ~3 % of peak"
                if t_a >= t_b else
-               "table-lookup latency and issue: ~68 % issue active, long-scoreboard (L1 hit) stalls, DRAM idle")
+               "table-lookup latency and issue: ~67 % issue active, long-scoreboard (L1 hit) stalls, DRAM idle")
     wl = dict(WL, V=nv)
     achieved = algo_bytes_op(wl) / dom_t / 1e9
     traffic = None
