@@ -12,14 +12,18 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-LIB = PKG / "libxrecon_b200.so"
+# XRECON_B200_BOUNDS=1 selects a separate build with the kernels' index
+# checks compiled in (XR_DEBUG_BOUNDS: an index outside its buffer sets bit 2
+# of the device error word and is clamped); it is slower and only for tests.
+BOUNDS = os.environ.get("XRECON_B200_BOUNDS", "0") not in ("", "0")
+LIB = PKG / ("libxrecon_b200_bounds.so" if BOUNDS else "libxrecon_b200.so")
 SOURCES = [PKG / "csrc" / "xr_abi.cu"]
 DEPS = SOURCES + sorted((PKG / "csrc").glob("*.cuh")) + sorted((PKG / "csrc").glob("*.hpp")) + \
     [ROOT / "include" / "xrecon_b200.h"]
 NVCC = os.environ.get("NVCC", str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "bin" / "nvcc"))
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared", f"-I{ROOT / 'include'}",
-         "-lpthread"]
+         "-lpthread"] + (["-DXR_DEBUG_BOUNDS"] if BOUNDS else [])
 
 
 def stale() -> bool:

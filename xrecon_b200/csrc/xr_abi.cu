@@ -7,6 +7,7 @@
 #include <string>
 
 #include <cudaTypedefs.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <array>
 #include <atomic>
@@ -968,6 +969,26 @@ int noalloc_scratch(void** ptr) {
 
 }  // namespace
 
+// NVTX range over one C-ABI call: host markers for a profiler's timeline
+// (nvtx3 is header-only and does next to nothing when no tool is attached).
+struct Trace {
+    explicit Trace(const char* name) { nvtxRangePushA(name); }
+    ~Trace() { nvtxRangePop(); }
+    Trace(const Trace&) = delete;
+    Trace& operator=(const Trace&) = delete;
+};
+
+// "<entry> <operator>" for the range names of the DD entry points
+inline const char* op_trace_name(int dim, int op) {
+    static const char* const names[3][6] = {
+        {"xr_dd2d A", "xr_dd2d AT", "xr_dd2d B", "xr_dd2d BT", "xr_dd2d BW", "xr_dd2d BWT"},
+        {"xr_dd3d A", "xr_dd3d AT", "xr_dd3d B", "xr_dd3d BT", "xr_dd3d BW", "xr_dd3d BWT"},
+        {"xr_helical3d A", "xr_helical3d AT", "xr_helical3d B", "xr_helical3d BT", "xr_helical3d BW",
+         "xr_helical3d BWT"}};
+    static const char* const other[3] = {"xr_dd2d", "xr_dd3d", "xr_helical3d"};
+    return (op >= 0 && op < 6) ? names[dim][op] : other[dim];
+}
+
 // FFT filter (xr_fft_filter.cuh) of `nrows` rows from `rows_src`: one wave of
 // CTAs, each transforming the filter once and then a share of the rows.
 template <typename RowsT>
@@ -1009,6 +1030,7 @@ size_t xr_dd3d_workspace_size(int op, const xr_geom3d* geom, int nbatch, int nvi
 int xr_dd2d(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,
             const float* angles, int nbatch, int nview, void* workspace, size_t workspace_bytes,
             void* stream) {
+    xr::Trace tr(xr::op_trace_name(0, op));
     if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
     return xr::apply(0, op, xr::geom_from(geom), in, dtype_in, out, dtype_out, angles, nbatch, nview,
                      workspace, workspace_bytes, stream, 1.0f);
@@ -1017,6 +1039,7 @@ int xr_dd2d(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* o
 int xr_dd3d(int op, const xr_geom3d* geom, const void* in, int dtype_in, void* out, int dtype_out,
             const float* angles, int nbatch, int nview, void* workspace, size_t workspace_bytes,
             void* stream) {
+    xr::Trace tr(xr::op_trace_name(1, op));
     if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
     return xr::apply(1, op, xr::geom_from(geom), in, dtype_in, out, dtype_out, angles, nbatch, nview,
                      workspace, workspace_bytes, stream, 1.0f);
@@ -1030,6 +1053,7 @@ size_t xr_helical3d_workspace_size(int op, const xr_geom3d* geom, int nbatch, in
 int xr_helical3d(int op, const xr_geom3d* geom, const xr_helical_opts* opts, const float* in, float* out,
                  const float* angles, const float* source_pos, int nbatch, int nview, void* workspace,
                  size_t workspace_bytes, void* stream) {
+    xr::Trace tr(xr::op_trace_name(2, op));
     if (!geom || !opts) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry or options");
     xr::HelOpts o;
     o.view_mode = opts->view_mode;
@@ -1044,6 +1068,7 @@ int xr_helical3d(int op, const xr_geom3d* geom, const xr_helical_opts* opts, con
 
 int xr_fbp_filter(const void* in, int dtype_in, float* out, int nrows, int Nu, int nview, int rows_per_view,
                   const float* cosw, const float* filt, const float* parker, void* stream) {
+    xr::Trace tr("xr_fbp_filter");
     if (!in || !out || !filt) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
     if (Nu < 1 || nrows < 0 || nview < 1 || rows_per_view < 1)
         return xr::fail(XR_ERR_INVALID_ARGUMENT, "bad filter sizes");
@@ -1137,6 +1162,7 @@ int xr_test_hooks(unsigned int hooks) {
 
 int xr_dd2d_noalloc(int op, const xr_geom2d* geom, const void* in, int dtype_in, void* out, int dtype_out,
                     const float* angles, int nbatch, int nview, void* stream) {
+    xr::Trace tr("xr_dd2d_noalloc");
     if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
     const xr::Geom g = xr::geom_from(geom);
     if (int rc = xr::validate(g, 0, op, nbatch, nview)) return rc;
@@ -1159,6 +1185,7 @@ unsigned long long xr_launch_count(void) { return xr::g_launches.load(std::memor
 int xr_rebin_parallel(const void* in, int dtype_in, float* out, int nbatch, int nview, int Nv, int Nu,
                       const float* grid, int nview_out, int Nt, const float* filt, void* stream) {
     using namespace xr;
+    Trace tr("xr_rebin_parallel");
     if (!in || !out || !grid) return fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
     if (nbatch < 0 || nview < 1 || Nv < 1 || Nu < 1 || nview_out < 0 || Nt < 1)
         return fail(XR_ERR_INVALID_ARGUMENT, "bad rebinning sizes");
@@ -1224,6 +1251,7 @@ size_t xr_sysmat3d_workspace_size(const xr_geom3d* geom, int nview) {
 
 int xr_sysmat2d(const xr_geom2d* geom, const float* angles, int nview, const long long* offsets, long long* counts,
                 long long* rows, long long* cols, float* vals, void* workspace, size_t workspace_bytes, void* stream) {
+    xr::Trace tr("xr_sysmat2d");
     if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
     return xr::sysmat(0, xr::geom_from(geom), angles, nview, offsets, counts, rows, cols, vals, workspace,
                       workspace_bytes, stream);
@@ -1231,6 +1259,7 @@ int xr_sysmat2d(const xr_geom2d* geom, const float* angles, int nview, const lon
 
 int xr_sysmat3d(const xr_geom3d* geom, const float* angles, int nview, const long long* offsets, long long* counts,
                 long long* rows, long long* cols, float* vals, void* workspace, size_t workspace_bytes, void* stream) {
+    xr::Trace tr("xr_sysmat3d");
     if (!geom) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null geometry");
     return xr::sysmat(1, xr::geom_from(geom), angles, nview, offsets, counts, rows, cols, vals, workspace,
                       workspace_bytes, stream);
@@ -1347,6 +1376,7 @@ int xr_ragged2d_plan_bind(xr_ragged2d_plan* P, const float* images, float* sino,
 
 int xr_ragged2d_run(const xr_ragged2d_plan* P, int project, int a_cols_log2, int view_split_log2, void* stream) {
     using namespace xr;
+    Trace tr("xr_ragged2d_run");
     if (!P || !P->workspace) return fail(XR_ERR_INVALID_ARGUMENT, "plan not bound to a workspace");
     if (a_cols_log2 < 0 || a_cols_log2 > 3 || view_split_log2 < 0 || view_split_log2 > 3)
         return fail(XR_ERR_INVALID_ARGUMENT, "tile parameters out of range");
@@ -1390,6 +1420,7 @@ void xr_ragged2d_plan_destroy(xr_ragged2d_plan* plan) { delete plan; }
 
 int xr_ctpd_load(const char* const* paths, int nfiles, int rows, int cols, int col_stride, int row_stride,
                  int nthreads, float* sino, float* views, int* failed_file) {
+    xr::Trace tr("xr_ctpd_load");
     if (failed_file) *failed_file = -1;
     if (!paths || !sino || !views || nfiles < 1 || rows < 1 || cols < 1 || col_stride < 1 || row_stride < 1)
         return xr::fail(XR_ERR_INVALID_ARGUMENT, "xr_ctpd_load: null pointer or non-positive size");

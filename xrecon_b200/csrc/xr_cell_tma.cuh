@@ -312,11 +312,11 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         // every t of the CTA otherwise).
                         const float fu = f + (float)(j0 - win.z0);
                         const float uhi = (float)(win.zlast - win.z0) + 0.999f;
-                        const TI* sb = stage + (size_t)s * stage_elems + (pc - win.p0);
+                        const TI* sb = stage + (size_t)s * stage_elems + XR_BOUND(pc - win.p0, 0, BP - np);
                         auto slice_at = [&](float u, float& n) -> float {
                             const int ri = __float2int_rd(u);
                             n = (float)ri;
-                            return band_smem<TI, NB>(sb + ri * BP, w, np) * slice_w(win.z0 + ri);
+                            return band_smem<TI, NB>(sb + XR_BOUND(ri, 0, BZ) * BP, w, np) * slice_w(win.z0 + ri);
                         };
                         float up = fminf(fmaxf(fu, 0.0f), uhi);
                         float np0;
@@ -338,12 +338,12 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         // single virtual zero voxel ends at win.z0, past
                         // win.zlast the value is zero and the next boundary
                         // infinite.
-                        const TI* sbase = stage + (size_t)s * stage_elems + (pc - win.p0);
+                        const TI* sbase = stage + (size_t)s * stage_elems + XR_BOUND(pc - win.p0, 0, BP - np);
                         const TI* ptr;
                         int jabs;
                         if (j0 >= win.z0) {
                             jabs = j0;
-                            ptr = sbase + (size_t)(j0 - win.z0) * BP;
+                            ptr = sbase + (size_t)XR_BOUND(j0 - win.z0, 0, BZ) * BP;
                             vj = band_smem<TI, NB>(ptr, w, np) * slice_w(jabs);
                         } else {
                             jabs = win.z0 - 1;
@@ -360,6 +360,9 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                                 pos = jn;
                                 ++jabs;
                                 ptr += BP;
+#ifdef XR_DEBUG_BOUNDS
+                                if (jabs <= win.zlast) ptr = sbase + (size_t)XR_BOUND(jabs - win.z0, 0, BZ) * BP;
+#endif
                                 if (jabs <= win.zlast) { vj = band_smem<TI, NB>(ptr, w, np) * slice_w(jabs); jn += 1.0f; }
                                 else { vj = 0.0f; jn = 3.0e38f; }
                             }

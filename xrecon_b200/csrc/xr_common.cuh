@@ -26,6 +26,34 @@
 
 namespace xr {
 
+// Device-wide sticky error word (one per device that loads the library).
+// 0 = no error; kernels OR in a code when a bounded wait gives up (bits 0
+// and 1) or, in builds with XR_DEBUG_BOUNDS, when an index checked by
+// XR_BOUND falls outside its buffer (bit 2).  Defined here: the library is
+// a single translation unit.
+__device__ unsigned int g_device_error = 0;
+
+constexpr unsigned XR_DEVERR_BOUNDS = 4u;
+
+// XR_BOUND(i, lo, hi): the index i of a shared- or global-memory access.
+// Release builds return i unchanged (the kernels' own arithmetic keeps every
+// index inside its buffer).  Builds with XR_DEBUG_BOUNDS check it: an index
+// outside [lo, hi] sets XR_DEVERR_BOUNDS in the error word and is clamped
+// into the range, so the access stays in bounds and the kernel goes on; no
+// check traps.
+#ifdef XR_DEBUG_BOUNDS
+__device__ __forceinline__ long long xr_check_index(long long i, long long lo, long long hi) {
+    if (i < lo || i > hi) {
+        atomicOr(&g_device_error, XR_DEVERR_BOUNDS);
+        i = i < lo ? lo : hi;
+    }
+    return i;
+}
+#define XR_BOUND(i, lo, hi) (::xr::xr_check_index((i), (lo), (hi)))
+#else
+#define XR_BOUND(i, lo, hi) (i)
+#endif
+
 enum GeoType : int { GEO_PARALLEL = 0, GEO_FLAT = 1, GEO_ARC = 2 };
 enum OpKind : int { OP_A = 0, OP_AT = 1, OP_B = 2, OP_BT = 3, OP_BW = 4, OP_BWT = 5 };
 enum DType : int { DT_F32 = 0, DT_BF16 = 1, DT_F16 = 2 };

@@ -610,8 +610,13 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
                         const float uc = fminf(fmaxf(fmaf((float)i, fib, f0), ulo), uhi);
                         const float tr = uc + 12582912.0f;  // round to nearest integer (FMA pipe)
                         const float nf = tr - 12582912.0f;
+#ifdef XR_DEBUG_BOUNDS
+                        const long long t = XR_BOUND((long long)r0 + 1 + (__float_as_int(tr) - 0x4B400000), 0, Nv + 1);
+                        const float2 e = __ldg(reinterpret_cast<const float2*>(tvb) + (size_t)t * Nu + XR_BOUND(col, 0, Nu - 1));
+#else
                         const float2 e = __ldg(reinterpret_cast<const float2*>(
                             cb + (size_t)(unsigned)__float_as_int(tr) * Nu8));
+#endif
                         const float gi = fmaf(uc - nf, e.y, e.x);
                         if (i > 0) acc[i - 1] = fmaf(wk * wt[i - 1], gi - gprev, acc[i - 1]);
                         gprev = gi;

@@ -683,7 +683,7 @@ __device__ __forceinline__ float cell2d_sum(const Geom& g, const ViewTables& vt,
                 pixel_center(g, h, L, pp, px, py);
                 w *= fbp_weight(g, h, px, py);
             }
-            acc = fmaf(w, ld(line + pp), acc);
+            acc = fmaf(w, ld(line + XR_BOUND(pp, 0, npix - 1)), acc);
         }
     }
     if (MODE == OP_A && ls == 1) acc *= vt.colE[(size_t)v * Nu + k];
@@ -800,7 +800,7 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
                 const float wd = fminf(1.0f, pk1) - fmaxf(0.0f, pkl);
                 if (wd > 0.0f) {
                     const int col = h.keep ? k : Nu - 1 - k;
-                    acc = fmaf(wd * lf, ld(sv + col), acc);
+                    acc = fmaf(wd * lf, ld(sv + XR_BOUND(col, 0, Nu - 1)), acc);
                 }
                 if (++k > kb) break;
                 pkl = pk1;
@@ -823,7 +823,7 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
             float w = wd * lf;
             if (MODE == OP_AT) w *= vt.colE[(size_t)v * Nu + k];
             const int col = h.keep ? k : Nu - 1 - k;
-            acc = fmaf(w, ld(sv + col), acc);
+            acc = fmaf(w, ld(sv + XR_BOUND(col, 0, Nu - 1)), acc);
         }
     }
     return acc;

@@ -13,11 +13,6 @@
 
 namespace xr {
 
-// Device-wide sticky error word (one per device that loads the library).
-// 0 = no error; kernels OR in a code when a bounded wait gives up.  Defined
-// here: the library is a single translation unit.
-__device__ unsigned int g_device_error = 0;
-
 constexpr unsigned XR_DEVERR_TMA_TIMEOUT = 1u;
 
 // Poll limits of the bounded waits, per device (xr_set_wait_limits).  After

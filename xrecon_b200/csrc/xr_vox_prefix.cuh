@@ -250,6 +250,18 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                 if (ub >= (float)Nv - 0.5f || ut <= -0.5f) break;
                 const int col = keep ? k : Nu - 1 - k;
                 const char* cb = reinterpret_cast<const char*>(rb + (uintptr_t)col * 8u);
+                // the table entry of a row rounded by the 1.5 * 2^23 add: local row
+                // bits(tr) - bits(1.5 * 2^23), table row r0 + 1 + that
+#ifdef XR_DEBUG_BOUNDS
+                auto entry = [&](float tr) -> float2 {
+                    const long long t = XR_BOUND((long long)r0 + 1 + (__float_as_int(tr) - 0x4B400000), 0, Nv + 1);
+                    return __ldg(reinterpret_cast<const float2*>(tvb) + (size_t)t * Nu + XR_BOUND(col, 0, Nu - 1));
+                };
+#else
+                auto entry = [&](float tr) -> float2 {
+                    return __ldg(reinterpret_cast<const float2*>(cb + (size_t)(unsigned)__float_as_int(tr) * Nu8));
+                };
+#endif
                 const float wk = __fdividef(wf * lf, fib);
                 // rows the run reaches, inside [0, Nv - 1] in every active lane?
                 const bool inside = (ub >= 0.0f) && (ut <= (float)(Nv - 1));
@@ -267,10 +279,8 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                             const float2 tr2 = __fadd2_rn(u2, mg2);   // round to nearest integer
                             const float2 nf2 = __fadd2_rn(tr2, nmg2);
                             const float2 fr2 = __ffma2_rn(nf2, neg2, u2);  // u - n
-                            const float2 ea = __ldg(reinterpret_cast<const float2*>(
-                                cb + (size_t)(unsigned)__float_as_int(tr2.x) * Nu8));
-                            const float2 eb = __ldg(reinterpret_cast<const float2*>(
-                                cb + (size_t)(unsigned)__float_as_int(tr2.y) * Nu8));
+                            const float2 ea = entry(tr2.x);
+                            const float2 eb = entry(tr2.y);
                             const float ga = fmaf(fr2.x, ea.y, ea.x);
                             const float gb = fmaf(fr2.y, eb.y, eb.x);
                             if (i > 0) acc[i - 1] = fmaf(wk, ga - gprev, acc[i - 1]);
@@ -280,8 +290,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                             const float uc = fmaf((float)i, fib, f0);
                             const float tr = uc + 12582912.0f;
                             const float nf = tr - 12582912.0f;
-                            const float2 e = __ldg(reinterpret_cast<const float2*>(
-                                cb + (size_t)(unsigned)__float_as_int(tr) * Nu8));
+                            const float2 e = entry(tr);
                             const float gi = fmaf(uc - nf, e.y, e.x);
                             acc[i - 1] = fmaf(wk, gi - gprev, acc[i - 1]);
                         }
@@ -293,8 +302,7 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
                         const float uc = fminf(fmaxf(fmaf((float)i, fib, f0), ulo), uhi);
                         const float tr = uc + 12582912.0f;
                         const float nf = tr - 12582912.0f;
-                        const float2 e = __ldg(reinterpret_cast<const float2*>(
-                            cb + (size_t)(unsigned)__float_as_int(tr) * Nu8));
+                        const float2 e = entry(tr);
                         const float gi = fmaf(uc - nf, e.y, e.x);
                         if (i > 0) acc[i - 1] = fmaf(wk, gi - gprev, acc[i - 1]);
                         gprev = gi;
