@@ -70,6 +70,9 @@ def build_ref(force: bool = False) -> Path | None:
         return REF_SO if REF_SO.exists() else None
     srcs = [cpu_dir / s for s in REF_CPU_SOURCES] + [HERE / "ref_shim.cpp"]
     REF_DIR.mkdir(exist_ok=True)
+    # where the reference tree was found, for the tests that import its
+    # Python package next to this one (skipped where the tree is absent)
+    (REF_DIR / "reference_root.txt").write_text(str(root) + "\n")
     if force or _stale(REF_SO, srcs):
         # -O3 matches the reference's own C++ flags (setup.py:15).
         _run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread",
