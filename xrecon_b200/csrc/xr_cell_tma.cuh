@@ -239,6 +239,13 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     for (int i = 0; i < R; ++i) acc[i] = 0.0f;
     const double zr0 = zd0 + r0 * dvv;
     const float dpdz = (float)(h.dpix * g.dz);
+    // Per-line terms, affine in the line L (q = q0 + q1 L): the run's first
+    // row in slice units t0 = Qk q zr0 - z0dz (FP64: its floor and fraction
+    // place every row), rows per slice bt = Qk q dvv and q itself for the
+    // line factor (FP32, rounded as the kernel uses them).
+    const double t0c = fma(Qk * h.q0, zr0, -z0dz), t0l = Qk * h.q1 * zr0;
+    const float btc = (float)(Qk * dvv * h.q0), btl = (float)(Qk * dvv * h.q1);
+    const float qc = (float)h.q0, ql = (float)h.q1;
 
     // After a wait gave up, the CTA still walks its remaining lines (every
     // read stays inside the staged windows, whatever they hold) so that all
@@ -257,20 +264,18 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
             const double pk1 = fma(bB1, (double)L, bA1);
             const int pa = max((int)floor(pk), 0);
             const int pb = min((int)ceil(pk1) - 1, npix - 1);
-            const double q = fma(h.q1, (double)L, h.q0);
-            const double gq = Qk * q;
-            const double t0 = fma(gq, zr0, -z0dz);
-            const double bt = gq * dvv;
-            const bool live = !win.empty && (pa <= pb) && (bt > 1.0e-4 && bt < 1.0e4) &&
-                              !(t0 + R * bt <= 0.0 || t0 >= (double)g.D);
+            const float Lf = (float)L;
+            const double t0 = fma(t0l, (double)L, t0c);
+            const float bf = fmaf(btl, Lf, btc);
+            const bool live = !win.empty && (pa <= pb) && (bf > 1.0e-4f && bf < 1.0e4f) &&
+                              !(t0 + R * (double)bf <= 0.0 || t0 >= (double)g.D);
             if (live) {
                 const double jf = floor(t0);
                 const int j0 = (int)jf;
                 const float f = (float)(t0 - jf);
-                const float bf = (float)bt;
                 float lf = cw;
                 if (MODE == OP_A) {
-                    const float qf = (float)q;
+                    const float qf = fmaf(ql, Lf, qc);
                     lf = __fdividef(dpdz, qf * qf);
                 }
                 const float u0 = (float)(pk - (double)pa), u1 = (float)(pk1 - (double)pa);
