@@ -717,11 +717,8 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
     const float yc_x = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);          //   and line centre
     const float xc_y = (float)((ix - 0.5 * g.W + 0.5) * g.dx + g.shx);          // y-axis views: line centre
     const float ya_y = (float)(-0.5 * g.H * g.dy + g.shy) + (float)(g.H - 1 - iy) * dyf;  //   and y edges
-    float pcx = 0.0f, pcy = 0.0f;
-    if (MODE == OP_BW) {
-        pcx = (float)((ix - 0.5 * g.W + 0.5) * g.dx + g.shx);
-        pcy = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);
-    }
+    const float pcx = (float)((ix - 0.5 * g.W + 0.5) * g.dx + g.shx);  // pixel centre
+    const float pcy = (float)((0.5 * g.H - iy - 0.5) * g.dy + g.shy);
     const float sodf = (float)g.sod, shuf = (float)g.shu, inv_du = (float)(1.0 / g.du);
     const float inv_dx = (float)(1.0 / g.dx), inv_dy = (float)(1.0 / g.dy);
     // column bracket margin: half a column, plus the arc guess's angle error
@@ -753,12 +750,21 @@ __device__ __forceinline__ float pix2d_sum(const Geom& g, const ViewTables& vt, 
             kf0 = (__fdividef(sodf * (xa * cf + ya * sf), sodf + xa * sf - ya * cf) - shuf) * inv_du;
             kf1 = (__fdividef(sodf * (xb * cf + yb * sf), sodf + xb * sf - yb * cf) - shuf) * inv_du;
         } else if (g.type == GEO_ARC) {
+            // One guess, at the pixel centre, and a bound on the footprint's
+            // half-width: the segment between the pixel's edges on this line
+            // (half-length a) seen from the source at distance r from its
+            // centre spans at most asin(a / r) <= a / (r - a) rad on each
+            // side.  The bracket may take a column more than the edges'
+            // own guesses would; the walk skips it.
             const float dcx = h.dcx, dcy = h.dcy;
-            const float sxf = (float)h.sx, syf = (float)h.sy;
-            float ex = xa - sxf, ey = ya - syf;
-            kf0 = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
-            ex = xb - sxf; ey = yb - syf;
-            kf1 = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
+            const float ex = pcx - (float)h.sx, ey = pcy - (float)h.sy;
+            const float kc = guess_atan2f(dcx * ey - dcy * ex, dcx * ex + dcy * ey) * inv_du;
+            const float a = 0.5f * (h.use_x ? dxf : dyf);
+            const float r2 = fmaf(ex, ex, ey * ey);
+            const float r = r2 * rsqrtf(r2);
+            const float hw = __fdividef(a, fmaxf(r - a, a)) * inv_du * 1.001f;
+            kf0 = kc - hw;
+            kf1 = kc + hw;
         } else {
             kf0 = (xa * cf + ya * sf - shuf) * inv_du;
             kf1 = (xb * cf + yb * sf - shuf) * inv_du;
