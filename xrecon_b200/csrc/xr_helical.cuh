@@ -553,8 +553,13 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
         const float lf = __fdiv_rn(s.cwW, __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
         const float margin = 0.5f + XR_GUESS_ATAN_ERR * hv.inv_du;
         const float sf = (float)h.s, cf = (float)h.c;
-        const float kf0 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xa, ya, hv.inv_du);
-        const float kf1 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xb, yb, hv.inv_du);
+        // one guess at the pixel centre and a bound on the footprint's
+        // half-width: the pixel's edge segment on this line (half-length a,
+        // at rxy from the source) spans at most a / (rxy - a) rad each side
+        const float kc = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, px, py, hv.inv_du);
+        const float ha = 0.5f * (h.use_x ? gf.dx : gf.dy);
+        const float hw = __fdividef(ha, fmaxf(rxy - ha, ha)) * hv.inv_du * 1.001f;
+        const float kf0 = kc - hw, kf1 = kc + hw;
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const int ka = max(0, (int)floorf(lo - margin));

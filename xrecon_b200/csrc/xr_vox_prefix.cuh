@@ -178,8 +178,23 @@ vox_prefix3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const flo
         lf *= oscale;
         const float sf = (float)h.s, cf = (float)h.c;
         const float dcx = h.dcx, dcy = h.dcy;
-        const float kf0 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xa, ya, inv_du);
-        const float kf1 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xb, yb, inv_du);
+        float kf0, kf1;
+        if (CHAIN) {  // arc detector (the other instantiations keep two guesses: fewer live registers)
+            // one guess at the pixel centre and a bound on the footprint's
+            // half-width: the pixel's edge segment on this line (half-length
+            // a, distance r from the source) spans at most a / (r - a) rad
+            // each side of the centre
+            const float kc = col_guess_fast(gf, h, sf, cf, dcx, dcy, px, py, inv_du);
+            const float ex = px - (float)h.sx, ey = py - (float)h.sy;
+            const float a = 0.5f * (h.use_x ? gf.dx : gf.dy);
+            const float r2 = fmaf(ex, ex, ey * ey);
+            const float hw = __fdividef(a, fmaxf(r2 * rsqrtf(r2) - a, a)) * inv_du * 1.001f;
+            kf0 = kc - hw;
+            kf1 = kc + hw;
+        } else {
+            kf0 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xa, ya, inv_du);
+            kf1 = col_guess_fast(gf, h, sf, cf, dcx, dcy, xb, yb, inv_du);
+        }
         const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
         const int ka = max(0, (int)floorf(lo - margin));
