@@ -458,7 +458,7 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
                const float* __restrict__ ang, const float* __restrict__ zsrc, const float2* __restrict__ tab,
                float* __restrict__ out, const int nview, const int nzg, const double dvv) {
     __shared__ HelZ szw[R];
-    __shared__ int sv[3];
+    __shared__ int sv[5];
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y * NWY + threadIdx.y;
     const int zg = blockIdx.z % nzg, b = blockIdx.z / nzg;
@@ -472,19 +472,27 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
     }
     __syncthreads();
     if (tid == 0) {
-        int lo = nview, hi = -1, allfull = 1;
+        int lo = nview, hi = -1, allfull = 1, in_lo = 0, in_hi = nview - 1;
         for (int i = 0; i < R; ++i) {
             if (szw[i].vs <= szw[i].ve) { lo = min(lo, szw[i].vs); hi = max(hi, szw[i].ve); }
             allfull &= szw[i].full;
+            in_lo = max(in_lo, szw[i].vs);
+            in_hi = min(in_hi, szw[i].ve);
         }
         sv[0] = lo;
         sv[1] = hi;
         sv[2] = allfull;
+        sv[3] = in_lo;  // views inside every slice's window: in_lo .. in_hi
+        sv[4] = in_hi;
     }
     __syncthreads();
     // every slice's weight comes from the table: no exact fan angle needed
     // unless a test falls near an edge
     const bool allfull = sv[2] != 0;
+    const int in_lo = sv[3], in_hi = sv[4];
+    // slice i's centre z (for the approximate row test): pz_0 + i dz
+    const float pz0 = szw[0].pz, dzf = (float)g.dz;
+    const float row_off = 0.5f * (float)g.Nv - 0.5f;
     if (ix >= g.W || iy >= g.H || j0 >= g.D) return;
     const int Nu = g.Nu, Nv = g.Nv;
     const size_t vstride = (size_t)(Nv + 2) * Nu;
@@ -514,18 +522,45 @@ hel_wbp_kernel(const Geom g, const GeomF gf, const ViewTables vt, const HelOpts 
         const float tz = __fdividef(w.sdd, rxy);
         float wt[R];
         bool any = false;
+        if (allfull && v >= in_lo && v <= in_hi) {
+            // CTA-uniform: every slice tabulated and inside its window.  The
+            // approximate row of slice i's centre ray is affine in i (the
+            // slices' z are pz_0 + i dz up to rounding far inside the test's
+            // band); the exact test runs near an edge, as in hw_row_in_fast.
+            const float rk = tz * inv_dv;
+            const float row0 = fmaf(fmaf(pz0 - w.szv, tz, w.szv - w.zs - (float)g.shv), inv_dv, row_off);
+            const float drow = dzf * rk;
+            const float top = (float)g.Nv - 0.5f;
 #pragma unroll
-        for (int i = 0; i < R; ++i) {
-            const HelZ& z = szw[i];
-            float wi = 0.0f;
-            if (v >= z.vs && v <= z.ve)
-                wi = z.full ? wtab[(size_t)(j0 + i) * nview + v]
-                            : hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db,
-                                        s.gmax, ang, zsrc, nview);
-            wt[i] = wi;
-            if (wi != 0.0f) {
-                any = true;
-                if (col_in && hw_row_in_fast(g, w, rxy, tz, inv_dv, z.pz)) valid[i] += wi;
+            for (int i = 0; i < R; ++i) {
+                const float wi = wtab[(size_t)(j0 + i) * nview + v];
+                wt[i] = wi;
+                if (wi != 0.0f) {
+                    any = true;
+                    if (col_in) {
+                        const float row = fmaf((float)i, drow, row0);
+                        bool in;
+                        if (row > -0.5f + HW_BAND && row < top - HW_BAND) in = true;
+                        else if (row < -0.5f - HW_BAND || row > top + HW_BAND) in = false;
+                        else in = hw_row_in(g, w, rxy, szw[i].pz);
+                        if (in) valid[i] += wi;
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const HelZ& z = szw[i];
+                float wi = 0.0f;
+                if (v >= z.vs && v <= z.ve)
+                    wi = z.full ? wtab[(size_t)(j0 + i) * nview + v]
+                                : hw_weight(o, g, px, py, z.pz, w.beta, gamma, w.szv, rxy, z.bc, z.bs, z.be, s.db,
+                                            s.gmax, ang, zsrc, nview);
+                wt[i] = wi;
+                if (wi != 0.0f) {
+                    any = true;
+                    if (col_in && hw_row_in_fast(g, w, rxy, tz, inv_dv, z.pz)) valid[i] += wi;
+                }
             }
         }
         if (!DD || !any) continue;
