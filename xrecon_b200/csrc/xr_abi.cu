@@ -227,7 +227,7 @@ CellPlan plan_cell(const Geom& g) {
     p.BP = round_up(std::max(maxspan, 8), 8);
     p.BZ = (int)maxnz;
     p.ok = p.BP <= 256 && p.BZ <= 256 && p.BZ >= 1 &&
-           (size_t)2 * p.BP * (p.BZ + 1) * 4 + (size_t)std::max(g.W, g.H) * 16 + 16 <= 200 * 1024;
+           (size_t)CELL_NS * p.BP * (p.BZ + 1) * 4 + (size_t)std::max(g.W, g.H) * 16 + 8 * CELL_NS <= 200 * 1024;
     std::lock_guard<std::mutex> lk(mu);
     cache[key] = p;
     return p;
@@ -397,7 +397,8 @@ int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr
     auto kern = p.fine ? cell_tma3d_kernel<TI, TO, R, 2, MODE, true, HEL>
                        : cell_tma3d_kernel<TI, TO, R, 2, MODE, false, HEL>;
     const int maxlines = std::max(g.W, g.H);
-    const size_t smem = 2 * (size_t)cell_stage_elems<TI>(p.BP, p.BZ) * sizeof(TI) + 16 + (size_t)maxlines * sizeof(int4);
+    const size_t smem = CELL_NS * (size_t)cell_stage_elems<TI>(p.BP, p.BZ) * sizeof(TI) + 8 * CELL_NS +
+                        (size_t)maxlines * sizeof(int4);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
     const int RG = CELL_NW * R;

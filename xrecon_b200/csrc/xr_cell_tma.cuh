@@ -88,14 +88,22 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
     return w;
 }
 
-// After a wait gave up: only the last two lines issued, `last` - 1 and
-// `last`, may still have copies in flight (each earlier line's copy was seen
-// to land by the issuing thread before it issued the next line into that
-// stage).  The issuing thread lets them land, or gives up once more, before
-// the CTA exits, which keeps its shared memory allocated until then.
+// Stages of the line ring; the block barrier that frees a stage comes after
+// every XR_CELL_STAGES / 2 lines.
+#ifndef XR_CELL_STAGES
+#define XR_CELL_STAGES 4
+#endif
+constexpr int CELL_NS = XR_CELL_STAGES;
+static_assert(CELL_NS == 2 || CELL_NS == 4, "two or four stages");
+
+// After a wait gave up: only the last CELL_NS lines issued, up to `last`,
+// may still have copies in flight (each earlier line's copy was seen to land
+// by the issuing thread before it issued the next line into that stage).
+// The issuing thread lets them land, or gives up once more, before the CTA
+// exits, which keeps its shared memory allocated until then.
 __device__ __noinline__ void drain_stages(uint64_t* bar, int last) {
-    for (int Lp = max(last - 1, 0); Lp <= last; ++Lp)
-        mbar_wait_bounded(&bar[Lp & 1], (unsigned)((Lp >> 1) & 1));
+    for (int Lp = max(last - (CELL_NS - 1), 0); Lp <= last; ++Lp)
+        mbar_wait_bounded(&bar[Lp % CELL_NS], (unsigned)((Lp / CELL_NS) & 1));
 }
 
 // FINE: the geometry's detector rows are (nearly) all shorter than a voxel,
@@ -129,9 +137,9 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     // branch-free walk (never used in a result)
     const int stage_elems = cell_stage_elems<TI>(BP, BZ);
     TI* stage = reinterpret_cast<TI*>(smem_raw);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)2 * stage_elems * sizeof(TI));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)CELL_NS * stage_elems * sizeof(TI));
     // window of every line of this CTA (computed once, below)
-    int4* wins = reinterpret_cast<int4*>(bar + 2);
+    int4* wins = reinterpret_cast<int4*>(bar + CELL_NS);
 
     const int lane = threadIdx.x, tid = threadIdx.y * 32 + threadIdx.x;
     const int Nu = g.Nu;
@@ -213,8 +221,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     __shared__ int s_abort;
     volatile int* abort = &s_abort;
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int i = 0; i < CELL_NS; ++i) mbar_init(&bar[i], 1);
         fence_barrier_init();
         s_abort = 0;
     }
@@ -225,14 +232,12 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     }
     // The spare row BZ of each stage is never written by TMA; the look-ahead
     // read multiplies it by zero, so it must hold finite values (zeros).
-    for (int i = tid; i < 2 * BP; i += blockDim.x * blockDim.y)
+    for (int i = tid; i < CELL_NS * BP; i += blockDim.x * blockDim.y)
         stage[(size_t)(i / BP) * stage_elems + (size_t)BZ * BP + (i % BP)] = TI(0.0f);
     __syncthreads();
     int last = -1;  // last line issued (issuing thread)
-    if (tid == 0) {
-        if (nlines > 0) issue(0, 0), last = 0;
-        if (nlines > 1) issue(1, 1), last = 1;
-    }
+    if (tid == 0)
+        for (int L = 0; L < min(CELL_NS, nlines); ++L) issue(L, L), last = L;
 
     float acc[R];
 #pragma unroll
@@ -251,8 +256,8 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     // read stays inside the staged windows, whatever they hold) so that all
     // threads meet every barrier; the results are dropped at the end.
     for (int L = 0; L < nlines; ++L) {
-        const int s = L & 1;
-        const unsigned parity = (unsigned)((L >> 1) & 1);
+        const int s = L % CELL_NS;
+        const unsigned parity = (unsigned)((L / CELL_NS) & 1);
         mbar_wait_bounded(&bar[s], parity, abort);
         CellWindow win;
         {
@@ -397,14 +402,20 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                 }
             }
         }
-        __syncthreads();
-        if (tid == 0 && L + 2 < nlines && !*abort) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(L + 2, s);
-            last = L + 2;
+        // every CELL_NS / 2 lines: all warps are done with those lines' stages,
+        // which take the lines CELL_NS further on
+        constexpr int BATCH = CELL_NS / 2;
+        if ((L + 1) % BATCH == 0) {
+            __syncthreads();
+            if (tid == 0 && !*abort) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                for (int j = L + 1 - BATCH; j <= L; ++j)
+                    if (j + CELL_NS < nlines) issue(j + CELL_NS, j % CELL_NS), last = j + CELL_NS;
+            }
         }
     }
-    // every wait ended before the last barrier, so all threads read the same
+    __syncthreads();
+    // every wait ended before this barrier, so all threads read the same
     if (*abort) {
         if (tid == 0) drain_stages(bar, last);
         return;
