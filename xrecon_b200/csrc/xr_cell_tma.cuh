@@ -95,6 +95,10 @@ __host__ __device__ inline CellWindow cell_window(const CellCtaGeo& c, const Vie
 #endif
 constexpr int CELL_NS = XR_CELL_STAGES;
 static_assert(CELL_NS == 2 || CELL_NS == 4, "two or four stages");
+#ifndef XR_CELL_BATCH
+#define XR_CELL_BATCH (XR_CELL_STAGES / 2)  // lines per block barrier
+#endif
+static_assert(XR_CELL_BATCH >= 1 && XR_CELL_BATCH < XR_CELL_STAGES, "a barrier frees at most all but one stage");
 
 // After a wait gave up: only the last CELL_NS lines issued, up to `last`,
 // may still have copies in flight (each earlier line's copy was seen to land
@@ -402,9 +406,9 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                 }
             }
         }
-        // every CELL_NS / 2 lines: all warps are done with those lines' stages,
+        // every BATCH lines: all warps are done with those lines' stages,
         // which take the lines CELL_NS further on
-        constexpr int BATCH = CELL_NS / 2;
+        constexpr int BATCH = XR_CELL_BATCH;
         if ((L + 1) % BATCH == 0) {
             __syncthreads();
             if (tid == 0 && !*abort) {
