@@ -170,7 +170,10 @@ int xr_set_wait_limits(long long tma_polls, long long barrier_polls);
  * copy, so every consumer wait runs out with nothing in flight.  Bit 1: the
  * ragged kernel's grid barriers expect one block more than the grid, so every
  * barrier wait runs out.  Nothing faults; the waits end at their limits
- * (xr_set_wait_limits) and set the device error word.  Synchronous.
+ * (xr_set_wait_limits) and set the device error word.  Bit 2: the staged
+ * prefix backprojection treats every odd view as not fitting its box, so its
+ * fallback launch adds those views.  Bit 3 (read on the host): the prefix
+ * backprojection is not staged.  Synchronous.
  */
 int xr_test_hooks(unsigned int hooks);
 
@@ -178,6 +181,12 @@ int xr_test_hooks(unsigned int hooks);
  * TMA line windows are used, their box size (pixels x z voxels), and whether
  * the fine-row kernel (detector rows shorter than a voxel) is chosen. */
 int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, int* rows_per_thread, int* fine);
+
+/* Staging plan of the 3D prefix backprojection (B, Bw, A^T) for this
+ * geometry: whether each view's table footprint is staged into shared memory
+ * (flat and parallel detectors with an even column count), and the box size
+ * in table columns x rows.  Host-only; no device is touched. */
+int xr_pfx_stage_plan(const xr_geom3d* geom, int* ok, int* box_cols, int* box_rows);
 
 /* Testing aid: nonzero routes every operator through the plain (non-TMA)
  * kernels, so both paths can be compared. */

@@ -75,6 +75,8 @@ def lib():
     L.xr_device_error.argtypes = [ctypes.POINTER(ctypes.c_uint), c_int]
     L.xr_cell_plan.restype = c_int
     L.xr_cell_plan.argtypes = [ctypes.POINTER(Geom3d)] + [ctypes.POINTER(c_int)] * 5
+    L.xr_pfx_stage_plan.restype = c_int
+    L.xr_pfx_stage_plan.argtypes = [ctypes.POINTER(Geom3d)] + [ctypes.POINTER(c_int)] * 3
     L.xr_set_plain_kernels.restype = c_int
     L.xr_set_plain_kernels.argtypes = [c_int]
     L.xr_set_wait_limits.restype = c_int
@@ -377,6 +379,15 @@ def cell_plan(geom: Geom3d) -> dict:
         _raise(rc, "xr_cell_plan")
     return dict(ok=bool(vals[0].value), box_pixels=vals[1].value, box_z=vals[2].value,
                 rows_per_thread=vals[3].value, fine=bool(vals[4].value))
+
+
+def pfx_stage_plan(geom: Geom3d) -> dict:
+    """Staging plan of the 3D prefix backprojection (table box size) for a geometry."""
+    vals = [c_int(0) for _ in range(3)]
+    rc = lib().xr_pfx_stage_plan(ctypes.byref(geom), *[ctypes.byref(v) for v in vals])
+    if rc != 0:
+        _raise(rc, "xr_pfx_stage_plan")
+    return dict(ok=bool(vals[0].value), box_cols=vals[1].value, box_rows=vals[2].value)
 
 
 def set_plain_kernels(on: bool) -> None:

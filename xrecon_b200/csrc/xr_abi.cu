@@ -19,6 +19,7 @@
 
 #include "xr_cell_tma.cuh"
 #include "xr_vox_prefix.cuh"
+#include "xr_vox_stage.cuh"
 #include "xr_ragged.cuh"
 #include "xr_sysmat.cuh"
 #include "xr_rebin.cuh"
@@ -35,6 +36,8 @@ thread_local std::string g_last_error;
 
 // Test hook: route every operator through the plain (non-TMA) kernels.
 bool g_force_plain = false;
+// Host copy of the test hooks (xr_test_hooks); the launch code reads bit 3.
+unsigned g_host_hooks = 0;
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -125,7 +128,7 @@ Geom geom_from(const xr_geom2d* p) {
 }
 
 struct Layout {
-    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, arc, colWR, volT, volR, volF, sinoS, total;
+    size_t hdr, bA, bB, colQ, colR, colE, colF, colM, arc, colWR, volT, volR, volF, sinoS, pfxF, total;
     bool has_arc, has_pfx;
 };
 
@@ -269,6 +272,14 @@ bool encode_line_map(CUtensorMap* m, int dt, const void* base, int npix, int nli
 
 // Image-input ops of the cell gather need the flipped transpose of the image
 // (lines of y-axis views); cone A^T needs an FP32 pre-scaled sinogram.
+#ifndef XR_PFX_R
+#define XR_PFX_R 16
+#endif
+#ifndef XR_PFX_NWY
+#define XR_PFX_NWY 8
+#endif
+constexpr int PFX_R = XR_PFX_R;  // z voxels per thread of the prefix backprojection
+
 Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype_in, bool chain_ok = true) {
     Layout l{};
     size_t o = 0;
@@ -314,6 +325,11 @@ Layout layout(int dim3d, int op, const Geom& g, int nbatch, int nview, int dtype
     l.sinoS = o;
     if (dim3d && (eff == OP_AT || eff == OP_B || eff == OP_BW))
         o = align256(o + (size_t)nbatch * V * (g.Nv + 2) * g.Nu * sizeof(float2));
+    // the staged prefix gather's per-CTA flags (views left to its fallback)
+    l.pfxF = o;
+    if (l.has_pfx)
+        o = align256(o + (size_t)((g.W + PS_T - 1) / PS_T) * ((g.H + PS_T - 1) / PS_T) *
+                             ((g.D + PFX_R - 1) / PFX_R) * nbatch * sizeof(int));
     l.total = o;
     return l;
 }
@@ -372,22 +388,176 @@ GeomF make_geomf(const Geom& g, int dim3d) {
     return f;
 }
 
+// Box of the staged prefix gather (vox_stage3d_kernel), sized by evaluating
+// its window over every tile and z-run of views sampled densely in angle
+// (the windows are smooth functions of the angle; the 45-degree axis
+// switches are sampled on both sides), with two columns and two rows to
+// spare.  A view whose box still comes out larger at run time goes to the
+// fallback launch.  Cached per geometry.
+struct PfxStagePlan {
+    bool ok;
+    int BC, BR;
+};
+
+PfxStagePlan plan_pfx_stage(const Geom& g) {
+    static std::mutex mu;
+    static std::map<std::string, PfxStagePlan> cache;
+    const std::string key(reinterpret_cast<const char*>(&g), sizeof(Geom));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    PfxStagePlan p{false, 0, 0};
+    if ((g.type == GEO_FLAT || g.type == GEO_PARALLEL) && g.Nu % 2 == 0) {
+        const GeomF gf = make_geomf(g, 1);
+        double zd0, dvv, z0dz;
+        {
+            const double rs = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
+            zd0 = (-0.5 * g.Nv * g.dv + g.shv) * rs;
+            dvv = g.dv * rs;
+            z0dz = (-0.5 * g.D * g.dz + g.shz) / g.dz;
+        }
+        const double zoffh = -zd0 / dvv - 0.5;
+        const double uscale = (g.type == GEO_FLAT) ? g.sod / g.sdd : 1.0;
+        std::vector<double> angles;
+        for (int i = 0; i < 256; ++i) angles.push_back(2.0 * M_PI * i / 256 + 0.37 / 256);
+        for (int i = 0; i < 8; ++i) {
+            angles.push_back(M_PI / 4 * i + 1e-5);
+            angles.push_back(M_PI / 4 * i - 1e-5);
+        }
+        int maxc = 0, maxr = 0;
+        bool bad = false;
+        for (double ang : angles) {
+            ViewHdr h;
+            make_view_hdr(g, (float)ang, h);
+            auto colk = [&](double x, double y) {  // fractional column (traversal order) of a point
+                double sg;
+                if (g.type == GEO_FLAT) {
+                    const double R = g.sod;
+                    const double u = R * (x * h.c + y * h.s) / (R + x * h.s - y * h.c);
+                    sg = (u / uscale - g.shu) / g.du;
+                } else {
+                    sg = (x * h.c + y * h.s - g.shu) / g.du;
+                }
+                return h.keep ? sg + 0.5 * g.Nu : 0.5 * g.Nu - sg;
+            };
+            auto colR = [&](int k) { return g.type == GEO_PARALLEL ? g.dz : g.dz / column_mag(g, h, k, uscale); };
+            for (int iy0 = 0; iy0 < g.H; iy0 += PS_T)
+                for (int ix0 = 0; ix0 < g.W; ix0 += PS_T) {
+                    const int ixe = std::min(ix0 + PS_T, g.W) - 1, iye = std::min(iy0 + PS_T, g.H) - 1;
+                    double xl, xr, yl, yh;
+                    int L0, L1;
+                    if (h.use_x) {
+                        L0 = iy0; L1 = iye;
+                        xl = gf.x0 + ix0 * (double)gf.dx; xr = gf.x0 + (ixe + 1) * (double)gf.dx;
+                        yh = gf.yc0 - L0 * (double)gf.dy; yl = gf.yc0 - L1 * (double)gf.dy;
+                    } else {
+                        L0 = ix0; L1 = ixe;
+                        xl = gf.xc0 + L0 * (double)gf.dx; xr = gf.xc0 + L1 * (double)gf.dx;
+                        yl = gf.y0 + (g.H - 1 - iye) * (double)gf.dy; yh = gf.y0 + (g.H - iy0) * (double)gf.dy;
+                    }
+                    const double ks[4] = {colk(xl, yl), colk(xl, yh), colk(xr, yl), colk(xr, yh)};
+                    double gmin = std::min(std::min(ks[0], ks[1]), std::min(ks[2], ks[3]));
+                    double gmax = std::max(std::max(ks[0], ks[1]), std::max(ks[2], ks[3]));
+                    gmin = std::max(std::min(gmin, g.Nu + 2.0), -2.0);
+                    gmax = std::max(std::min(gmax, g.Nu + 2.0), -2.0);
+                    const int kw0 = std::max(0, (int)std::floor(gmin - 1.5)), kw1 = std::min(g.Nu - 1, (int)std::floor(gmax + 1.5));
+                    if (kw0 > kw1) continue;
+                    const int c0 = (h.keep ? kw0 : g.Nu - 1 - kw1) & ~1, c1 = h.keep ? kw1 : g.Nu - 1 - kw0;
+                    maxc = std::max(maxc, c1 - c0 + 1);
+                    const double d0 = std::fma(h.q1, (double)L0, h.q0) * dvv, d1 = std::fma(h.q1, (double)L1, h.q0) * dvv;
+                    const double Ra = colR(kw0), Rb = colR(kw1);
+                    if (!(d0 > 0.0 && d1 > 0.0 && Ra > 0.0 && Rb > 0.0)) { bad = true; continue; }
+                    const double ibmin = std::min(Ra, Rb) / std::max(d0, d1), ibmax = std::max(Ra, Rb) / std::min(d0, d1);
+                    for (int j0 = 0; j0 < g.D; j0 += PFX_R) {
+                        const double zs = j0 + z0dz, zt = zs + PFX_R;
+                        const double ulo = zoffh + std::min(zs * ibmin, zs * ibmax);
+                        const double uhi = zoffh + std::max(zt * ibmin, zt * ibmax);
+                        if (!(ulo <= uhi) || ulo > g.Nv + 2.0 || uhi < -3.0) continue;
+                        const int rlo = std::max(0, (int)std::floor(std::max(ulo, -4.0)));
+                        const int rhi = std::min(g.Nv + 1, (int)std::ceil(std::min(uhi, g.Nv + 4.0)) + 2);
+                        maxr = std::max(maxr, rhi - rlo + 1);
+                    }
+                }
+        }
+        int BC = round_up(std::max(maxc + 2, 8), 2);
+        if (BC % 16 == 0) BC += 2;  // rows of the box then start on different banks
+        const int BR = maxr + 2;
+        // at least 3 CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
+        p.ok = !bad && maxc > 0 && maxr > 0 && BC <= 256 && BR <= 256 && 3 * (pfx_stage_smem(BC, BR) + 1024) <= 228 * 1024;
+        p.BC = BC;
+        p.BR = BR;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = p;
+    return p;
+}
+
+// 3D map over the row-prefix tables [batch x views][Nv + 2][Nu] of float2,
+// read as 8-byte elements, with box (BC, BR, 1).
+bool encode_table_map(CUtensorMap* m, const float2* tab, const Geom& g, int nbv, int BC, int BR) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)g.Nu, (cuuint64_t)(g.Nv + 2), (cuuint64_t)nbv};
+    cuuint64_t strides[2] = {(cuuint64_t)g.Nu * 8, (cuuint64_t)g.Nu * 8 * (g.Nv + 2)};
+    cuuint32_t box[3] = {(cuuint32_t)BC, (cuuint32_t)BR, 1u};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<float2*>(tab), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 constexpr int CELL_R = 8;
 constexpr int VOX_R = 16;
 constexpr int VOX_NW = 4;
-#ifndef XR_PFX_R
-#define XR_PFX_R 16
-#endif
-#ifndef XR_PFX_NWY
-#define XR_PFX_NWY 8
-#endif
-constexpr int PFX_R = XR_PFX_R;      // z voxels per thread of the prefix backprojection
 constexpr int PFX_NWY = XR_PFX_NWY;  // image lines (warps) per CTA
 
 template <typename T> constexpr int dtype_code();
 template <> constexpr int dtype_code<float>() { return DT_F32; }
 template <> constexpr int dtype_code<__nv_bfloat16>() { return DT_BF16; }
 template <> constexpr int dtype_code<__half>() { return DT_F16; }
+
+// Staged prefix gather (vox_stage3d_kernel), then its fallback launch for
+// the views a CTA could not stage; -1 when this geometry is not covered (the
+// caller then uses vox_prefix3d_kernel).
+template <typename TO, int MODE>
+int launch_pfx_stage_mode(const Geom& g, const GeomF& gf, const ViewTables& vt, const CUtensorMap& map,
+                          const float2* tab, TO* out, int* flags, int nbatch, int nview, int nzp, int BC, int BR,
+                          cudaStream_t st, double z0dz, double zd0, double dvv, float cw, float atconst, float oscale) {
+    auto ks = vox_stage3d_kernel<TO, PFX_R, MODE, false>;
+    auto kf = vox_stage3d_kernel<TO, PFX_R, MODE, true>;
+    const size_t smem = pfx_stage_smem(BC, BR), smem_fb = 2 * PS_WCH * sizeof(int4) + 128;
+    if (cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
+    const dim3 grid((g.W + PS_T - 1) / PS_T, (g.H + PS_T - 1) / PS_T, nzp * nbatch);
+    ks<<<grid, PS_T * PS_T, smem, st>>>(g, gf, vt, map, tab, out, flags, nview, nzp, z0dz, zd0, dvv, cw, atconst,
+                                        oscale, BC, BR);
+    if (int rc = check_cuda("vox_stage3d")) return rc;
+    kf<<<grid, PS_T * PS_T, smem_fb, st>>>(g, gf, vt, map, tab, out, flags, nview, nzp, z0dz, zd0, dvv, cw, atconst,
+                                           oscale, BC, BR);
+    return check_cuda("vox_stage3d (fallback)");
+}
+
+template <typename TO>
+int run_pfx_stage(int eff, const Geom& g, const GeomF& gf, const ViewTables& vt, const float2* tab, TO* out,
+                  int nbatch, int nview, int nzp, char* ws, const Layout& l, cudaStream_t st, double z0dz,
+                  double zd0, double dvv, float cw, float atconst, float oscale) {
+    const PfxStagePlan sp = plan_pfx_stage(g);
+    if (!sp.ok) return -1;
+    CUtensorMap map;
+    if (!encode_table_map(&map, tab, g, nbatch * nview, sp.BC, sp.BR)) return -1;
+    int* flags = reinterpret_cast<int*>(ws + l.pfxF);
+    if (eff == OP_AT)
+        return launch_pfx_stage_mode<TO, OP_AT>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
+                                                z0dz, zd0, dvv, cw, atconst, oscale);
+    if (eff == OP_B)
+        return launch_pfx_stage_mode<TO, OP_B>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
+                                               z0dz, zd0, dvv, cw, atconst, oscale);
+    return launch_pfx_stage_mode<TO, OP_BW>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
+                                            z0dz, zd0, dvv, cw, atconst, oscale);
+}
 
 template <typename TI, typename TO, int R, int MODE, bool HEL>
 int launch_cell_tma_mode(const Geom& g, const CellPlan& p, const CUtensorMap& mr, const CUtensorMap& mc,
@@ -556,6 +726,11 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
         if (int rc = check_cuda("row_prefix3d")) return rc;
         const int nzp = (g.D + PFX_R - 1) / PFX_R;
         if ((long long)nzp * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
+        if (!vt.arc && !(g_host_hooks & XR_HOOK_PFX_NOSTAGE)) {
+            const int rc = run_pfx_stage<TO>(eff, g, gf, vt, tab, out, nbatch, nview, nzp, ws, l, st, z0dz, zd0, dvv,
+                                             cw, atconst, oscale);
+            if (rc >= 0) return rc;
+        }
         dim3 pgrid((g.W + 31) / 32, (g.H + PFX_NWY - 1) / PFX_NWY, nzp * nbatch);
         dim3 pblock(32, PFX_NWY);
         if (eff == OP_AT)
@@ -1129,6 +1304,17 @@ int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, in
     return XR_OK;
 }
 
+int xr_pfx_stage_plan(const xr_geom3d* geom, int* ok, int* box_cols, int* box_rows) {
+    if (!geom || !ok || !box_cols || !box_rows) return xr::fail(XR_ERR_INVALID_ARGUMENT, "null pointer");
+    const xr::Geom g = xr::geom_from(geom);
+    if (int rc = xr::validate(g, 1, 0, 1, 1)) return rc;
+    const xr::PfxStagePlan p = xr::plan_pfx_stage(g);
+    *ok = p.ok;
+    *box_cols = p.BC;
+    *box_rows = p.BR;
+    return XR_OK;
+}
+
 int xr_set_plain_kernels(int on) {
     xr::g_force_plain = (on != 0);
     return XR_OK;
@@ -1156,6 +1342,7 @@ int xr_set_wait_limits(long long tma_polls, long long barrier_polls) {
 }
 
 int xr_test_hooks(unsigned int hooks) {
+    xr::g_host_hooks = hooks;
     if (cudaMemcpyToSymbol(xr::g_test_hooks, &hooks, sizeof(hooks)) != cudaSuccess)
         return xr::fail(XR_ERR_CUDA, "setting the test hooks failed");
     return XR_OK;
