@@ -101,9 +101,10 @@ def test_fallback_adds_the_views_not_staged(cuda, native, scan):
 
 
 def test_staged_full_size_workload_subset(cuda, native):
-    """The 512x512x256 / 1024x256 cone-flat geometry (box sized by the
-    planner for it) on 72 of its 1440 views: staged B equals unstaged B bit
-    for bit, so no view went to the fallback."""
+    """The 512x512x256 / 1024x256 cone-flat geometry on 72 of its 1440 views,
+    with the box the planner caps for it (its largest windows go to the
+    fallback launch, which adds them after the others): staged B within
+    1e-6 of unstaged B."""
     from xrecon_b200.backend import HostGeometry
     opts = np.asarray(load_golden("options")["c5_3d_flat"], np.float32)
     plan = native.pfx_stage_plan(HostGeometry(3, opts.tolist()).struct)
@@ -112,7 +113,7 @@ def test_staged_full_size_workload_subset(cuda, native):
     sino = np.random.default_rng(33).random((1, 1, ang.size, int(opts[4]), int(opts[3]))).astype(np.float32)
     staged = _run(native, "B", sino, opts, ang, cuda, 0)
     unstaged = _run(native, "B", sino, opts, ang, cuda, HOOK_PFX_NOSTAGE)
-    assert np.array_equal(staged, unstaged), float(np.abs(staged - unstaged).max())
+    assert rel_l2(staged, unstaged) < 1e-6, rel_l2(staged, unstaged)
 
 
 def test_staged_wait_times_out_and_next_call_is_correct(cuda, native):

@@ -166,14 +166,15 @@ def test_projection_staging_plans_without_gpu():
 
 def test_backprojection_staging_plans_without_gpu():
     """The host planner of the staged prefix backprojection (no GPU needed):
-    the table box of the 512x512x256 / 1024x256 cone-flat workload fits two
-    stages at three CTAs per SM; parallel geometries are staged too, arc
+    the table box of the 512x512x256 / 1024x256 cone-flat workload is capped
+    at two stages for four CTAs per SM (the few larger windows go to the
+    fallback launch); parallel geometries are staged too, arc
     detectors and odd column counts are not."""
     opts = load_golden("options")
     c5 = _native.pfx_stage_plan(_native.geom3d_from_values(opts["c5_3d_flat"]))
     assert c5["ok"] and c5["box_cols"] % 2 == 0, c5
     smem = 2 * 64 * 16 + 128 + 2 * ((c5["box_cols"] * c5["box_rows"] * 8 + 127) // 128 * 128)
-    assert 3 * (smem + 1024) <= 228 * 1024, (c5, smem)
+    assert 4 * (smem + 1024) <= 228 * 1024, (c5, smem)
     par = _native.pfx_stage_plan(_native.geom3d_from_values(
         G.pack_options3d(G.Volume3d((64, 64, 32), 1.0), G.ParallelBeam3d(G.Detector3d((96, 40), 1.0)))))
     assert par["ok"], par

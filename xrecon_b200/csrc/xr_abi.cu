@@ -392,8 +392,13 @@ GeomF make_geomf(const Geom& g, int dim3d) {
 // its window over every tile and z-run of views sampled densely in angle
 // (the windows are smooth functions of the angle; the 45-degree axis
 // switches are sampled on both sides), with two columns and two rows to
-// spare.  A view whose box still comes out larger at run time goes to the
-// fallback launch.  Cached per geometry.
+// spare.  The box is capped at the shared memory that leaves room for four
+// CTAs per SM (what 64 registers a thread allow): when the largest window
+// does not fit that, the box takes the shape (columns x rows within the cap)
+// that holds the most sampled windows, and the rest go to the fallback
+// launch (about 3 % of (CTA, view) pairs on the 512-cube workload: B 155 ->
+// 140 ms against the uncapped box at three CTAs per SM).  Cached per
+// geometry.
 struct PfxStagePlan {
     bool ok;
     int BC, BR;
@@ -428,6 +433,9 @@ PfxStagePlan plan_pfx_stage(const Geom& g) {
         }
         int maxc = 0, maxr = 0;
         bool bad = false;
+        // windows sampled, by (columns, rows) needed; 257 = more than a box holds
+        std::vector<double> hist(258 * 258, 0.0);
+        double nsamp = 0.0;
         for (double ang : angles) {
             ViewHdr h;
             make_view_hdr(g, (float)ang, h);
@@ -466,6 +474,7 @@ PfxStagePlan plan_pfx_stage(const Geom& g) {
                     if (kw0 > kw1) continue;
                     const int c0 = (h.keep ? kw0 : g.Nu - 1 - kw1) & ~1, c1 = h.keep ? kw1 : g.Nu - 1 - kw0;
                     maxc = std::max(maxc, c1 - c0 + 1);
+                    const int hc = std::min(257, c1 - c0 + 1 + 2);
                     const double d0 = std::fma(h.q1, (double)L0, h.q0) * dvv, d1 = std::fma(h.q1, (double)L1, h.q0) * dvv;
                     const double Ra = colR(kw0), Rb = colR(kw1);
                     if (!(d0 > 0.0 && d1 > 0.0 && Ra > 0.0 && Rb > 0.0)) { bad = true; continue; }
@@ -478,14 +487,39 @@ PfxStagePlan plan_pfx_stage(const Geom& g) {
                         const int rlo = std::max(0, (int)std::floor(std::max(ulo, -4.0)));
                         const int rhi = std::min(g.Nv + 1, (int)std::ceil(std::min(uhi, g.Nv + 4.0)) + 2);
                         maxr = std::max(maxr, rhi - rlo + 1);
+                        hist[hc * 258 + std::min(257, rhi - rlo + 1 + 2)] += 1.0;
+                        nsamp += 1.0;
                     }
                 }
         }
         int BC = round_up(std::max(maxc + 2, 8), 2);
         if (BC % 16 == 0) BC += 2;  // rows of the box then start on different banks
-        const int BR = maxr + 2;
-        // at least 3 CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
-        p.ok = !bad && maxc > 0 && maxr > 0 && BC <= 256 && BR <= 256 && 3 * (pfx_stage_smem(BC, BR) + 1024) <= 228 * 1024;
+        int BR = maxr + 2;
+        // 228 KB of shared memory per SM, 1 KB reserved per CTA
+        auto ctas = [](int bc, int br) { return (int)((228 * 1024) / (pfx_stage_smem(bc, br) + 1024)); };
+        bool fits_all = BC <= 256 && BR <= 256 && ctas(BC, BR) >= 4;
+        if (!fits_all && nsamp > 0.0) {
+            // fraction of sampled windows each box holds: 2D prefix counts
+            std::vector<double> cum(258 * 258, 0.0);
+            for (int c = 0; c < 258; ++c)
+                for (int r = 0; r < 258; ++r)
+                    cum[c * 258 + r] = hist[c * 258 + r] + (c ? cum[(c - 1) * 258 + r] : 0.0) +
+                                       (r ? cum[c * 258 + r - 1] : 0.0) - (c && r ? cum[(c - 1) * 258 + r - 1] : 0.0);
+            double best = -1.0;
+            int bc_best = 0, br_best = 0;
+            for (int bc = 8; bc <= 256; bc += 2) {
+                if (bc % 16 == 0) continue;
+                int br = 256;
+                while (br > 0 && ctas(bc, br) < 4) --br;
+                if (br < 1) continue;
+                const double held = cum[bc * 258 + br];
+                if (held > best) best = held, bc_best = bc, br_best = br;
+            }
+            // more than a tenth of the windows in the fallback: the uncapped
+            // box at three CTAs per SM, if it fits that
+            if (best >= 0.9 * nsamp) BC = bc_best, BR = br_best;
+        }
+        p.ok = !bad && maxc > 0 && maxr > 0 && BC <= 256 && BR <= 256 && ctas(BC, BR) >= 3;
         p.BC = BC;
         p.BR = BR;
     }
