@@ -414,7 +414,8 @@ PfxStagePlan plan_pfx_stage(const Geom& g) {
         if (it != cache.end()) return it->second;
     }
     PfxStagePlan p{false, 0, 0};
-    if ((g.type == GEO_FLAT || g.type == GEO_PARALLEL) && g.Nu % 2 == 0) {
+    if ((g.type == GEO_FLAT || g.type == GEO_PARALLEL || g.type == GEO_ARC) && g.Nu % 2 == 0 &&
+        (g.type != GEO_ARC || XR_GUESS_ATAN_ERR / g.du < 0.25)) {
         const GeomF gf = make_geomf(g, 1);
         double zd0, dvv, z0dz;
         {
@@ -441,7 +442,10 @@ PfxStagePlan plan_pfx_stage(const Geom& g) {
             make_view_hdr(g, (float)ang, h);
             auto colk = [&](double x, double y) {  // fractional column (traversal order) of a point
                 double sg;
-                if (g.type == GEO_FLAT) {
+                if (g.type == GEO_ARC) {
+                    const double ex = x - h.sx, ey = y - h.sy;
+                    sg = std::atan2(h.dcx * ey - h.dcy * ex, h.dcx * ex + h.dcy * ey) / g.du;
+                } else if (g.type == GEO_FLAT) {
                     const double R = g.sod;
                     const double u = R * (x * h.c + y * h.s) / (R + x * h.s - y * h.c);
                     sg = (u / uscale - g.shu) / g.du;
@@ -476,9 +480,14 @@ PfxStagePlan plan_pfx_stage(const Geom& g) {
                     maxc = std::max(maxc, c1 - c0 + 1);
                     const int hc = std::min(257, c1 - c0 + 1 + 2);
                     const double d0 = std::fma(h.q1, (double)L0, h.q0) * dvv, d1 = std::fma(h.q1, (double)L1, h.q0) * dvv;
-                    const double Ra = colR(kw0), Rb = colR(kw1);
-                    if (!(d0 > 0.0 && d1 > 0.0 && Ra > 0.0 && Rb > 0.0)) { bad = true; continue; }
-                    const double ibmin = std::min(Ra, Rb) / std::max(d0, d1), ibmax = std::max(Ra, Rb) / std::min(d0, d1);
+                    double slack = 0.0;
+                    if (g.type == GEO_ARC) {
+                        const double wd = (double)(kw1 - kw0 + 1) * g.du;
+                        slack = 1.01 * g.dz * g.sdd / std::fabs(h.sperp) * wd * wd / 8.0 + 1e-12;
+                    }
+                    const double Rlo = std::min(colR(kw0), colR(kw1)) - slack, Rhi = std::max(colR(kw0), colR(kw1)) + slack;
+                    if (!(d0 > 0.0 && d1 > 0.0 && Rlo > 0.0)) { bad = true; continue; }
+                    const double ibmin = Rlo / std::max(d0, d1), ibmax = Rhi / std::min(d0, d1);
                     for (int j0 = 0; j0 < g.D; j0 += PFX_R) {
                         const double zs = j0 + z0dz, zt = zs + PFX_R;
                         const double ulo = zoffh + std::min(zs * ibmin, zs * ibmax);

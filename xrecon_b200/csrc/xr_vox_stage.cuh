@@ -1,6 +1,7 @@
 // Voxel gather (B, Bw, A^T) with TMA-staged row-prefix tables.
 //
-// Flat and parallel geometries.  The arithmetic per (pixel, view, column) is
+// Flat, parallel and (for A^T, whose column walk is not chained) arc
+// detectors.  The arithmetic per (pixel, view, column) is
 // that of vox_prefix3d_kernel (xr_vox_prefix.cuh), and so are the results
 // when every view is staged; what changes is where the table lookups go.
 //
@@ -13,8 +14,10 @@
 //            by the brackets' half column and one column more;
 //   rows:    the rows the z-run reaches at the extremes of the rows-per-voxel
 //            factor colR / (q dvv) over those columns and the tile's lines
-//            (colR is linear in the column on these detectors, q in the line),
-//            one row of margin each side.
+//            (colR is linear in the column on flat detectors and a sinusoid
+//            of the column angle on arc ones, whose distance from its chord
+//            over the box is at most amplitude * width^2 / 8; q is linear in
+//            the line), one row of margin each side.
 // One thread copies each view's box into a ring of PS_NS stages with a tiled
 // TMA load, PS_NS views ahead of the consumers; the lookups are shared-memory
 // loads with 32-bit addresses.  A global-memory lookup of the same table, even
@@ -99,13 +102,22 @@ __device__ inline int4 pfx_window(const Geom& g, const GeomF& gf, const ViewTabl
     corner(xl, yl); corner(xl, yh); corner(xr, yl); corner(xr, yh);
     const float lo = fmaxf(fminf(gmin, (float)g.Nu + 2.0f), -2.0f);
     const float hi = fmaxf(fminf(gmax, (float)g.Nu + 2.0f), -2.0f);
-    const int kw0 = max(0, (int)floorf(lo - 1.5f)), kw1 = min(g.Nu - 1, (int)floorf(hi + 1.5f));
+    // the consumers' half column and guess error, the corners' guess error, one column
+    const float wm = 1.5f + (g.type == GEO_ARC ? 2.0f * XR_GUESS_ATAN_ERR * gf.inv_du : 0.0f);
+    const int kw0 = max(0, (int)floorf(lo - wm)), kw1 = min(g.Nu - 1, (int)floorf(hi + wm));
     if (kw0 > kw1) return none;
     // rows per voxel ib = colR / (q dvv) at its extremes over the box
     const double d0 = fma(h.q1, (double)L0, h.q0) * dvv, d1 = fma(h.q1, (double)L1, h.q0) * dvv;
-    const double Ra = vt.colR[(size_t)v * g.Nu + kw0], Rb = vt.colR[(size_t)v * g.Nu + kw1];
-    if (!(d0 > 0.0 && d1 > 0.0 && Ra > 0.0 && Rb > 0.0)) return unfit;
-    const double ibmin = fmin(Ra, Rb) / fmax(d0, d1), ibmax = fmax(Ra, Rb) / fmin(d0, d1);
+    double Ra = vt.colR[(size_t)v * g.Nu + kw0], Rb = vt.colR[(size_t)v * g.Nu + kw1];
+    double slack = 0.0;
+    if (g.type == GEO_ARC) {
+        // colR = dz (1 -/+ sdd trig(angle) / sperp): amplitude dz sdd / |sperp|
+        const double wd = (double)(kw1 - kw0 + 1) * g.du;
+        slack = 1.01 * g.dz * g.sdd / fabs(h.sperp) * wd * wd / 8.0 + 1e-12;
+    }
+    const double Rlo = fmin(Ra, Rb) - slack, Rhi = fmax(Ra, Rb) + slack;
+    if (!(d0 > 0.0 && d1 > 0.0 && Rlo > 0.0)) return unfit;
+    const double ibmin = Rlo / fmax(d0, d1), ibmax = Rhi / fmin(d0, d1);
     const double zt = zs + (double)R;
     const double ulo = zoffh + fmin(zs * ibmin, zs * ibmax), uhi = zoffh + fmax(zt * ibmin, zt * ibmax);
     // table row of detector coordinate d: 1 + round(d); one row of margin
@@ -165,7 +177,8 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
     const double zoffh = -zd0 / dvv - 0.5;  // u0 = zs * (rows per voxel) + zoffh
     const float dpdz = (float)g.dz;
     const float inv_du = gf.inv_du;
-    const float margin = 0.5f;
+    // column bracket margin: half a column, plus the arc guess's angle error
+    const float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * inv_du : 0.0f);
 
     __shared__ int s_abort, s_unfit;
     volatile int* abort = &s_abort;
