@@ -138,3 +138,32 @@ def test_staged_wait_times_out_and_next_call_is_correct(cuda, native):
     got = _run(native, "B", sino, opts, ang, cuda, 0)
     assert native.device_error(clear=True) == 0
     assert rel_l2(got, O.dd3d("B", sino, opts, ang)) < 1e-5
+
+
+@pytest.mark.parametrize("case", ["ffs", "reverse", "half_scan"])
+def test_helical_staged_equals_unstaged(cuda, native, case):
+    """Helical B and A^T (per-view z placement and column pitch, views whose
+    z reach misses a run skipped): staged equals unstaged bit for bit; with
+    every odd view left to the fallback, within 1e-6."""
+    from test_gpu_helical import CASES as HCASES, METHOD, _case_angles, _inputs, _projector, _source_pos
+    over, ffs = HCASES[case]
+    P = _projector(**over)
+    V = 240
+    ang = _case_angles(case, V)
+    sp = _source_pos(P, ang, ffs)
+    _, y = _inputs(P, V, batch=2)
+    a, s, yt = torch.from_numpy(ang).to(cuda), torch.from_numpy(sp).to(cuda), torch.from_numpy(y).to(cuda)
+
+    def run(op, hooks):
+        native.test_hooks(hooks)
+        out = getattr(P, METHOD[op])(yt, a, s)
+        torch.cuda.synchronize()
+        native.test_hooks(0)
+        return out.cpu().numpy()
+
+    for op in ("B", "AT"):
+        staged, unstaged = run(op, 0), run(op, HOOK_PFX_NOSTAGE)
+        assert np.array_equal(staged, unstaged), (case, op, float(np.abs(staged - unstaged).max()))
+        assert rel_l2(run(op, HOOK_PFX_UNFIT), unstaged) < 1e-6, (case, op)
+        assert rel_l2(staged, O.helical3d(op, y, P.options.numpy(), ang, sp)) < 1e-5, (case, op)
+    assert native.device_error(clear=True) == 0

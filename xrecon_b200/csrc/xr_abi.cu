@@ -565,12 +565,12 @@ template <> constexpr int dtype_code<__half>() { return DT_F16; }
 // Staged prefix gather (vox_stage3d_kernel), then its fallback launch for
 // the views a CTA could not stage; -1 when this geometry is not covered (the
 // caller then uses vox_prefix3d_kernel).
-template <typename TO, int MODE>
+template <typename TO, int MODE, bool HEL>
 int launch_pfx_stage_mode(const Geom& g, const GeomF& gf, const ViewTables& vt, const CUtensorMap& map,
                           const float2* tab, TO* out, int* flags, int nbatch, int nview, int nzp, int BC, int BR,
                           cudaStream_t st, double z0dz, double zd0, double dvv, float cw, float atconst, float oscale) {
-    auto ks = vox_stage3d_kernel<TO, PFX_R, MODE, false>;
-    auto kf = vox_stage3d_kernel<TO, PFX_R, MODE, true>;
+    auto ks = vox_stage3d_kernel<TO, PFX_R, MODE, false, HEL>;
+    auto kf = vox_stage3d_kernel<TO, PFX_R, MODE, true, HEL>;
     const size_t smem = pfx_stage_smem(BC, BR), smem_fb = 2 * PS_WCH * sizeof(int4) + 128;
     if (cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
@@ -583,7 +583,7 @@ int launch_pfx_stage_mode(const Geom& g, const GeomF& gf, const ViewTables& vt, 
     return check_cuda("vox_stage3d (fallback)");
 }
 
-template <typename TO>
+template <typename TO, bool HEL = false>
 int run_pfx_stage(int eff, const Geom& g, const GeomF& gf, const ViewTables& vt, const float2* tab, TO* out,
                   int nbatch, int nview, int nzp, char* ws, const Layout& l, cudaStream_t st, double z0dz,
                   double zd0, double dvv, float cw, float atconst, float oscale) {
@@ -593,13 +593,14 @@ int run_pfx_stage(int eff, const Geom& g, const GeomF& gf, const ViewTables& vt,
     if (!encode_table_map(&map, tab, g, nbatch * nview, sp.BC, sp.BR)) return -1;
     int* flags = reinterpret_cast<int*>(ws + l.pfxF);
     if (eff == OP_AT)
-        return launch_pfx_stage_mode<TO, OP_AT>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
-                                                z0dz, zd0, dvv, cw, atconst, oscale);
+        return launch_pfx_stage_mode<TO, OP_AT, HEL>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR,
+                                                     st, z0dz, zd0, dvv, cw, atconst, oscale);
     if (eff == OP_B)
-        return launch_pfx_stage_mode<TO, OP_B>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
-                                               z0dz, zd0, dvv, cw, atconst, oscale);
-    return launch_pfx_stage_mode<TO, OP_BW>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
-                                            z0dz, zd0, dvv, cw, atconst, oscale);
+        return launch_pfx_stage_mode<TO, OP_B, HEL>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR,
+                                                    st, z0dz, zd0, dvv, cw, atconst, oscale);
+    if (HEL) return -1;  // the helical Bw is hel_wbp_kernel
+    return launch_pfx_stage_mode<TO, OP_BW, HEL>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
+                                                 z0dz, zd0, dvv, cw, atconst, oscale);
 }
 
 template <typename TI, typename TO, int R, int MODE, bool HEL>
@@ -1095,6 +1096,14 @@ int helical(int op, const Geom& g, const HelOpts& o, const float* in, float* out
     dim3 pgrid((g.W + 31) / 32, (g.H + PFX_NWY - 1) / PFX_NWY, nzp * nbatch);
     dim3 pblock(32, PFX_NWY);
     const float atconst = (float)(g.dx * g.dy * g.dz / (g.du * g.dv));
+    // the table footprints staged in shared memory (the box from the plan of
+    // the same volume and detector on a circular scan; views whose box does
+    // not fit go to the fallback launch)
+    if (!(g_host_hooks & XR_HOOK_PFX_NOSTAGE)) {
+        const int rc = run_pfx_stage<float, true>(op, g, gf, vt, tab, out, nbatch, nview, nzp, ws, hl.l, st, z0dz, zd0,
+                                                  dvv, 0.0f, atconst, 1.0f);
+        if (rc >= 0) return rc;
+    }
     if (op == OP_AT)
         vox_prefix3d_kernel<float, PFX_R, PFX_NWY, OP_AT, true><<<pgrid, pblock, 0, st>>>(
             g, gf, vt, tab, out, nview, nzp, z0dz, zd0, dvv, 0.0f, atconst, 1.0f);

@@ -68,12 +68,28 @@ __host__ __device__ inline size_t pfx_stage_smem(int BC, int BR) {
 //    first and last traversal column klo, khi}.
 // klo > khi: nothing of the tile reaches the view (nothing to stage).
 // c0 < 0: the box does not fit BC x BR (the view is left to the fallback).
+// HEL: helical scan; the view's z placement and angular column pitch come
+// from vt.hel (zs and zoffh are then the view's, from the run's first voxel
+// j0), and a view whose z reach misses the run has nothing to stage.
+template <bool HEL>
 __device__ inline int4 pfx_window(const Geom& g, const GeomF& gf, const ViewTables& vt, const int v, const int ix0,
-                                  const int iy0, const double zs, const double zoffh, const double dvv, const int R,
+                                  const int iy0, const int j0, double zs, double zoffh, const double dvv, const int R,
                                   const int BC, const int BR) {
     const int4 unfit = make_int4(-1, 0, 0, 0), none = make_int4(0, 0, 1, 0);
     if ((*(volatile unsigned*)&g_test_hooks & XR_HOOK_PFX_UNFIT) && (v & 1)) return unfit;
     const ViewHdr& h = vt.hdr[v];
+    float inv_du = gf.inv_du;
+    double du = g.du;
+    if (HEL) {
+        const HelView& hv = vt.hel[v];
+        const float zrun_lo = (float)((-0.5 * g.D + j0) * g.dz + g.shz);
+        const float zrun_hi = (float)((-0.5 * g.D + min(j0 + R, g.D)) * g.dz + g.shz);
+        if (zrun_hi < hv.zlo || zrun_lo > hv.zhi) return none;
+        zs = (double)j0 + hv.z0dz;
+        zoffh = hv.zoffh;
+        inv_du = hv.inv_du;
+        du = 1.0 / (double)hv.inv_du;
+    }
     const int ixe = min(ix0 + PS_T, g.W) - 1, iye = min(iy0 + PS_T, g.H) - 1;
     // the tile's points as the consumers place them (segment ends of each
     // pixel on its line) and its first and last line
@@ -95,7 +111,7 @@ __device__ inline int4 pfx_window(const Geom& g, const GeomF& gf, const ViewTabl
     const float sf = (float)h.s, cf = (float)h.c;
     float gmin = 3.0e38f, gmax = -3.0e38f;
     auto corner = [&](float x, float y) {
-        const float k = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, x, y, gf.inv_du);
+        const float k = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, x, y, inv_du);
         gmin = fminf(gmin, k);
         gmax = fmaxf(gmax, k);
     };
@@ -103,7 +119,7 @@ __device__ inline int4 pfx_window(const Geom& g, const GeomF& gf, const ViewTabl
     const float lo = fmaxf(fminf(gmin, (float)g.Nu + 2.0f), -2.0f);
     const float hi = fmaxf(fminf(gmax, (float)g.Nu + 2.0f), -2.0f);
     // the consumers' half column and guess error, the corners' guess error, one column
-    const float wm = 1.5f + (g.type == GEO_ARC ? 2.0f * XR_GUESS_ATAN_ERR * gf.inv_du : 0.0f);
+    const float wm = 1.5f + (HEL || g.type == GEO_ARC ? 2.0f * XR_GUESS_ATAN_ERR * inv_du : 0.0f);
     const int kw0 = max(0, (int)floorf(lo - wm)), kw1 = min(g.Nu - 1, (int)floorf(hi + wm));
     if (kw0 > kw1) return none;
     // rows per voxel ib = colR / (q dvv) at its extremes over the box
@@ -112,7 +128,7 @@ __device__ inline int4 pfx_window(const Geom& g, const GeomF& gf, const ViewTabl
     double slack = 0.0;
     if (g.type == GEO_ARC) {
         // colR = dz (1 -/+ sdd trig(angle) / sperp): amplitude dz sdd / |sperp|
-        const double wd = (double)(kw1 - kw0 + 1) * g.du;
+        const double wd = (double)(kw1 - kw0 + 1) * du;
         slack = 1.01 * g.dz * g.sdd / fabs(h.sperp) * wd * wd / 8.0 + 1e-12;
     }
     const double Rlo = fmin(Ra, Rb) - slack, Rhi = fmax(Ra, Rb) + slack;
@@ -148,7 +164,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 // elements, box {BC, BR, 1}.  unfit[cta]: set by the staged launch when it
 // skipped a view; the FALLBACK launch does only those CTAs' skipped views,
 // adding to what the staged launch stored.
-template <typename TO, int R, int MODE, bool FALLBACK>
+template <typename TO, int R, int MODE, bool FALLBACK, bool HEL = false>
 __global__ void __launch_bounds__(PS_T * PS_T, XR_PFXS_MINB)
 vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __grid_constant__ CUtensorMap map,
                    const float2* __restrict__ tab, TO* __restrict__ vol, int* __restrict__ unfit, const int nview,
@@ -173,12 +189,10 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
     const unsigned Nu8 = (unsigned)Nu * 8u;
     const size_t vstride = (size_t)(Nv + 2) * Nu;
     const float2* __restrict__ tb = tab + (size_t)b * nview * vstride;
-    const double zs = (double)j0 + z0dz;  // run bottom, in voxel units from z = 0
-    const double zoffh = -zd0 / dvv - 0.5;  // u0 = zs * (rows per voxel) + zoffh
+    const double zs0 = (double)j0 + z0dz;  // run bottom, in voxel units from z = 0
+    const double zoffh0 = -zd0 / dvv - 0.5;  // u0 = zs * (rows per voxel) + zoffh
     const float dpdz = (float)g.dz;
-    const float inv_du = gf.inv_du;
-    // column bracket margin: half a column, plus the arc guess's angle error
-    const float margin = 0.5f + (g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * inv_du : 0.0f);
+
 
     __shared__ int s_abort, s_unfit;
     volatile int* abort = &s_abort;
@@ -192,7 +206,7 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
     }
     auto windows = [&](int vbase) {
         if (tid < PS_WCH && vbase + tid < nview) {
-            const int4 w = pfx_window(g, gf, vt, vbase + tid, ix0, iy0, zs, zoffh, dvv, R, BC, BR);
+            const int4 w = pfx_window<HEL>(g, gf, vt, vbase + tid, ix0, iy0, j0, zs0, zoffh0, dvv, R, BC, BR);
             wins[((vbase / PS_WCH) & 1) * PS_WCH + tid] = w;
             if (w.x < 0) s_unfit = 1;
         }
@@ -234,6 +248,19 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
         if (mine && active && !(!FALLBACK && *abort)) do {
             const ViewHdr& h = vt.hdr[v];
             const int keep = h.keep;
+            // the view's z placement, column width and angular pitch
+            // (helical), and the column bracket margin: half a column, plus
+            // the arc guess's angle error
+            double zs = zs0, zoffh = zoffh0;
+            float cwv = cw, inv_du = gf.inv_du;
+            if (HEL) {
+                const HelView& hv = vt.hel[v];
+                zs = (double)j0 + hv.z0dz;
+                zoffh = hv.zoffh;
+                cwv = hv.cw;
+                inv_du = hv.inv_du;
+            }
+            const float margin = 0.5f + (HEL || g.type == GEO_ARC ? XR_GUESS_ATAN_ERR * inv_du : 0.0f);
             int L, p;
             float xa, ya, xb, yb, px, py;
             if (h.use_x) {
@@ -256,7 +283,7 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
                 if (g.type == GEO_PARALLEL) lf = atconst;
                 else { const float qf = (float)q; lf = (float)h.dpix * dpdz / (qf * qf); }
             } else {
-                lf = cw;
+                lf = cwv;
                 if (MODE == OP_BW) lf *= fbp_weight(g, h, px, py);
             }
             lf *= oscale;
