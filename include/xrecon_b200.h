@@ -184,9 +184,8 @@ int xr_cell_plan(const xr_geom3d* geom, int* ok, int* box_pixels, int* box_z, in
 
 /* Staging plan of the 3D prefix backprojection (B, Bw, A^T) for this
  * geometry: whether each view's table footprint is staged into shared memory
- * (flat, parallel and arc detectors with an even column count; on arc
- * detectors B and Bw, whose column walk is chained, are not staged), and the
- * box size in table columns x rows.  Host-only; no device is touched. */
+ * (flat, parallel and arc detectors with an even column count), and the box
+ * size in table columns x rows.  Host-only; no device is touched. */
 int xr_pfx_stage_plan(const xr_geom3d* geom, int* ok, int* box_cols, int* box_rows);
 
 /* Testing aid: nonzero routes every operator through the plain (non-TMA)

@@ -83,8 +83,7 @@ def test_staged_equals_unstaged_and_oracle(cuda, native, scan):
         plan = native.pfx_stage_plan(HostGeometry(3, opts.tolist()).struct)
         assert plan["ok"], (scan, plan)
         sino = rng.random((1, 1, ang.size, int(opts[4]), int(opts[3]))).astype(np.float32)
-        # on the arc detector only A^T is staged (B and Bw chain their columns)
-        for op in (("AT",) if scan == "arc" else ("B", "BW", "AT")):
+        for op in ("B", "BW", "AT"):
             staged = _run(native, op, sino, opts, ang, cuda, 0)
             unstaged = _run(native, op, sino, opts, ang, cuda, HOOK_PFX_NOSTAGE)
             assert np.array_equal(staged, unstaged), (scan, op, float(np.abs(staged - unstaged).max()))
@@ -97,7 +96,7 @@ def test_fallback_adds_the_views_not_staged(cuda, native, scan):
     rng = np.random.default_rng(32)
     for opts in CASES[scan][:2]:
         sino = rng.random((2, 1, ang.size, int(opts[4]), int(opts[3]))).astype(np.float32)
-        for op in (("AT",) if scan == "arc" else ("B", "AT")):
+        for op in ("B", "AT"):
             half = _run(native, op, sino, opts, ang, cuda, HOOK_PFX_UNFIT)
             unstaged = _run(native, op, sino, opts, ang, cuda, HOOK_PFX_NOSTAGE)
             assert rel_l2(half, unstaged) < 1e-6, (scan, op)

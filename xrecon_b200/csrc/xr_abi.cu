@@ -474,7 +474,15 @@ PfxStagePlan plan_pfx_stage(const Geom& g) {
                     double gmax = std::max(std::max(ks[0], ks[1]), std::max(ks[2], ks[3]));
                     gmin = std::max(std::min(gmin, g.Nu + 2.0), -2.0);
                     gmax = std::max(std::min(gmax, g.Nu + 2.0), -2.0);
-                    const int kw0 = std::max(0, (int)std::floor(gmin - 1.5)), kw1 = std::min(g.Nu - 1, (int)std::floor(gmax + 1.5));
+                    // arc B / Bw (chained walk): widened by the brackets' half-width bound
+                    double wm = 1.5;
+                    if (g.type == GEO_ARC) {
+                        const double ddx = std::max(std::max(xl - h.sx, h.sx - xr), 0.0);
+                        const double ddy = std::max(std::max(yl - h.sy, h.sy - yh), 0.0);
+                        const double a = 0.5 * (h.use_x ? gf.dx : gf.dy), rlo = std::sqrt(ddx * ddx + ddy * ddy);
+                        wm += a / std::max(rlo - a, a) / g.du * 1.002;
+                    }
+                    const int kw0 = std::max(0, (int)std::floor(gmin - wm)), kw1 = std::min(g.Nu - 1, (int)std::floor(gmax + wm));
                     if (kw0 > kw1) continue;
                     const int c0 = (h.keep ? kw0 : g.Nu - 1 - kw1) & ~1, c1 = h.keep ? kw1 : g.Nu - 1 - kw0;
                     maxc = std::max(maxc, c1 - c0 + 1);
@@ -565,12 +573,12 @@ template <> constexpr int dtype_code<__half>() { return DT_F16; }
 // Staged prefix gather (vox_stage3d_kernel), then its fallback launch for
 // the views a CTA could not stage; -1 when this geometry is not covered (the
 // caller then uses vox_prefix3d_kernel).
-template <typename TO, int MODE, bool HEL>
+template <typename TO, int MODE, bool HEL, bool CHAIN = false>
 int launch_pfx_stage_mode(const Geom& g, const GeomF& gf, const ViewTables& vt, const CUtensorMap& map,
                           const float2* tab, TO* out, int* flags, int nbatch, int nview, int nzp, int BC, int BR,
                           cudaStream_t st, double z0dz, double zd0, double dvv, float cw, float atconst, float oscale) {
-    auto ks = vox_stage3d_kernel<TO, PFX_R, MODE, false, HEL>;
-    auto kf = vox_stage3d_kernel<TO, PFX_R, MODE, true, HEL>;
+    auto ks = vox_stage3d_kernel<TO, PFX_R, MODE, false, HEL, CHAIN>;
+    auto kf = vox_stage3d_kernel<TO, PFX_R, MODE, true, HEL, CHAIN>;
     const size_t smem = pfx_stage_smem(BC, BR), smem_fb = 2 * PS_WCH * sizeof(int4) + 128;
     if (cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return fail(XR_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
@@ -595,10 +603,16 @@ int run_pfx_stage(int eff, const Geom& g, const GeomF& gf, const ViewTables& vt,
     if (eff == OP_AT)
         return launch_pfx_stage_mode<TO, OP_AT, HEL>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR,
                                                      st, z0dz, zd0, dvv, cw, atconst, oscale);
+    if (eff == OP_B && vt.arc && !HEL)
+        return launch_pfx_stage_mode<TO, OP_B, false, true>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC,
+                                                           sp.BR, st, z0dz, zd0, dvv, cw, atconst, oscale);
     if (eff == OP_B)
         return launch_pfx_stage_mode<TO, OP_B, HEL>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR,
                                                     st, z0dz, zd0, dvv, cw, atconst, oscale);
     if (HEL) return -1;  // the helical Bw is hel_wbp_kernel
+    if (vt.arc)  // arc detector: the chained column walk
+        return launch_pfx_stage_mode<TO, OP_BW, false, true>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC,
+                                                            sp.BR, st, z0dz, zd0, dvv, cw, atconst, oscale);
     return launch_pfx_stage_mode<TO, OP_BW, HEL>(g, gf, vt, map, tab, out, flags, nbatch, nview, nzp, sp.BC, sp.BR, st,
                                                  z0dz, zd0, dvv, cw, atconst, oscale);
 }
@@ -770,7 +784,7 @@ int run3d(int op, const Geom& g, const TI* in, TO* out, const float* ang, int nb
         if (int rc = check_cuda("row_prefix3d")) return rc;
         const int nzp = (g.D + PFX_R - 1) / PFX_R;
         if ((long long)nzp * nbatch > 65535) return fail(XR_ERR_UNSUPPORTED, "depth x batch too large for one launch");
-        if (!vt.arc && !(g_host_hooks & XR_HOOK_PFX_NOSTAGE)) {
+        if (!(g_host_hooks & XR_HOOK_PFX_NOSTAGE)) {
             const int rc = run_pfx_stage<TO>(eff, g, gf, vt, tab, out, nbatch, nview, nzp, ws, l, st, z0dz, zd0, dvv,
                                              cw, atconst, oscale);
             if (rc >= 0) return rc;

@@ -1,7 +1,8 @@
 // Voxel gather (B, Bw, A^T) with TMA-staged row-prefix tables.
 //
-// Flat, parallel and (for A^T, whose column walk is not chained) arc
-// detectors.  The arithmetic per (pixel, view, column) is
+// Flat, parallel and arc detectors (CHAIN: B and Bw on arc detectors, whose
+// columns are walked with the reference's chained float32 angles, as in
+// vox_prefix3d_kernel).  The arithmetic per (pixel, view, column) is
 // that of vox_prefix3d_kernel (xr_vox_prefix.cuh), and so are the results
 // when every view is staged; what changes is where the table lookups go.
 //
@@ -71,7 +72,13 @@ __host__ __device__ inline size_t pfx_stage_smem(int BC, int BR) {
 // HEL: helical scan; the view's z placement and angular column pitch come
 // from vt.hel (zs and zoffh are then the view's, from the run's first voxel
 // j0), and a view whose z reach misses the run has nothing to stage.
-template <bool HEL>
+// CHAIN: the consumers bracket a pixel by one guess at its centre and a
+// bound on its footprint's half-width, a / (r - a) rad (a the half-length of
+// the pixel's edge segment, r its distance from the source); the box widens
+// by that bound at the least distance from the source to the tile, so that
+// no bracket is clamped and every chain starts where the unstaged kernel's
+// does.
+template <bool HEL, bool CHAIN>
 __device__ inline int4 pfx_window(const Geom& g, const GeomF& gf, const ViewTables& vt, const int v, const int ix0,
                                   const int iy0, const int j0, double zs, double zoffh, const double dvv, const int R,
                                   const int BC, const int BR) {
@@ -119,7 +126,15 @@ __device__ inline int4 pfx_window(const Geom& g, const GeomF& gf, const ViewTabl
     const float lo = fmaxf(fminf(gmin, (float)g.Nu + 2.0f), -2.0f);
     const float hi = fmaxf(fminf(gmax, (float)g.Nu + 2.0f), -2.0f);
     // the consumers' half column and guess error, the corners' guess error, one column
-    const float wm = 1.5f + (HEL || g.type == GEO_ARC ? 2.0f * XR_GUESS_ATAN_ERR * inv_du : 0.0f);
+    float wm = 1.5f + (HEL || g.type == GEO_ARC ? 2.0f * XR_GUESS_ATAN_ERR * inv_du : 0.0f);
+    if (CHAIN) {
+        // least distance from the source to the tile (the pixel centres lie inside it)
+        const float ddx = fmaxf(fmaxf(xl - (float)h.sx, (float)h.sx - xr), 0.0f);
+        const float ddy = fmaxf(fmaxf(yl - (float)h.sy, (float)h.sy - yh), 0.0f);
+        const float rlo = sqrtf(ddx * ddx + ddy * ddy) * 0.9999f;
+        const float a = 0.5f * (h.use_x ? gf.dx : gf.dy);
+        wm += a / fmaxf(rlo - a, a) * inv_du * 1.002f;
+    }
     const int kw0 = max(0, (int)floorf(lo - wm)), kw1 = min(g.Nu - 1, (int)floorf(hi + wm));
     if (kw0 > kw1) return none;
     // rows per voxel ib = colR / (q dvv) at its extremes over the box
@@ -164,7 +179,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 // elements, box {BC, BR, 1}.  unfit[cta]: set by the staged launch when it
 // skipped a view; the FALLBACK launch does only those CTAs' skipped views,
 // adding to what the staged launch stored.
-template <typename TO, int R, int MODE, bool FALLBACK, bool HEL = false>
+template <typename TO, int R, int MODE, bool FALLBACK, bool HEL = false, bool CHAIN = false>
 __global__ void __launch_bounds__(PS_T * PS_T, XR_PFXS_MINB)
 vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __grid_constant__ CUtensorMap map,
                    const float2* __restrict__ tab, TO* __restrict__ vol, int* __restrict__ unfit, const int nview,
@@ -206,7 +221,7 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
     }
     auto windows = [&](int vbase) {
         if (tid < PS_WCH && vbase + tid < nview) {
-            const int4 w = pfx_window<HEL>(g, gf, vt, vbase + tid, ix0, iy0, j0, zs0, zoffh0, dvv, R, BC, BR);
+            const int4 w = pfx_window<HEL, CHAIN>(g, gf, vt, vbase + tid, ix0, iy0, j0, zs0, zoffh0, dvv, R, BC, BR);
             wins[((vbase / PS_WCH) & 1) * PS_WCH + tid] = w;
             if (w.x < 0) s_unfit = 1;
         }
@@ -288,8 +303,20 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
             }
             lf *= oscale;
             const float sf = (float)h.s, cf = (float)h.c;
-            const float kf0 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xa, ya, inv_du);
-            const float kf1 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xb, yb, inv_du);
+            float kf0, kf1;
+            if (CHAIN) {
+                // one guess at the pixel centre and the footprint's half-width bound
+                const float kc = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, px, py, inv_du);
+                const float ex = px - (float)h.sx, ey = py - (float)h.sy;
+                const float a = 0.5f * (h.use_x ? gf.dx : gf.dy);
+                const float r2 = fmaf(ex, ex, ey * ey);
+                const float hw = __fdividef(a, fmaxf(r2 * rsqrtf(r2) - a, a)) * inv_du * 1.001f;
+                kf0 = kc - hw;
+                kf1 = kc + hw;
+            } else {
+                kf0 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xa, ya, inv_du);
+                kf1 = col_guess_fast(gf, h, sf, cf, h.dcx, h.dcy, xb, yb, inv_du);
+            }
             const float lo = fmaxf(fminf(fminf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
             const float hi = fmaxf(fminf(fmaxf(kf0, kf1), (float)Nu + 2.0f), -2.0f);
             // staged views: the bracket within the box's columns; the rows of
@@ -315,6 +342,17 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
                 pd += width(k);
             }
             float pk1 = pd;
+            ArcChain ch;
+            float qd = 0.0f;
+            const float4* __restrict__ ea = nullptr;
+            if (CHAIN) {
+                ea = vt.arc + 2 * (size_t)v * (Nu + 1);
+                qd = __fdividef((float)q, h.use_x ? gf.dx : gf.dy);  // pixels per axis unit on this line
+                ch.start(ea, k, keep, gf.du);
+                float d = ch.next_linear(ea, k + 1);
+                if (k + 1 == Nu) d = fminf(d, 0.0f);  // the detector's end
+                pk1 = fmaf(d, qd, pd);
+            }
             const float4 Wr = cWR[k];
             const float2 Rr = make_float2(Wr.z, Wr.w);
             const double ibr = mvdv * ((double)Rr.x + (double)Rr.y);
@@ -404,6 +442,11 @@ vox_stage3d_kernel(const Geom g, const GeomF gf, const ViewTables vt, const __gr
                 if (pkl >= 1.0f) break;  // column k starts right of the pixel
                 pd += width(k);
                 pk1 = pd;
+                if (CHAIN) {
+                    float d = ch.next_linear(ea, k + 1);
+                    if (k + 1 == Nu) d = fminf(d, 0.0f);
+                    pk1 = fmaf(d, qd, pd);
+                }
             }
         } while (false);
         if (!FALLBACK) {
