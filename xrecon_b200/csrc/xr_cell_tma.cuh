@@ -253,6 +253,39 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
     // place every row), rows per slice bt = Qk q dvv and q itself for the
     // line factor (FP32, rounded as the kernel uses them).
     const double t0c = fma(Qk * h.q0, zr0, -z0dz), t0l = Qk * h.q1 * zr0;
+    // Bw^T: the FBP weight of pixel p on line L.  The pixel centre is affine
+    // in (L, p), so the flat detector's distance term R - (s . x) / R and the
+    // arc detector's source offset are FMAs of L and p from per-view
+    // constants (FP64, rounded once).
+    float bw0 = 0.0f, bwL = 0.0f, bwp = 0.0f, bv0 = 0.0f, bvL = 0.0f, bvp = 0.0f;
+    if (MODE == OP_BWT) {
+        const double ax = (0.5 - 0.5 * g.W) * g.dx + g.shx;
+        const double ay = (h.use_x ? (0.5 * g.H - 0.5) : (0.5 - 0.5 * g.H)) * g.dy + g.shy;
+        const double bxL = h.use_x ? 0.0 : g.dx, bxp = h.use_x ? g.dx : 0.0;
+        const double byL = h.use_x ? -g.dy : 0.0, byp = h.use_x ? 0.0 : g.dy;
+        if (g.type == GEO_FLAT) {
+            const double R = g.sod;
+            bw0 = (float)(R - (h.sx * ax + h.sy * ay) / R);
+            bwL = (float)(-(h.sx * bxL + h.sy * byL) / R);
+            bwp = (float)(-(h.sx * bxp + h.sy * byp) / R);
+        } else if (g.type == GEO_ARC) {
+            bw0 = (float)(h.sx - ax); bwL = (float)(-bxL); bwp = (float)(-bxp);
+            bv0 = (float)(h.sy - ay); bvL = (float)(-byL); bvp = (float)(-byp);
+        }
+    }
+    auto bwt_weight = [&](float Lf, int pix) -> float {
+        const float pf = (float)pix;
+        if (g.type == GEO_FLAT) {
+            const float R = (float)g.sod;
+            const float den = fmaf(bwp, pf, fmaf(bwL, Lf, bw0));
+            return __fdividef(R * R, den * den);
+        }
+        if (g.type == GEO_ARC) {
+            const float ex = fmaf(bwp, pf, fmaf(bwL, Lf, bw0)), ey = fmaf(bvp, pf, fmaf(bvL, Lf, bv0));
+            return __fdividef(1.0f, fmaf(ex, ex, ey * ey));
+        }
+        return 1.0f;
+    };
     const float btc = (float)(Qk * dvv * h.q0), btl = (float)(Qk * dvv * h.q1);
     const float qc = (float)h.q0, ql = (float)h.q1;
 
@@ -297,11 +330,7 @@ cell_tma3d_kernel(const Geom g, const ViewTables vt, const __grid_constant__ CUt
                         float wi = 0.0f;
                         if (i < np) {
                             wi = (fminf(off + (float)(i + 1), u1) - fmaxf(off + (float)i, u0)) * lf;
-                            if (MODE == OP_BWT) {
-                                float px, py;
-                                pixel_center(g, h, L, pc + i, px, py);
-                                wi *= fbp_weight(g, h, px, py);
-                            }
+                            if (MODE == OP_BWT) wi *= bwt_weight(Lf, pc + i);
                         }
                         w[i] = wi;
                     }
